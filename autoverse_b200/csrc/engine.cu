@@ -1,0 +1,763 @@
+// Host runtime of the engine and its C ABI (include/flowlenia_cuda.h).
+//
+// One flp_propagator owns a CUDA stream and all device buffers of one world:
+// the state (double-buffered; the reference swaps `channels` with
+// `next_channels`, src/compute/propagator.rs:416-419), the affinity field,
+// the convolution scratch (kernel spectra or stencil taps) and two flow-bound
+// slots that follow the state buffers.  A step is 2 kernels on the direct
+// path or 4 on the FFT path; run(n) replays a captured CUDA graph of
+// GRAPH_STEPS steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/flowlenia_cuda.h"
+#include "kernels.h"
+#include "schema.h"
+
+namespace flp {
+
+thread_local std::string g_last_error;
+
+// Steps per captured CUDA graph (even, so a replay leaves the state in the
+// buffer it started from).
+constexpr int GRAPH_STEPS = 16;
+
+struct FlpError : std::runtime_error {
+    int code;
+    FlpError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        int code = (e == cudaErrorMemoryAllocation) ? FLP_ERR_OOM : FLP_ERR_CUDA;
+        throw FlpError(code, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+#define CK(x) cuda_check((x), #x)
+
+template <class T>
+T* dalloc(size_t n) {
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    return static_cast<T*>(p);
+}
+
+bool make_plan(int L, FftPlan& p) {
+    p = FftPlan();
+    p.L = L;
+    int m = L;
+    const int rads[4] = {4, 2, 3, 5};
+    for (int r : rads)
+        while (m % r == 0 && p.nst < 24) {
+            p.rad[p.nst++] = r;
+            m /= r;
+        }
+    return m == 1 && L >= 1;
+}
+
+static void upload_twiddles(std::vector<float2>& dst, int L, int count) {
+    for (int t = 0; t < count; ++t) {
+        double ang = -2.0 * M_PI * double(t) / double(L);
+        dst.push_back(make_float2(float(std::cos(ang)), float(std::sin(ang))));
+    }
+}
+
+static std::once_flag g_attr_once;
+static void set_attributes_once() {
+    std::call_once(g_attr_once, [] {
+        transport_2d_set_attributes();
+        fft2d_set_attributes(200 * 1024);
+    });
+}
+
+// Autotune cache: (W, H, D, C, K, rmax) -> chosen conv mode.
+static std::mutex g_tune_mu;
+static std::map<std::vector<int>, int> g_tune_cache;
+
+}  // namespace flp
+
+using namespace flp;
+
+struct flp_propagator {
+    SimulationConfig cfg;
+    int W = 0, H = 0, D = 1, C = 0, K = 0, dims = 2;
+    size_t N = 0;
+    cudaStream_t st = nullptr;
+    float* A[2] = {nullptr, nullptr};
+    int cur = 0;
+    float* U = nullptr;
+    std::vector<KDesc> kd;
+    KDesc* d_kd = nullptr;
+    float* d_taps = nullptr;
+    int rmax = 0;
+    bool direct_ok = false;
+    FlowParams fp{};
+    int* d_bound = nullptr;  // 2 slots x (max, min) as ordered ints
+    int* d_status = nullptr;
+    double2* d_partial = nullptr;
+    double* d_mass = nullptr;
+    int np = 0;
+    // FFT path
+    bool fft_ok = false;
+    FftGeom geom;
+    float2* d_tw = nullptr;
+    float2* d_S = nullptr;
+    float2* d_T = nullptr;
+    float2* d_KH = nullptr;
+    int* d_srcs = nullptr;
+    int* d_slot = nullptr;
+    int nsrc = 0;
+    int conv_mode = FLP_CONV_DIRECT;
+    float time = 0.f;
+    uint64_t step = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // profiling
+    std::vector<cudaEvent_t> prof_ev;
+    void* flush_buf = nullptr;
+    size_t flush_bytes = 0;
+
+    // Stage hook: called after each kernel of a step with its stage index
+    // (used by flp_profile_run to record events between kernels).
+    using Hook = void (*)(flp_propagator*, int);
+    Hook hook = nullptr;
+    void mark(int stage) {
+        if (hook) hook(this, stage);
+    }
+
+    void enqueue_conv(const float* a, int* reset_slot) {
+        if (K == 0) {
+            // No kernels: the affinity stays zero (it is cleared at creation).
+            launch_bound_reset(reset_slot, st);
+            mark(0);
+            return;
+        }
+        if (conv_mode == FLP_CONV_DIRECT) {
+            launch_conv_direct_2d(a, U, d_kd, K, d_taps, W, H, C, rmax, reset_slot, st);
+            mark(0);
+        } else {
+            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, reset_slot, st);
+            mark(0);
+            launch_fft_cols(d_S, d_KH, d_T, d_slot, K, W, H, geom, 0, 1.f, st);
+            mark(1);
+            launch_fft_c2r_growth(d_T, U, d_kd, K, W, H, C, geom, st);
+            mark(2);
+        }
+    }
+
+    std::vector<std::string> stage_names() const {
+        if (K == 0) return {"bound_reset", "transport_2d"};
+        if (conv_mode == FLP_CONV_DIRECT) return {"conv_direct_growth_2d", "transport_2d"};
+        return {"fft_rows_r2c", "fft_cols_conv", "fft_rows_c2r_growth", "transport_2d"};
+    }
+
+    void enqueue_step() {
+        const float* a = A[cur];
+        float* an = A[cur ^ 1];
+        int* bin = d_bound + 2 * cur;
+        int* bout = d_bound + 2 * (cur ^ 1);
+        enqueue_conv(a, bout);
+        launch_transport_2d(a, U, an, C, W, H, fp, bin, bout, d_status, st);
+        mark(int(stage_names().size()) - 1);
+        CK(cudaGetLastError());
+        cur ^= 1;
+    }
+
+    void advance_clock(uint64_t n) {
+        for (uint64_t i = 0; i < n; ++i) time += cfg.dt;  // f32 accumulation, propagator.rs:418
+        step += n;
+    }
+
+    void free_all() {
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_bound, d_status, d_partial, d_mass,
+                        d_tw, d_S, d_T, d_KH, d_srcs, d_slot};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto e : prof_ev) cudaEventDestroy(e);
+        if (flush_buf) cudaFree(flush_buf);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace flp {
+
+static void setup_direct(flp_propagator* h, const std::vector<KernelStencil>& ks) {
+    // Taps: flipped effective stencil (convolution, not correlation); when
+    // 2r+1 exceeds a side, offsets that alias onto one torus cell keep a
+    // single tap carrying the wrap-padded value (kernel.rs:98-117).
+    std::vector<float> taps;
+    h->rmax = 0;
+    for (int k = 0; k < h->K; ++k) {
+        const KernelStencil& s = ks[k];
+        int r = s.radius, side = s.size;
+        h->rmax = std::max(h->rmax, r);
+        h->kd[k].r = r;
+        h->kd[k].tap_off = int(taps.size());
+        std::vector<float> pad = pad_kernel(s, h->W, h->H, 1);
+        std::vector<float> eff(size_t(side) * side, 0.f);
+        std::vector<char> seen(size_t(h->W) * h->H, 0);
+        for (int dy = -r; dy <= r; ++dy)
+            for (int dx = -r; dx <= r; ++dx) {
+                int tx = ((dx % h->W) + h->W) % h->W, ty = ((dy % h->H) + h->H) % h->H;
+                size_t t = size_t(ty) * h->W + tx;
+                if (seen[t]) continue;
+                seen[t] = 1;
+                // out[x] = sum_d A[x - d] S[d] = sum_d A[x + d] S[-d]
+                eff[size_t(-dy + r) * side + (-dx + r)] = pad[t];
+            }
+        taps.insert(taps.end(), eff.begin(), eff.end());
+    }
+    h->direct_ok = h->rmax <= MAX_DIRECT_RADIUS;
+    if (!taps.empty()) {
+        h->d_taps = dalloc<float>(taps.size());
+        CK(cudaMemcpy(h->d_taps, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+}
+
+static void setup_fft(flp_propagator* h, const std::vector<KernelStencil>& ks) {
+    const int W = h->W, H = h->H;
+    h->fft_ok = false;
+    if (W % 2 != 0 || W < 2) return;
+    FftGeom g;
+    if (!make_plan(W / 2, g.pm) || !make_plan(H, g.ph)) return;
+    const int M = W / 2, Wc = M + 1;
+    g.NR = 8;
+    while (g.NR > 1 && fft_rows_smem(W, g.NR, true) > 200 * 1024) g.NR /= 2;
+    g.NC = 8;
+    while (g.NC > 1 && fft_cols_smem(H, g.NC) > 200 * 1024) g.NC /= 2;
+    if (fft_rows_smem(W, g.NR, true) > 200 * 1024 || fft_cols_smem(H, g.NC) > 200 * 1024) return;
+    std::vector<float2> tw;
+    upload_twiddles(tw, M, M);
+    upload_twiddles(tw, W, Wc);
+    upload_twiddles(tw, H, H);
+    h->d_tw = dalloc<float2>(tw.size());
+    CK(cudaMemcpy(h->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    g.twM = h->d_tw;
+    g.twW = h->d_tw + M;
+    g.twH = h->d_tw + M + Wc;
+    h->geom = g;
+    // source channels and their spectrum slots
+    std::vector<int> srcs, slot(h->K);
+    for (int k = 0; k < h->K; ++k) {
+        auto it = std::find(srcs.begin(), srcs.end(), h->kd[k].src);
+        if (it == srcs.end()) { slot[k] = int(srcs.size()); srcs.push_back(h->kd[k].src); }
+        else slot[k] = int(it - srcs.begin());
+    }
+    h->nsrc = int(srcs.size());
+    h->d_srcs = dalloc<int>(srcs.size());
+    h->d_slot = dalloc<int>(slot.size());
+    CK(cudaMemcpy(h->d_srcs, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_slot, slot.data(), slot.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const size_t spec = size_t(Wc) * H;
+    h->d_S = dalloc<float2>(spec * std::max(h->nsrc, 1));
+    h->d_T = dalloc<float2>(spec * h->K);
+    h->d_KH = dalloc<float2>(spec * h->K);
+    // Kernel spectra: FFT of the wrap-padded stencils, scaled by 1/(W*H)
+    // (the inverse's normalisation, fft.rs:389, folded in once).
+    std::vector<float> padded(size_t(h->K) * W * H);
+    for (int k = 0; k < h->K; ++k) {
+        std::vector<float> p = pad_kernel(ks[k], W, H, 1);
+        std::copy(p.begin(), p.end(), padded.begin() + size_t(k) * W * H);
+    }
+    float* d_pad = dalloc<float>(padded.size());
+    float2* d_tmp = dalloc<float2>(spec * h->K);
+    CK(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, H, g, nullptr, h->st);
+    launch_fft_cols(d_tmp, nullptr, h->d_KH, nullptr, h->K, W, H, g, 1, float(1.0 / (double(W) * double(H))), h->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    cudaFree(d_pad);
+    cudaFree(d_tmp);
+    h->fft_ok = true;
+}
+
+static float time_conv(flp_propagator* h, int mode, int reps) {
+    int saved = h->conv_mode;
+    h->conv_mode = mode;
+    for (int i = 0; i < 2; ++i) h->enqueue_conv(h->A[h->cur], nullptr);
+    CK(cudaEventRecord(h->ev0, h->st));
+    for (int i = 0; i < reps; ++i) h->enqueue_conv(h->A[h->cur], nullptr);
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->conv_mode = saved;
+    return ms / reps;
+}
+
+static void resolve_conv_mode(flp_propagator* h, int requested) {
+    if (h->K == 0) { h->conv_mode = FLP_CONV_DIRECT; return; }
+    if (requested == FLP_CONV_DIRECT) {
+        if (!h->direct_ok) throw FlpError(FLP_ERR_UNSUPPORTED, "direct convolution supports radius <= 24");
+        h->conv_mode = FLP_CONV_DIRECT;
+        return;
+    }
+    if (requested == FLP_CONV_FFT) {
+        if (!h->fft_ok) throw FlpError(FLP_ERR_UNSUPPORTED, "FFT path needs an even width and sides of factors 2,3,5");
+        h->conv_mode = FLP_CONV_FFT;
+        return;
+    }
+    if (!h->fft_ok && !h->direct_ok)
+        throw FlpError(FLP_ERR_UNSUPPORTED, "no convolution path for this grid/radius");
+    if (!h->fft_ok) { h->conv_mode = FLP_CONV_DIRECT; return; }
+    if (!h->direct_ok) { h->conv_mode = FLP_CONV_FFT; return; }
+    std::vector<int> key = {h->W, h->H, h->D, h->C, h->K, h->rmax, h->nsrc};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) { h->conv_mode = it->second; return; }
+    }
+    float t_direct = time_conv(h, FLP_CONV_DIRECT, 5);
+    float t_fft = time_conv(h, FLP_CONV_FFT, 5);
+    h->conv_mode = t_fft < t_direct ? FLP_CONV_FFT : FLP_CONV_DIRECT;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = h->conv_mode;
+}
+
+static FlowParams make_flow_params(const SimulationConfig& cfg) {
+    FlowParams fp{};
+    fp.dt = cfg.dt;
+    fp.s = cfg.flow.distribution_size;
+    float two_s = 2.0f * fp.s;
+    fp.total_area = two_s * two_s;
+    int e = 0;
+    float mant = std::frexp(fp.total_area, &e);
+    fp.area_pow2 = (fp.total_area > 0.f && mant == 0.5f && std::isnormal(fp.total_area)) ? 1 : 0;
+    fp.inv_area = fp.area_pow2 ? 1.0f / fp.total_area : 0.f;
+    fp.beta_a = cfg.flow.beta_a;
+    fp.nexp = cfg.flow.n;
+    fp.point_mode = fp.total_area < 1e-10f ? 1 : 0;
+    std::vector<float> wsum(cfg.channels, 0.f);
+    for (const auto& k : cfg.kernels) wsum[k.target_channel] += std::fabs(k.weight);
+    fp.ubound = 0.f;
+    for (float w : wsum) fp.ubound = std::max(fp.ubound, w);
+    return fp;
+}
+
+static void create(const std::string& json, flp_propagator* h) {
+    h->cfg = parse_config(json);
+    const SimulationConfig& c = h->cfg;
+    if (c.is_3d()) throw FlpError(FLP_ERR_UNSUPPORTED, "3D worlds are served by the 3D engine");
+    h->W = c.width; h->H = c.height; h->D = c.depth; h->C = c.channels; h->K = int(c.kernels.size());
+    h->dims = c.is_3d() ? 3 : 2;
+    h->N = c.grid_size();
+    set_attributes_once();
+    CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    const size_t CN = size_t(h->C) * h->N;
+    h->A[0] = dalloc<float>(CN);
+    h->A[1] = dalloc<float>(CN);
+    h->U = dalloc<float>(CN);
+    CK(cudaMemsetAsync(h->A[0], 0, CN * sizeof(float), h->st));
+    CK(cudaMemsetAsync(h->A[1], 0, CN * sizeof(float), h->st));
+    CK(cudaMemsetAsync(h->U, 0, CN * sizeof(float), h->st));
+    h->d_bound = dalloc<int>(4);
+    h->d_status = dalloc<int>(1);
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
+    h->np = 256;
+    h->d_partial = dalloc<double2>(h->np);
+    h->d_mass = dalloc<double>(1);
+    // kernels
+    std::vector<KernelStencil> ks;
+    h->kd.resize(h->K);
+    for (int k = 0; k < h->K; ++k) {
+        const KernelConfig& kc = c.kernels[k];
+        ks.push_back(build_kernel(kc, c.kernel_radius, h->dims));
+        KDesc d{};
+        d.src = kc.source_channel;
+        d.tgt = kc.target_channel;
+        d.weight = kc.weight;
+        d.mu = kc.mu;
+        float sigma_sq_2 = 2.0f * kc.sigma * kc.sigma;
+        d.inv2s2 = 1.0f / sigma_sq_2;
+        h->kd[k] = d;
+    }
+    setup_direct(h, ks);
+    h->d_kd = dalloc<KDesc>(h->kd.size());
+    if (h->K) CK(cudaMemcpy(h->d_kd, h->kd.data(), h->kd.size() * sizeof(KDesc), cudaMemcpyHostToDevice));
+    setup_fft(h, ks);
+    h->fp = make_flow_params(c);
+    launch_bound_init(h->A[0], h->C, h->N, h->d_bound, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    resolve_conv_mode(h, FLP_CONV_AUTO);
+}
+
+static void upload_state(flp_propagator* h, const float* src, size_t n) {
+    const size_t CN = size_t(h->C) * h->N;
+    if (n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "state size mismatch: expected " + std::to_string(CN));
+    CK(cudaMemcpyAsync(h->A[h->cur], src, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    launch_bound_init(h->A[h->cur], h->C, h->N, h->d_bound + 2 * h->cur, h->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+}
+
+static void build_graph(flp_propagator* h) {
+    int c0 = h->cur;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (int i = 0; i < GRAPH_STEPS; ++i) h->enqueue_step();
+    } catch (...) {
+        cudaStreamEndCapture(h->st, &g);
+        if (g) cudaGraphDestroy(g);
+        h->cur = c0;
+        throw;
+    }
+    CK(cudaStreamEndCapture(h->st, &g));
+    h->cur = c0;  // GRAPH_STEPS is even: the graph leaves the state in the same buffer
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    h->graph[c0] = ge;
+}
+
+static void run_steps(flp_propagator* h, uint64_t n) {
+    while (n >= uint64_t(GRAPH_STEPS)) {
+        if (!h->graph[h->cur]) build_graph(h);
+        CK(cudaGraphLaunch(h->graph[h->cur], h->st));
+        h->advance_clock(GRAPH_STEPS);
+        n -= GRAPH_STEPS;
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        h->enqueue_step();
+        h->advance_clock(1);
+    }
+}
+
+static void invalidate_graphs(flp_propagator* h) {
+    for (auto& g : h->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+static void prof_hook(flp_propagator* h, int stage) { CK(cudaEventRecord(h->prof_ev[1 + stage], h->st)); }
+
+static void profile_run(flp_propagator* h, int steps, int flush, float* stage_ms, int max_stages, int* n_stages,
+                        char* names, size_t names_len, float* step_ms) {
+    std::vector<std::string> nm = h->stage_names();
+    const int ns = int(nm.size());
+    while (int(h->prof_ev.size()) < ns + 1) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        h->prof_ev.push_back(e);
+    }
+    if (flush && !h->flush_buf) {
+        int dev = 0, l2 = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+        h->flush_bytes = std::max<size_t>(size_t(2) * size_t(l2), size_t(64) << 20);
+        CK(cudaMalloc(&h->flush_buf, h->flush_bytes));
+    }
+    std::vector<double> acc(ns, 0.0);
+    double total = 0.0;
+    h->hook = prof_hook;
+    try {
+        for (int s = 0; s < steps; ++s) {
+            if (flush) CK(cudaMemsetAsync(h->flush_buf, s & 0xFF, h->flush_bytes, h->st));
+            CK(cudaEventRecord(h->prof_ev[0], h->st));
+            h->enqueue_step();
+            h->advance_clock(1);
+            CK(cudaEventSynchronize(h->prof_ev[ns]));
+            for (int i = 0; i < ns; ++i) {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, h->prof_ev[i], h->prof_ev[i + 1]));
+                acc[i] += ms;
+            }
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->prof_ev[0], h->prof_ev[ns]));
+            total += ms;
+        }
+    } catch (...) {
+        h->hook = nullptr;
+        throw;
+    }
+    h->hook = nullptr;
+    if (n_stages) *n_stages = ns;
+    for (int i = 0; i < ns && i < max_stages; ++i)
+        if (stage_ms) stage_ms[i] = float(acc[i]);
+    if (step_ms) *step_ms = float(total);
+    if (names && names_len) {
+        std::string joined;
+        for (int i = 0; i < ns; ++i) joined += (i ? "," : "") + nm[i];
+        std::strncpy(names, joined.c_str(), names_len - 1);
+        names[names_len - 1] = 0;
+    }
+}
+
+}  // namespace flp
+
+// ------------------------------------------------------------------ C ABI ---
+#define FLP_TRY(body)                                                     \
+    try {                                                                 \
+        body;                                                             \
+        return FLP_OK;                                                    \
+    } catch (const flp::FlpError& e) {                                    \
+        flp::g_last_error = e.what();                                     \
+        return e.code;                                                    \
+    } catch (const flp::ConfigError& e) {                                 \
+        flp::g_last_error = e.what();                                     \
+        return FLP_ERR_INVALID_CONFIG;                                    \
+    } catch (const std::bad_alloc&) {                                     \
+        flp::g_last_error = "host allocation failed";                     \
+        return FLP_ERR_OOM;                                               \
+    } catch (const std::exception& e) {                                   \
+        flp::g_last_error = e.what();                                     \
+        return FLP_ERR_INVALID_ARGUMENT;                                  \
+    }
+
+#define FLP_CHECK_HANDLE(h)                                                    \
+    if (!(h)) {                                                                \
+        flp::g_last_error = "null handle";                                     \
+        return FLP_ERR_INVALID_ARGUMENT;                                       \
+    }
+
+extern "C" {
+
+const char* flp_last_error(void) { return flp::g_last_error.c_str(); }
+
+int flp_create(const char* config_json, flp_propagator** out) {
+    if (!config_json || !out) {
+        flp::g_last_error = "null argument";
+        return FLP_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    flp_propagator* h = new flp_propagator();
+    try {
+        flp::create(config_json, h);
+    } catch (...) {
+        h->free_all();
+        delete h;
+        FLP_TRY(throw)
+    }
+    *out = h;
+    return FLP_OK;
+}
+
+int flp_destroy(flp_propagator* h) {
+    if (!h) return FLP_OK;
+    cudaStreamSynchronize(h->st);
+    h->free_all();
+    delete h;
+    return FLP_OK;
+}
+
+int flp_seed_generate(const char* config_json, const char* seed_json, float* out, size_t n) {
+    FLP_TRY({
+        if (!config_json || !seed_json || !out) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null argument");
+        SimulationConfig c = parse_config(config_json);
+        std::vector<float> g = generate_seed(seed_json, c);
+        if (n != g.size()) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "output size mismatch: expected " + std::to_string(g.size()));
+        std::memcpy(out, g.data(), g.size() * sizeof(float));
+    })
+}
+
+int flp_state_from_seed(flp_propagator* h, const char* seed_json) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!seed_json) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null seed");
+        std::vector<float> g = generate_seed(seed_json, h->cfg);
+        upload_state(h, g.data(), g.size());
+        h->time = 0.f;
+        h->step = 0;
+    })
+}
+
+int flp_write_state(flp_propagator* h, const float* state, size_t n, float time, uint64_t step) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!state) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null state");
+        upload_state(h, state, n);
+        h->time = time;
+        h->step = step;
+    })
+}
+
+int flp_read_state(flp_propagator* h, float* out, size_t n, float* time, uint64_t* step) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        const size_t CN = size_t(h->C) * h->N;
+        if (!out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "state size mismatch: expected " + std::to_string(CN));
+        CK(cudaMemcpyAsync(out, h->A[h->cur], CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        if (time) *time = h->time;
+        if (step) *step = h->step;
+    })
+}
+
+int flp_step(flp_propagator* h) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        h->enqueue_step();
+        h->advance_clock(1);
+    })
+}
+
+int flp_run(flp_propagator* h, uint64_t n) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY(run_steps(h, n))
+}
+
+int flp_synchronize(flp_propagator* h) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        CK(cudaStreamSynchronize(h->st));
+        int status = 0;
+        CK(cudaMemcpy(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (status) {
+            CK(cudaMemset(h->d_status, 0, sizeof(int)));
+            if (status & STATUS_NONFINITE) throw FlpError(FLP_ERR_NONFINITE, "non-finite mass in the state");
+            if (status & STATUS_TIMEOUT) throw FlpError(FLP_ERR_TIMEOUT, "a bounded device wait timed out");
+        }
+    })
+}
+
+int flp_total_mass(flp_propagator* h, double* out) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!out) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null output");
+        launch_mass_fp64(h->A[h->cur], size_t(h->C) * h->N, h->d_partial, h->np, h->d_mass, h->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, h->d_mass, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    })
+}
+
+int flp_total_mass_f32(flp_propagator* h, float* out) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!out) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null output");
+        std::vector<float> s(size_t(h->C) * h->N);
+        CK(cudaMemcpyAsync(s.data(), h->A[h->cur], s.size() * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        float total = 0.f;
+        for (int c = 0; c < h->C; ++c) {
+            float m = 0.f;
+            for (size_t i = 0; i < h->N; ++i) m += s[size_t(c) * h->N + i];
+            total += m;
+        }
+        *out = total;
+    })
+}
+
+int flp_get_info(flp_propagator* h, flp_info* out) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!out) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null output");
+        out->width = h->W; out->height = h->H; out->depth = h->D;
+        out->channels = h->C; out->n_kernels = h->K;
+        out->conv_mode = h->conv_mode;
+        out->time = h->time;
+        out->step = h->step;
+    })
+}
+
+int flp_set_conv_mode(flp_propagator* h, int mode) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (mode < FLP_CONV_AUTO || mode > FLP_CONV_FFT) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "bad conv mode");
+        if (mode == FLP_CONV_AUTO) {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune_cache.erase({h->W, h->H, h->D, h->C, h->K, h->rmax, h->nsrc});
+        }
+        CK(cudaStreamSynchronize(h->st));
+        resolve_conv_mode(h, mode);
+        invalidate_graphs(h);
+    })
+}
+
+void* flp_stream(flp_propagator* h) { return h ? static_cast<void*>(h->st) : nullptr; }
+
+const float* flp_device_state(flp_propagator* h) { return h ? h->A[h->cur] : nullptr; }
+
+int flp_device_info(char* pci_bus_id, int len, int* sm_count, size_t* l2_bytes) {
+    FLP_TRY({
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        if (pci_bus_id && len > 0) CK(cudaDeviceGetPCIBusId(pci_bus_id, len, dev));
+        if (sm_count) CK(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
+        if (l2_bytes) {
+            int l2 = 0;
+            CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+            *l2_bytes = size_t(l2);
+        }
+    })
+}
+
+int flp_host_alloc(size_t bytes, void** out) {
+    FLP_TRY({
+        if (!out) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null output");
+        *out = nullptr;
+        CK(cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault));
+    })
+}
+
+int flp_host_free(void* p) {
+    FLP_TRY({
+        if (p) CK(cudaFreeHost(p));
+    })
+}
+
+int flp_profile_run(flp_propagator* h, int steps, int flush_l2, float* stage_ms, int max_stages, int* n_stages,
+                    char* names, size_t names_len, float* step_ms) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (steps < 0) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "negative step count");
+        profile_run(h, steps, flush_l2, stage_ms, max_stages, n_stages, names, names_len, step_ms);
+    })
+}
+
+int flp_debug_affinity(flp_propagator* h, float* aff_out, size_t n) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        const size_t CN = size_t(h->C) * h->N;
+        if (!aff_out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "size mismatch");
+        h->enqueue_conv(h->A[h->cur], nullptr);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(aff_out, h->U, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    })
+}
+
+int flp_debug_transport(flp_propagator* h, const float* state, const float* aff, float* out, size_t n) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        const size_t CN = size_t(h->C) * h->N;
+        if (!state || !aff || !out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "size mismatch");
+        float* a = dalloc<float>(CN);
+        float* u = dalloc<float>(CN);
+        float* o = dalloc<float>(CN);
+        int* slots = dalloc<int>(4);
+        try {
+            CK(cudaMemcpyAsync(a, state, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+            CK(cudaMemcpyAsync(u, aff, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+            launch_bound_init(a, h->C, h->N, slots, h->st);
+            launch_bound_reset(slots + 2, h->st);
+            launch_transport_2d(a, u, o, h->C, h->W, h->H, h->fp, slots, slots + 2, h->d_status, h->st);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(out, o, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+            CK(cudaStreamSynchronize(h->st));
+        } catch (...) {
+            cudaFree(a); cudaFree(u); cudaFree(o); cudaFree(slots);
+            throw;
+        }
+        cudaFree(a); cudaFree(u); cudaFree(o); cudaFree(slots);
+    })
+}
+
+}  // extern "C"

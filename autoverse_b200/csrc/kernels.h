@@ -1,0 +1,58 @@
+// Launch interface between the host runtime (engine.cu) and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "common.cuh"
+
+namespace flp {
+
+constexpr int MAX_DIRECT_RADIUS = 24;
+
+// Radix plan of one FFT length (radices 4, 2, 3, 5, in that order).
+struct FftPlan {
+    int L = 1;
+    int nst = 0;
+    int rad[24] = {0};
+};
+
+// Geometry and twiddle tables of one 2D world for the FFT path.
+struct FftGeom {
+    int NR = 8;  // rows per CTA in the row passes
+    int NC = 8;  // columns per CTA in the column pass
+    FftPlan pm;  // length W/2
+    FftPlan ph;  // length H
+    const float2* twM = nullptr;  // exp(-2 pi i t / (W/2)), t < W/2
+    const float2* twW = nullptr;  // exp(-2 pi i t / W),     t <= W/2
+    const float2* twH = nullptr;  // exp(-2 pi i t / H),     t < H
+};
+
+// direct convolution + growth
+size_t conv_direct_smem_bytes(int rmax);
+void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, const float* taps, int W, int H, int C,
+                           int rmax, int* reset_slot, cudaStream_t st);
+
+// fused transport
+size_t transport_smem_bytes();
+void transport_2d_set_attributes();
+void launch_transport_2d(const float* A, const float* U, float* Anext, int C, int W, int H, const FlowParams& fp,
+                         const int* bound_in, int* bound_out, int* status, cudaStream_t st);
+void launch_bound_init(const float* A, int C, size_t N, int* slot, cudaStream_t st);
+void launch_bound_reset(int* slot, cudaStream_t st);
+
+// FP64 compensated mass
+void launch_mass_fp64(const float* A, size_t n, double2* partial, int np, double* out, cudaStream_t st);
+
+// FFT path
+size_t fft_rows_smem(int W, int NR, bool with_u);
+size_t fft_cols_smem(int H, int NC);
+void fft2d_set_attributes(size_t max_bytes);
+void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
+                    int* reset_slot, cudaStream_t st);
+void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
+                     const FftGeom& g, int mode, float scale, cudaStream_t st);
+void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,
+                           cudaStream_t st);
+
+}  // namespace flp

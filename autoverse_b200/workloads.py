@@ -1,0 +1,83 @@
+"""Seeded synthetic workloads with the shapes, sizes and value distributions of
+the engine's benchmark configurations.  All randomness comes from
+``numpy.random.default_rng(seed)``; the default seed is 0x5EED.
+
+* ``single_blob``     — 2D, 1 channel, one ring kernel, Gaussian-blob seed
+                        (256x256, R=13 as benchmarked; any size for tests).
+* ``multispecies``    — 2D, C channels, all C*C source->target kernels with
+                        1-3 random rings each, uniform-noise patches.
+* ``batched_worlds``  — many independent 2D worlds of uneven sides, channels,
+                        radii and parameters (see batch.py).
+* ``sphere3d``        — 3D, one spherical-shell kernel, Gaussian-sphere seed.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DEFAULT_SEED = 0x5EED
+
+RING = {"amplitude": 1.0, "distance": 0.5, "width": 0.15}
+
+
+def kernel(src=0, tgt=0, rings=None, weight=1.0, mu=0.15, sigma=0.015, radius=1.0):
+    return {"radius": radius, "rings": rings or [dict(RING)], "weight": weight, "mu": mu, "sigma": sigma,
+            "source_channel": src, "target_channel": tgt}
+
+
+def config(width, height, channels, kernels, dt=0.2, kernel_radius=13, depth=1, beta_a=1.0, n=2.0, s=1.0):
+    return {"width": width, "height": height, "depth": depth, "channels": channels, "dt": dt,
+            "kernel_radius": kernel_radius, "kernels": kernels,
+            "flow": {"beta_a": beta_a, "n": n, "distribution_size": s}}
+
+
+def single_blob(size=256, R=13, mu=0.15, sigma=0.015, dt=0.2, blob_radius=0.1, height=None):
+    cfg = config(size, height or size, 1, [kernel(mu=mu, sigma=sigma)], dt=dt, kernel_radius=R)
+    seed = {"pattern": {"type": "GaussianBlob", "center": [0.5, 0.5], "radius": blob_radius, "amplitude": 1.0,
+                        "channel": 0}}
+    return cfg, seed
+
+
+def random_rings(rng, lo=1, hi=3):
+    return [{"amplitude": float(rng.uniform(0.2, 1.0)), "distance": float(rng.uniform(0.2, 0.9)),
+             "width": float(rng.uniform(0.05, 0.2))} for _ in range(int(rng.integers(lo, hi + 1)))]
+
+
+def multispecies(size=512, channels=3, R=15, patches=20, patch=40, seed=DEFAULT_SEED, height=None, dt=0.2):
+    """C channels, K = C*C kernels (every source->target pair), random rings and
+    growth parameters; state = `patches` uniform-noise squares per channel on
+    zeros (later patches overwrite earlier ones)."""
+    rng = np.random.default_rng(seed)
+    H = height or size
+    ks = []
+    for src in range(channels):
+        for tgt in range(channels):
+            ks.append(kernel(src, tgt, random_rings(rng), weight=float(rng.uniform(0.3, 1.0)),
+                             mu=float(rng.uniform(0.1, 0.3)), sigma=float(rng.uniform(0.01, 0.05))))
+    cfg = config(size, H, channels, ks, dt=dt, kernel_radius=R)
+    state = np.zeros((channels, H, size), dtype=np.float32)
+    for c in range(channels):
+        for _ in range(patches):
+            x0 = int(rng.integers(0, size - patch + 1)) if size > patch else 0
+            y0 = int(rng.integers(0, H - patch + 1)) if H > patch else 0
+            ph, pw = min(patch, H), min(patch, size)
+            state[c, y0:y0 + ph, x0:x0 + pw] = rng.uniform(0.0, 1.0, (ph, pw)).astype(np.float32)
+    return cfg, state.reshape(channels, -1)
+
+
+def patches_as_custom_seed(state: np.ndarray, width: int, height: int) -> dict:
+    """The same state expressed in the reference's seed schema (Pattern::Custom,
+    src/schema/seed.rs:126-129); only non-zero cells are listed."""
+    vals = []
+    C = state.shape[0]
+    st = state.reshape(C, height, width)
+    for c in range(C):
+        ys, xs = np.nonzero(st[c])
+        vals.extend([int(x), int(y), c, float(st[c, y, x])] for y, x in zip(ys, xs))
+    return {"pattern": {"type": "Custom", "values": vals}}
+
+
+def sphere3d(size=128, R=10, mu=0.15, sigma=0.017, radius=0.12, dt=0.2):
+    cfg = config(size, size, 1, [kernel(mu=mu, sigma=sigma)], dt=dt, kernel_radius=R, depth=size)
+    seed = {"pattern": {"type": "GaussianSphere", "center": [0.5, 0.5, 0.5], "radius": radius, "amplitude": 1.0,
+                        "channel": 0}}
+    return cfg, seed

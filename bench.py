@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Benchmark of the Flow Lenia step engine (one JSON line on stdout, rank 0).
+
+Default workload: 2D multispecies world, 512x512 torus, 3 channels, 9 kernels
+(every source->target pair, 1-3 random rings each), R=15, dt=0.2, state = 20
+uniform-noise 40x40 patches per channel; seeded synthetic data (seed 0x5EED).
+
+* ``value``: cell-steps/s over exactly K steps, device time from CUDA events
+  on the engine's stream, every step preceded by an L2 flush (a write of twice
+  the L2 size, outside the timed events), max over ranks.
+* ``e2e``: the same metric through the public API with pinned host buffers:
+  every step copies the state host->device, steps, and copies it back.
+* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
+  average event-timed duration, against the measured HBM copy bandwidth.
+* ``cpu_baseline``: the CPU oracle (a C restatement of the reference's
+  CpuPropagator) on the host cores, on a bounded sample of the same workload.
+
+``--impl reference`` times that CPU implementation alone on the same config
+and metric (rank 0; other ranks exit 0).  With ``--gpus N`` under torchrun
+every rank runs an independent replica of the world (a single world does not
+shard), so ``value`` is N x the per-GPU work over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+RANK = int(os.environ.get("RANK", "0"))
+LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+if WORLD > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
+    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+
+import numpy as np  # noqa: E402
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=["multispecies512", "blob256"], default="multispecies512")
+    ap.add_argument("--e2e-steps", type=int, default=300)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-flush", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name):
+    from autoverse_b200 import workloads as wl
+    if name == "multispecies512":
+        cfg, state = wl.multispecies(512, channels=3, R=15)
+        desc = {"workload": "multispecies 512x512 torus, 3 channels, 9 kernels (all src->tgt pairs, 1-3 rings), "
+                            "R=15, dt=0.2, beta_a=1, n=2, s=1, 20 U(0,1) 40x40 patches per channel",
+                "width": 512, "height": 512, "channels": 3, "kernels": 9, "kernel_radius": 15}
+    else:
+        from oracle import oracle as O
+        cfg, seed = wl.single_blob(256)
+        state = O.seed_generate(seed, cfg)
+        desc = {"workload": "single blob 256x256 torus, 1 channel, 1 kernel (ring 1.0/0.5/0.15), R=13, mu=0.15, "
+                            "sigma=0.015, dt=0.2, Gaussian blob r=0.1",
+                "width": 256, "height": 256, "channels": 1, "kernels": 1, "kernel_radius": 13}
+    return cfg, state, desc
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def stage_bytes(cfg, stage):
+    """Algorithmic HBM bytes of one launch of each stage."""
+    W, H, C = cfg["width"], cfg["height"], cfg["channels"]
+    K = len(cfg["kernels"])
+    N = W * H
+    nsrc = len({k["source_channel"] for k in cfg["kernels"]})
+    spec = (W // 2 + 1) * H * 8
+    return {
+        "fft_rows_r2c": nsrc * N * 4 + nsrc * spec,
+        "fft_cols_conv": K * spec * 3,
+        "fft_rows_c2r_growth": K * spec + C * N * 4,
+        "transport_2d": 3 * C * N * 4,
+        "conv_direct_growth_2d": nsrc * N * 4 + C * N * 4,
+    }.get(stage)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str):
+        self.bus = bus_id.lower()
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0:  # wait for the first sample
+                time.sleep(0.05)
+                if os.path.getsize(self.file.name) > 0:
+                    break
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                bus = parts[0].lower()
+                if self.bus and not (bus.endswith(self.bus[-12:]) or self.bus.endswith(bus[-12:])):
+                    continue
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows), "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init():
+    if WORLD <= 1:
+        return None
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("gloo", timeout=timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_run(cfg, state, seconds: float, max_steps: int, warmup: int = 1):
+    """The oracle on all host cores: conv parallel over kernels and stencil
+    over channels, as the reference's rayon loops (propagator.rs:259-267, 332-371)."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    p = O.OraclePropagator(cfg)
+    st = p.run(state, warmup, threads=threads) if warmup else state
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (time.perf_counter() - t0) < seconds:
+        st = p.run(st, 1, threads=threads)
+        n += 1
+    dt = time.perf_counter() - t0
+    return n, dt, threads
+
+
+def main():
+    args = parse_args()
+    cfg, state, desc = workload(args.workload)
+    W, H, C = cfg["width"], cfg["height"], cfg["channels"]
+    cells = W * H
+    metric = "cell-steps/s"
+
+    if args.impl == "reference":
+        dist = dist_init()
+        if RANK != 0:
+            return
+        budget = 60.0
+        n, dt, threads = cpu_reference_run(cfg, state, budget, max(args.steps, 1), warmup=min(args.warmup, 2))
+        v = cells * n / dt
+        line = {"metric": metric, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": n,
+                "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, 0x5EED)",
+                "config": dict(desc, parallelism="host threads"), "impl": "reference",
+                "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                                 "sample": f"{n} of {args.steps} requested steps (time-bounded at {budget:.0f} s) "
+                                           "of the same workload; C restatement of CpuPropagator, f32"},
+                "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import autoverse_b200 as fl
+    from autoverse_b200 import _native as nat
+    dist = dist_init()
+    dev = nat.device_info()
+    p = fl.CudaPropagator(cfg)
+    mode = {fl.CONV_DIRECT: "direct", fl.CONV_FFT: "fft"}[p.conv_mode]
+    p.write_state(state)
+    flush = not args.no_flush
+    # warm-up (untimed)
+    p.profile_run(max(args.warmup, 3), flush_l2=flush)
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(dev["pci_bus_id"]) if RANK == 0 else None
+    if sampler:
+        sampler.start()
+    prof = p.profile_run(args.steps, flush_l2=flush)
+    clocks = sampler.stop() if sampler else None
+    p.synchronize()
+    t_local = prof["step_ms"] / 1e3
+    t = reduce_max(dist, t_local)
+    value = WORLD * cells * args.steps / t
+    stages = prof["stages"]
+    dom = max(stages, key=stages.get)
+    dom_ms = stages[dom] / args.steps
+    dom_bytes = stage_bytes(cfg, dom)
+    peak, peak_kind = hbm_peak()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_bytes else None
+    traffic = None
+    prof_json = os.path.join(ROOT, "profiles", f"{dom}_{args.workload}.json")
+    if os.path.exists(prof_json):
+        with open(prof_json) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    # end to end through the public API with pinned host buffers
+    pin_in = fl.propagator.PinnedBuffer(state.shape)
+    pin_out = fl.propagator.PinnedBuffer(state.shape)
+    pin_in.array[...] = state
+    lib = nat.lib()
+    for _ in range(3):
+        p.write_state(pin_in.array)
+        p.run_device(1)
+        nat.check(lib.flp_read_state(p._h, pin_out.array.ctypes.data, pin_out.array.size, None, None))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        p.write_state(pin_in.array)
+        p.run_device(1)
+        nat.check(lib.flp_read_state(p._h, pin_out.array.ctypes.data, pin_out.array.size, None, None))
+        pin_in.array[...] = pin_out.array
+    e2e_t = reduce_max(dist, time.perf_counter() - t0)
+    e2e_value = WORLD * cells * args.e2e_steps / e2e_t
+
+    cpu = None
+    if RANK == 0 and WORLD == 1:
+        n, dt, threads = cpu_reference_run(cfg, state, args.cpu_seconds, 200)
+        cpu = {"value": cells * n / dt, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{n} steps of the same workload (time-bounded at {args.cpu_seconds:.0f} s, 1 warm-up), "
+                         "C restatement of CpuPropagator in f32, OpenMP over kernels/channels"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if RANK != 0:
+        return
+    line = {
+        "metric": metric, "value": value, "unit": "cell-steps/s", "n_gpus": WORLD, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, 0x5EED)",
+        "config": dict(desc, conv_path=mode, parallelism=("replicas x%d" % WORLD) if WORLD > 1 else "single GPU",
+                       l2="flushed before every timed step" if flush else "warm"),
+        "cell_channel_steps_per_s": value * C,
+        "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s", "algorithmic_bytes_per_launch": dom_bytes},
+        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(state.nbytes),
+                "d2h_bytes_per_step": int(state.nbytes), "steps": args.e2e_steps},
+        "gpu_launches": prof["launches_per_step"] * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/*
+ * flowlenia_cuda.h — C ABI of the B200 Flow Lenia step engine.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status
+ * (FLP_OK == 0, negative on failure) and never aborts the process; the text of
+ * the last failure on the calling thread is available from flp_last_error().
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * within the nathan-gage/autoverse crate).  Configs and seeds are the
+ * reference's unchanged JSON schema (src/schema/config.rs:14-111,
+ * src/schema/seed.rs:13-135).
+ *
+ * State layout on both sides of the boundary is the reference's
+ * SimulationState layout: channel-major planes, each plane z*H*W + y*W + x
+ * (src/compute/propagator.rs:18-21), f32.
+ *
+ * Threading: one handle per host thread.  All device work of a handle runs on
+ * one CUDA stream owned by the handle; calls on different handles may run
+ * concurrently.
+ */
+#ifndef FLOWLENIA_CUDA_H
+#define FLOWLENIA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FLP_API __attribute__((visibility("default")))
+#else
+#define FLP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLP_OK 0
+#define FLP_ERR_INVALID_CONFIG -1 /* config.rs:136-164 ConfigError, or bad JSON */
+#define FLP_ERR_INVALID_ARGUMENT -2
+#define FLP_ERR_OOM -3
+#define FLP_ERR_CUDA -4
+#define FLP_ERR_TIMEOUT -5   /* a bounded device wait gave up */
+#define FLP_ERR_NONFINITE -6 /* NaN/Inf found in the state */
+#define FLP_ERR_UNSUPPORTED -7
+
+/* Convolution strategy (the reference always uses FFT, src/compute/fft.rs). */
+#define FLP_CONV_AUTO 0   /* measured choice, cached per (grid, radius, channels) */
+#define FLP_CONV_DIRECT 1 /* shared-memory tiled torus convolution */
+#define FLP_CONV_FFT 2    /* batched real-to-complex Stockham FFT */
+
+typedef struct flp_propagator flp_propagator;
+
+typedef struct {
+    int32_t width, height, depth, channels, n_kernels;
+    int32_t conv_mode;      /* FLP_CONV_DIRECT or FLP_CONV_FFT once resolved */
+    float time;             /* SimulationState.time, propagator.rs:28-29 */
+    uint64_t step;          /* SimulationState.step, propagator.rs:30-31 */
+} flp_info;
+
+/* Text of the last error raised on this thread ("" if none). */
+FLP_API const char* flp_last_error(void);
+
+/* CudaPropagator::new — replaces CpuPropagator::new (src/compute/propagator.rs:157-236)
+ * and CpuPropagator3D::new (src/compute/propagator3d.rs:49-116).  Validates like
+ * SimulationConfig::validate (src/schema/config.rs:136-164) and returns
+ * FLP_ERR_INVALID_CONFIG instead of panicking.  The state starts all zero. */
+FLP_API int flp_create(const char* config_json, flp_propagator** out);
+
+/* Drop. */
+FLP_API int flp_destroy(flp_propagator* h);
+
+/* SimulationState::from_seed (src/compute/propagator.rs:36-59, seed generation
+ * src/schema/seed.rs:160-304): generate on the host and upload; time=0, step=0. */
+FLP_API int flp_state_from_seed(flp_propagator* h, const char* seed_json);
+
+/* Seed::generate without a propagator: fills out[channels*depth*height*width]. */
+FLP_API int flp_seed_generate(const char* config_json, const char* seed_json, float* out, size_t n);
+
+/* Replace the device state with a caller-owned host buffer (copied in). */
+FLP_API int flp_write_state(flp_propagator* h, const float* state, size_t n, float time, uint64_t step);
+
+/* Copy the device state out to a caller-owned host buffer; time/step may be NULL. */
+FLP_API int flp_read_state(flp_propagator* h, float* out, size_t n, float* time, uint64_t* step);
+
+/* CpuPropagator::step (src/compute/propagator.rs:239-420) and
+ * CpuPropagator3D::step (src/compute/propagator3d.rs:119-308).  Asynchronous:
+ * enqueues on the handle's stream. */
+FLP_API int flp_step(flp_propagator* h);
+
+/* CpuPropagator::run (src/compute/propagator.rs:423-427): n steps, replayed
+ * from a captured CUDA graph.  Asynchronous. */
+FLP_API int flp_run(flp_propagator* h, uint64_t n);
+
+/* Wait for the handle's stream; reports device-side status words
+ * (FLP_ERR_NONFINITE when the bound check saw a non-finite mass). */
+FLP_API int flp_synchronize(flp_propagator* h);
+
+/* SimulationState::total_mass (src/compute/propagator.rs:80-82) computed on
+ * the device as an FP64 compensated (Neumaier) sum over all channels. */
+FLP_API int flp_total_mass(flp_propagator* h, double* out);
+
+/* The reference's own f32 total_mass: sequential f32 sums per channel, then
+ * summed over channels (src/compute/reintegration.rs:221-228). */
+FLP_API int flp_total_mass_f32(flp_propagator* h, float* out);
+
+FLP_API int flp_get_info(flp_propagator* h, flp_info* out);
+
+/* Force a convolution strategy (FLP_CONV_*); FLP_CONV_AUTO re-runs the tuner. */
+FLP_API int flp_set_conv_mode(flp_propagator* h, int mode);
+
+/* The handle's cudaStream_t, for callers that time or order work around it. */
+FLP_API void* flp_stream(flp_propagator* h);
+
+/* Device pointer of the current state (channels*N floats) for zero-copy
+ * callers; valid until the next step/run/write. */
+FLP_API const float* flp_device_state(flp_propagator* h);
+
+/* Current device's PCI bus id (for matching nvidia-smi samples), SM count and
+ * L2 size. */
+FLP_API int flp_device_info(char* pci_bus_id, int len, int* sm_count, size_t* l2_bytes);
+
+/* Pinned (page-locked) host buffers for callers that stream states to and
+ * from the device every step; flp_write_state/flp_read_state copy from and to
+ * them at full PCIe/C2C bandwidth. */
+FLP_API int flp_host_alloc(size_t bytes, void** out);
+FLP_API int flp_host_free(void* p);
+
+/* Measurement entry point: runs `steps` steps eagerly, each optionally
+ * preceded by a write of a buffer twice the size of L2 (so every step starts
+ * with a cold cache), with CUDA events on the handle's stream around every
+ * kernel.  Writes the summed device time of each stage (ms) to stage_ms[i]
+ * (up to max_stages entries), the stage names (comma-separated) to names,
+ * the number of stages to n_stages and the summed step time to step_ms.
+ * Synchronous. */
+FLP_API int flp_profile_run(flp_propagator* h, int steps, int flush_l2, float* stage_ms, int max_stages,
+                            int* n_stages, char* names, size_t names_len, float* step_ms);
+
+/* Stage entry points used by stage-level parity tests.
+ * Affinity U = sum_k w_k G(K_k * A_src) (src/compute/propagator.rs:244-279):
+ * reads the current state, writes channels*N floats to the host buffer. */
+FLP_API int flp_debug_affinity(flp_propagator* h, float* aff_out, size_t n);
+
+/* Transport stage (propagator.rs:304-419) from a host state and host affinity:
+ * mass sum, Sobel, flow, reintegration.  Writes the next state to out. */
+FLP_API int flp_debug_transport(flp_propagator* h, const float* state, const float* aff, float* out, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLOWLENIA_CUDA_H */
