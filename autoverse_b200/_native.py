@@ -10,7 +10,7 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libflowlenia_cuda.so")
+LIB_PATH = os.environ.get("FLOWLENIA_LIB") or os.path.join(HERE, "_lib", "libflowlenia_cuda.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "flowlenia_cuda.h")
 
 FLP_OK = 0

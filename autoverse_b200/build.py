@@ -20,6 +20,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(HERE, "_lib")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libflowlenia_cuda.so")
+EXTRA = os.environ.get("FLP_NVCC_EXTRA", "").split()
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
@@ -36,17 +37,18 @@ def _newest_header() -> float:
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    os.makedirs(LIBDIR, exist_ok=True)
-    os.makedirs(OBJDIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False, lib: str = LIB,
+          objdir: str = OBJDIR) -> str:
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
+    os.makedirs(objdir, exist_ok=True)
     hdr = _newest_header()
     objs = []
     for src in sources():
-        obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
         if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr):
             continue
-        cmd = [NVCC, *ARCH, *COMMON, "-c", src, "-o", obj]
+        cmd = [NVCC, *ARCH, *COMMON, *EXTRA, "-c", src, "-o", obj]
         if src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if ptxas_verbose else []
         else:
@@ -54,12 +56,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    if force or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -31,6 +31,7 @@ struct FlowParams {
     float inv_area;     // exact reciprocal when total_area is a power of two
     float beta_a, nexp;
     float ubound;       // max over channels of sum_k |w_k| for kernels targeting the channel
+    float pos_eps;      // absolute margin (cells) for rounding of positions in the gather window
     int area_pow2;      // 1 when the division by total_area is a multiplication
     int point_mode;     // total_area < 1e-10: nearest-cell deposit
 };
@@ -58,6 +59,23 @@ __host__ __device__ inline float ordered_to_float(int i) {
 }
 
 __device__ __forceinline__ int wrap_coord(int c, int size) { return ((c % size) + size) % size; }
+
+// Wrap for coordinates a few sides off the torus: conditional add/subtract
+// (no integer division); the loops run at most a handful of times even for
+// grids narrower than a tile.
+__device__ __forceinline__ int wrap_near(int c, int size) {
+    while (c < 0) c += size;
+    while (c >= size) c -= size;
+    return c;
+}
+
+// Flow-bound slots: C pairs (max, min) of ordered ints, reset to (-inf, +inf).
+__device__ __forceinline__ void reset_bound_slots(int* slot, int C) {
+    for (int c = 0; c < C; ++c) {
+        slot[2 * c] = float_to_ordered(-INFINITY);
+        slot[2 * c + 1] = float_to_ordered(INFINITY);
+    }
+}
 
 // alpha = clamp((A/beta)^n, 0, 1) with the reference's integer-n fast paths
 // (src/compute/flow.rs:14-32).  Division is IEEE (nvcc default prec-div).

@@ -103,7 +103,7 @@ struct flp_propagator {
     int rmax = 0;
     bool direct_ok = false;
     FlowParams fp{};
-    int* d_bound = nullptr;  // 2 slots x (max, min) as ordered ints
+    int* d_bound = nullptr;  // 2 state buffers x C channels x (max, min) as ordered ints
     int* d_status = nullptr;
     double2* d_partial = nullptr;
     double* d_mass = nullptr;
@@ -139,7 +139,7 @@ struct flp_propagator {
     void enqueue_conv(const float* a, int* reset_slot) {
         if (K == 0) {
             // No kernels: the affinity stays zero (it is cleared at creation).
-            launch_bound_reset(reset_slot, st);
+            launch_bound_reset(reset_slot, C, st);
             mark(0);
             return;
         }
@@ -147,7 +147,7 @@ struct flp_propagator {
             launch_conv_direct_2d(a, U, d_kd, K, d_taps, W, H, C, rmax, reset_slot, st);
             mark(0);
         } else {
-            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, reset_slot, st);
+            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, reset_slot, C, st);
             mark(0);
             launch_fft_cols(d_S, d_KH, d_T, d_slot, K, W, H, geom, 0, 1.f, st);
             mark(1);
@@ -165,8 +165,8 @@ struct flp_propagator {
     void enqueue_step() {
         const float* a = A[cur];
         float* an = A[cur ^ 1];
-        int* bin = d_bound + 2 * cur;
-        int* bout = d_bound + 2 * (cur ^ 1);
+        int* bin = d_bound + 2 * C * cur;
+        int* bout = d_bound + 2 * C * (cur ^ 1);
         enqueue_conv(a, bout);
         launch_transport_2d(a, U, an, C, W, H, fp, bin, bout, d_status, st);
         mark(int(stage_names().size()) - 1);
@@ -277,7 +277,7 @@ static void setup_fft(flp_propagator* h, const std::vector<KernelStencil>& ks) {
     float* d_pad = dalloc<float>(padded.size());
     float2* d_tmp = dalloc<float2>(spec * h->K);
     CK(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
-    launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, H, g, nullptr, h->st);
+    launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, H, g, nullptr, 0, h->st);
     launch_fft_cols(d_tmp, nullptr, h->d_KH, nullptr, h->K, W, H, g, 1, float(1.0 / (double(W) * double(H))), h->st);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
@@ -346,6 +346,10 @@ static FlowParams make_flow_params(const SimulationConfig& cfg) {
     for (const auto& k : cfg.kernels) wsum[k.target_channel] += std::fabs(k.weight);
     fp.ubound = 0.f;
     for (float w : wsum) fp.ubound = std::max(fp.ubound, w);
+    // dest = x + dt*F and x_min/x_max are rounded at the scale of the largest
+    // coordinate; allow a few ulps of it plus a fixed slack.
+    const float maxside = float(std::max(std::max(cfg.width, cfg.height), cfg.depth));
+    fp.pos_eps = 8.0f * maxside * 1.1920929e-07f + 1e-4f;
     return fp;
 }
 
@@ -367,7 +371,7 @@ static void create(const std::string& json, flp_propagator* h) {
     CK(cudaMemsetAsync(h->A[0], 0, CN * sizeof(float), h->st));
     CK(cudaMemsetAsync(h->A[1], 0, CN * sizeof(float), h->st));
     CK(cudaMemsetAsync(h->U, 0, CN * sizeof(float), h->st));
-    h->d_bound = dalloc<int>(4);
+    h->d_bound = dalloc<int>(4 * size_t(h->C));
     h->d_status = dalloc<int>(1);
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
     h->np = 256;
@@ -402,7 +406,7 @@ static void upload_state(flp_propagator* h, const float* src, size_t n) {
     const size_t CN = size_t(h->C) * h->N;
     if (n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "state size mismatch: expected " + std::to_string(CN));
     CK(cudaMemcpyAsync(h->A[h->cur], src, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
-    launch_bound_init(h->A[h->cur], h->C, h->N, h->d_bound + 2 * h->cur, h->st);
+    launch_bound_init(h->A[h->cur], h->C, h->N, h->d_bound + 2 * h->C * h->cur, h->st);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
 }
@@ -742,13 +746,13 @@ int flp_debug_transport(flp_propagator* h, const float* state, const float* aff,
         float* a = dalloc<float>(CN);
         float* u = dalloc<float>(CN);
         float* o = dalloc<float>(CN);
-        int* slots = dalloc<int>(4);
+        int* slots = dalloc<int>(4 * size_t(h->C));
         try {
             CK(cudaMemcpyAsync(a, state, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
             CK(cudaMemcpyAsync(u, aff, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
             launch_bound_init(a, h->C, h->N, slots, h->st);
-            launch_bound_reset(slots + 2, h->st);
-            launch_transport_2d(a, u, o, h->C, h->W, h->H, h->fp, slots, slots + 2, h->d_status, h->st);
+            launch_bound_reset(slots + 2 * h->C, h->C, h->st);
+            launch_transport_2d(a, u, o, h->C, h->W, h->H, h->fp, slots, slots + 2 * h->C, h->d_status, h->st);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(out, o, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
             CK(cudaStreamSynchronize(h->st));

@@ -132,7 +132,7 @@ __device__ void load_twiddles(float2* dst, const float2* __restrict__ src, int n
 __global__ void __launch_bounds__(256) fft_rows_r2c(const float* __restrict__ A, float2* __restrict__ S,
                                                     const int* __restrict__ srcs, int W, int H, int NR, FftPlan pm,
                                                     const float2* __restrict__ twM_g, const float2* __restrict__ twW_g,
-                                                    int* reset_slot) {
+                                                    int* reset_slot, int nreset) {
     extern __shared__ float2 fsm[];
     const int M = W / 2, Wc = M + 1;
     float2* twM = fsm;
@@ -140,10 +140,7 @@ __global__ void __launch_bounds__(256) fft_rows_r2c(const float* __restrict__ A,
     float2* a = twW + Wc;
     float2* b = a + NR * Wc;
     const int tid = threadIdx.x;
-    if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
-        reset_slot[0] = float_to_ordered(-INFINITY);
-        reset_slot[1] = float_to_ordered(INFINITY);
-    }
+    if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) reset_bound_slots(reset_slot, nreset);
     const int y0 = blockIdx.x * NR;
     const int slot = blockIdx.y;
     const int c = srcs ? srcs[slot] : slot;
@@ -290,13 +287,16 @@ void fft2d_set_attributes(size_t max_bytes) {
     cudaFuncSetAttribute(fft_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, int(max_bytes));
     cudaFuncSetAttribute(fft_cols_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(max_bytes));
     cudaFuncSetAttribute(fft_rows_c2r_growth, cudaFuncAttributeMaxDynamicSharedMemorySize, int(max_bytes));
+    cudaFuncSetAttribute(fft_rows_r2c, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(fft_cols_conv, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(fft_rows_c2r_growth, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
-                    int* reset_slot, cudaStream_t st) {
+                    int* reset_slot, int nreset, cudaStream_t st) {
     dim3 grid((H + g.NR - 1) / g.NR, nsrc);
     fft_rows_r2c<<<grid, 256, fft_rows_smem(W, g.NR, false), st>>>(A, S, srcs, W, H, g.NR, g.pm, g.twM, g.twW,
-                                                                    reset_slot);
+                                                                    reset_slot, nreset);
 }
 
 void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,

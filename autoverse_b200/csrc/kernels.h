@@ -39,7 +39,7 @@ void transport_2d_set_attributes();
 void launch_transport_2d(const float* A, const float* U, float* Anext, int C, int W, int H, const FlowParams& fp,
                          const int* bound_in, int* bound_out, int* status, cudaStream_t st);
 void launch_bound_init(const float* A, int C, size_t N, int* slot, cudaStream_t st);
-void launch_bound_reset(int* slot, cudaStream_t st);
+void launch_bound_reset(int* slot, int C, cudaStream_t st);
 
 // FP64 compensated mass
 void launch_mass_fp64(const float* A, size_t n, double2* partial, int np, double* out, cudaStream_t st);
@@ -49,7 +49,7 @@ size_t fft_rows_smem(int W, int NR, bool with_u);
 size_t fft_cols_smem(int H, int NC);
 void fft2d_set_attributes(size_t max_bytes);
 void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
-                    int* reset_slot, cudaStream_t st);
+                    int* reset_slot, int nreset, cudaStream_t st);
 void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
                      const FftGeom& g, int mode, float scale, cudaStream_t st);
 void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,

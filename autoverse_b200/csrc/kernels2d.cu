@@ -32,17 +32,15 @@ constexpr int CD_TW = 32, CD_TH = 32;
 __global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __restrict__ A, float* __restrict__ U,
                                                              const KDesc* __restrict__ kd, int K,
                                                              const float* __restrict__ taps, int W, int H, int rmax,
-                                                             int* reset_slot) {
+                                                             int* reset_slot, int nreset) {
     extern __shared__ float sm[];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * 32 + tx;
     const int c = blockIdx.z;
     const int x0 = blockIdx.x * CD_TW, y0 = blockIdx.y * CD_TH;
     const size_t N = size_t(W) * H;
-    if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
-        reset_slot[0] = float_to_ordered(-INFINITY);
-        reset_slot[1] = float_to_ordered(INFINITY);
-    }
+    if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0)
+        reset_bound_slots(reset_slot, nreset);
     const int Pmax = CD_TW + 2 * rmax;
     float* tile = sm;                                   // (CD_TH + 2r) x (CD_TW + 2r)
     float* tsm = sm + size_t(CD_TH + 2 * rmax) * Pmax;  // taps
@@ -102,30 +100,37 @@ void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, con
                            int rmax, int* reset_slot, cudaStream_t st) {
     dim3 grid((W + CD_TW - 1) / CD_TW, (H + CD_TH - 1) / CD_TH, C);
     size_t smem = conv_direct_smem_bytes(rmax);
-    conv_direct_growth_2d<<<grid, dim3(32, 8), smem, st>>>(A, U, kd, K, taps, W, H, rmax, reset_slot);
+    conv_direct_growth_2d<<<grid, dim3(32, 8), smem, st>>>(A, U, kd, K, taps, W, H, rmax, reset_slot, C);
 }
 
 // ---------------------------------------------------------------------------
-// Gather radius from the flow bound.
+// Gather window from the flow bound.
 // |F_x|,|F_y| <= max(max|grad U|, max|grad A_sum|) since F = (1-a)gU - a gA
 // with a in [0,1]; the Sobel/8 of a field ranges over at most half its spread,
-// |U| <= sum_k |w_k| (G in [-1,1]) and A_sum spans [amin, amax].  A source
-// at x can deposit only into cells ix with |ix - x| < dt|F| + s + 1.
+// |U| <= sum_k |w_k| (G in [-1,1]) and the spread of A_sum is at most
+// sum_c (max A_c - min A_c).  With |dest - x| <= D, a source at x overlaps
+// cell ix only if x - ix lies in (-(D+s), D+s+1) (reintegration.rs:105-146),
+// so sources x = ix + k with k in [-RN, RN+1], RN = ceil(D+s) - 1, cover every
+// deposit.  D carries a margin for the rounding of dest and x_min/x_max.
+// bound: C pairs (max, min) as ordered ints.  Returns RN.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int gather_radius(const int* bound, const FlowParams& fp, int maxside, int* status) {
-    float amax = ordered_to_float(bound[0]);
-    float amin = ordered_to_float(bound[1]);
-    float spread = amax - amin;
+__device__ __forceinline__ int gather_window(const int* bound, int C, const FlowParams& fp, int maxside, int* status) {
+    float hi = 0.f, lo = 0.f;
+    for (int c = 0; c < C; ++c) {
+        hi += ordered_to_float(bound[2 * c]);
+        lo += ordered_to_float(bound[2 * c + 1]);
+    }
+    float spread = (hi - lo) * 1.0001f;
     if (!(spread >= 0.f) || !isfinite(spread)) {
         if (status && threadIdx.x == 0 && threadIdx.y == 0) atomicOr(status, STATUS_NONFINITE);
-        return 1;
+        return 0;
     }
     float fb = fmaxf(fp.ubound, 0.5f * spread);
-    float Db = fp.dt * fb * 1.0001f + 1e-5f;
-    float rr = floorf(Db + fp.s + 1.0f);
+    float Db = fp.dt * fb * 1.0001f + fp.pos_eps;
+    float rn = ceilf(Db + fp.s) - 1.0f;
     int cap = 2 * maxside + 2;
-    if (!(rr < float(cap))) return cap;
-    return rr < 1.f ? 1 : int(rr);
+    if (!(rn < float(cap))) return cap;
+    return rn < 0.f ? 0 : int(rn);
 }
 
 // Rotated offset order: visits offsets k in [-R, R] so that the wrapped
@@ -226,20 +231,44 @@ __device__ float gather_generic_2d(const float* __restrict__ A, const float* __r
 }
 
 // ---------------------------------------------------------------------------
-// Fused transport: tile 64x32 destinations, 256 threads; thread (tx, ty)
-// owns the 4-cell row strips at (x0+4tx.., y0+ty) and (x0+4tx.., y0+ty+16).
-// Source region = tile + TP cells each side (TP = widest fast-path radius).
+// Fused transport.  Block = (64x16 tile, one channel), 256 threads; thread
+// (tx, ty) owns the 4-cell row strip x0+4tx.., y0+ty.  The source region is
+// the tile plus R rows above/below and TP(=4) columns left/right (columns
+// padded to keep float4 alignment); the Sobel inputs add a 1-cell ring.
+// Per source the kernel stores its square's bounds x_min, x_max, y_min, y_max
+// (reintegration.rs:105-108) and its mass; destinations then gather.
 // ---------------------------------------------------------------------------
-constexpr int TT_W = 64, TT_H = 32, TP = 4;
-constexpr int SR_W = TT_W + 2 * TP, SR_H = TT_H + 2 * TP;  // 72 x 40 sources
-constexpr int AR_W = SR_W + 2, AR_H = SR_H + 2;            // 74 x 42 with the Sobel ring
+#ifndef TRANSPORT_MIN_BLOCKS
+#define TRANSPORT_MIN_BLOCKS 2
+#endif
+// Fused transport.  Block = (64x16 tile, one channel), 256 threads; thread
+// (tx, ty) owns the 4-cell row strip x0+4tx.., y0+ty.  Sources are the cells
+// y0-RN .. y0+15+RN+1 by x0-TP .. x0+63+TP (columns padded to keep float4
+// alignment); the Sobel inputs add a 1-cell ring.  Per source the block
+// stores its square's bounds x_min, x_max, y_min, y_max
+// (reintegration.rs:105-108) and its mass; destinations then gather.
+constexpr int TT_W = 64, TT_H = 16, TP = 4, RN_MAX = 3;
+constexpr int SR_W = TT_W + 2 * TP;              // 72 source columns
+constexpr int SR_HMAX = TT_H + 2 * RN_MAX + 1;   // up to 23 source rows
+constexpr int AR_W = SR_W + 2;                   // 74 with the Sobel ring
+constexpr int AR_HMAX = SR_HMAX + 2;             // up to 25
+constexpr int SRC_CHUNK = 8;                     // sources per thread in the sliding Sobel
 
-size_t transport_smem_bytes() { return sizeof(float) * (2 * AR_W * AR_H + 3 * SR_W * SR_H); }
+// Region arrays are padded to a multiple of 4 floats so that every array,
+// and hence every float4 chunk of the source arrays, is 16-byte aligned.
+__host__ __device__ constexpr int region_floats(int arh) { return ((AR_W * arh + 3) / 4) * 4; }
+static_assert(SR_W % 4 == 0, "source rows must stay 16-byte aligned");
+
+size_t transport_smem_bytes() { return sizeof(float) * (3 * region_floats(AR_HMAX) + 5 * SR_W * SR_HMAX); }
 
 __device__ __forceinline__ int wrap_pass(int g, int size) { return g >= size ? 0 : (g < 0 ? 2 : 1); }
 
-__device__ __forceinline__ void block_minmax_atomic(float vmax, float vmin, int* slot) {
-    __shared__ float red_max[8], red_min[8];
+// Block max/min into an ordered-int slot pair.  A non-finite value anywhere
+// in the block publishes +inf as the max, so the next gather_window sees a
+// non-finite spread and raises STATUS_NONFINITE.
+__device__ __forceinline__ void block_minmax_atomic(float vmax, float vmin, bool bad, int* slot) {
+    __shared__ float red_max[32], red_min[32];
+    const int anybad = __syncthreads_or(bad ? 1 : 0);
     for (int o = 16; o > 0; o >>= 1) {
         vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
         vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
@@ -252,187 +281,247 @@ __device__ __forceinline__ void block_minmax_atomic(float vmax, float vmin, int*
         int nw = (blockDim.x * blockDim.y) >> 5;
         float mx = red_max[0], mn = red_min[0];
         for (int w = 1; w < nw; ++w) { mx = fmaxf(mx, red_max[w]); mn = fminf(mn, red_min[w]); }
-        // NaN propagates into the slot as a non-finite spread the next step detects.
-        if (mx != mx || mn != mn) { mx = NAN; mn = NAN; }
+        if (anybad) mx = INFINITY;
         atomicMax(slot + 0, float_to_ordered(mx));
         atomicMin(slot + 1, float_to_ordered(mn));
     }
 }
 
-template <bool POW2>
-__global__ void __launch_bounds__(256) transport_2d(const float* __restrict__ A, const float* __restrict__ U,
-                                                    float* __restrict__ Anext, int C, int W, int H, FlowParams fp,
-                                                    const int* __restrict__ bound_in, int* bound_out, int* status) {
-    extern __shared__ float sm[];
-    float* asum = sm;                   // AR_H x AR_W
-    float* usm = asum + AR_W * AR_H;    // AR_H x AR_W
-    float* dxs = usm + AR_W * AR_H;     // SR_H x SR_W
-    float* dys = dxs + SR_W * SR_H;
-    float* mss = dys + SR_W * SR_H;
-
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TT_W, y0 = blockIdx.y * TT_H;
-    const size_t N = size_t(W) * H;
-    const int R = gather_radius(bound_in, fp, max(W, H), status);
-
-    float nsum[2][4];
+// One source row of the gather for the thread's 4 destinations X0..X0+3.
+// Source column j of the strip window is x0-TP+4tx+j; its offset from
+// destination i is kx = j - TP - i, kept in [-RN, RN+1] at compile time.
+// Sources are streamed one float4 chunk (4 columns) at a time.  CHECK adds
+// the wrap-pass predicate for tiles whose source columns wrap the torus.
+template <int RN, bool POW2, bool CHECK>
+__device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, const float* __restrict__ rxmax,
+                                           const float* __restrict__ rymin, const float* __restrict__ rymax,
+                                           const float* __restrict__ rm, float cy0, float cy1, int X0, int gx_base,
+                                           int W, int cp, float inv_or_total, float (&acc)[4]) {
+    constexpr int JLO = TP - RN, JHI = TP + 3 + RN + 1;
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+    for (int q = 0; q < 3; ++q) {
+        if (4 * q + 3 < JLO || 4 * q > JHI) continue;
+        const float4 vxa = *reinterpret_cast<const float4*>(rxmin + 4 * q);
+        const float4 vxb = *reinterpret_cast<const float4*>(rxmax + 4 * q);
+        const float4 vya = *reinterpret_cast<const float4*>(rymin + 4 * q);
+        const float4 vyb = *reinterpret_cast<const float4*>(rymax + 4 * q);
+        const float4 vm = *reinterpret_cast<const float4*>(rm + 4 * q);
+        const float xa[4] = {vxa.x, vxa.y, vxa.z, vxa.w}, xb[4] = {vxb.x, vxb.y, vxb.z, vxb.w};
+        const float ya[4] = {vya.x, vya.y, vya.z, vya.w}, yb[4] = {vyb.x, vyb.y, vyb.z, vyb.w};
+        const float mm[4] = {vm.x, vm.y, vm.z, vm.w};
 #pragma unroll
-        for (int i = 0; i < 4; ++i) nsum[h][i] = 0.f;
-
-    const bool fast = R <= TP && 2 * R + 1 <= W && 2 * R + 1 <= H && !fp.point_mode;
-    if (!fast) {
-        for (int c = 0; c < C; ++c)
-            for (int h = 0; h < 2; ++h) {
-                int Y = y0 + ty + 16 * h;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    int X = x0 + 4 * tx + i;
-                    if (X < W && Y < H) {
-                        float v = gather_generic_2d(A, U, c, C, W, H, X, Y, R, fp);
-                        Anext[size_t(c) * N + size_t(Y) * W + X] = v;
-                        nsum[h][i] = __fadd_rn(nsum[h][i], v);
-                    }
-                }
+        for (int jj = 0; jj < 4; ++jj) {
+            const int j = 4 * q + jj;
+            if (j < JLO || j > JHI) continue;
+            int xsh = 0;
+            if (CHECK) {
+                const int gx = gx_base + j;
+                if (wrap_pass(gx, W) != cp) continue;
+                xsh = gx < 0 ? W : (gx >= W ? -W : 0);
             }
-    } else {
-        // Channel sum over the source region plus the Sobel ring.
-        for (int i = tid; i < AR_W * AR_H; i += 256) {
-            int ly = i / AR_W, lx = i - ly * AR_W;
-            int gy = wrap_coord(y0 - TP - 1 + ly, H), gx = wrap_coord(x0 - TP - 1 + lx, W);
-            size_t idx = size_t(gy) * W + gx;
-            float s = 0.f;
-            for (int c = 0; c < C; ++c) s = __fadd_rn(s, A[size_t(c) * N + idx]);
-            asum[i] = s;
-        }
-        // Which wrap passes occur for this tile (block-uniform).
-        const int rp_lo = (y0 + TT_H - 1 + R >= H) ? 0 : 1, rp_hi = (y0 - R < 0) ? 2 : 1;
-        const int cp_lo = (x0 + TT_W - 1 + R >= W) ? 0 : 1, cp_hi = (x0 - R < 0) ? 2 : 1;
-        const float s = fp.s;
-
-        for (int c = 0; c < C; ++c) {
-            const float* Ac = A + size_t(c) * N;
-            const float* Uc = U + size_t(c) * N;
-            __syncthreads();
-            for (int i = tid; i < AR_W * AR_H; i += 256) {
-                int ly = i / AR_W, lx = i - ly * AR_W;
-                int gy = wrap_coord(y0 - TP - 1 + ly, H), gx = wrap_coord(x0 - TP - 1 + lx, W);
-                usm[i] = Uc[size_t(gy) * W + gx];
-            }
-            __syncthreads();
-            // Per-source destination (reintegration.rs:81-82) and mass.
-            for (int i = tid; i < SR_W * SR_H; i += 256) {
-                int sy = i / SR_W, sx = i - sy * SR_W;
-                int yw = wrap_coord(y0 - TP + sy, H), xw = wrap_coord(x0 - TP + sx, W);
-                float mass = Ac[size_t(yw) * W + xw];
-                if (fabsf(mass) < 1e-10f) mass = 0.f;
-                const float* a = asum + sy * AR_W + sx;  // top-left of the 3x3 window
-                const float* u = usm + sy * AR_W + sx;
-                float gax, gay, gux, guy;
-                sobel2(a[0], a[1], a[2], a[AR_W], a[AR_W + 2], a[2 * AR_W], a[2 * AR_W + 1], a[2 * AR_W + 2], gax, gay);
-                sobel2(u[0], u[1], u[2], u[AR_W], u[AR_W + 2], u[2 * AR_W], u[2 * AR_W + 1], u[2 * AR_W + 2], gux, guy);
-                float alpha = flow_alpha(a[AR_W + 1], fp.beta_a, fp.nexp);
-                float oma = __fsub_rn(1.0f, alpha);
-                float fx = __fsub_rn(__fmul_rn(oma, gux), __fmul_rn(alpha, gax));
-                float fy = __fsub_rn(__fmul_rn(oma, guy), __fmul_rn(alpha, gay));
-                dxs[i] = __fadd_rn(float(xw), __fmul_rn(fp.dt, fx));
-                dys[i] = __fadd_rn(float(yw), __fmul_rn(fp.dt, fy));
-                mss[i] = mass;
-            }
-            __syncthreads();
-            // Gather.
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                const int Y = y0 + ty + 16 * h;
-                const int X0 = x0 + 4 * tx;
-                float acc[4] = {0.f, 0.f, 0.f, 0.f};
-                if (Y < H && X0 < W) {
-#pragma unroll 1
-                    for (int rp = rp_lo; rp <= rp_hi; ++rp) {
-#pragma unroll 1
-                        for (int ky = -R; ky <= R; ++ky) {
-                            const int gy = Y + ky;
-                            if (wrap_pass(gy, H) != rp) continue;
-                            const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
-                            const float cy0 = float(iy), cy1 = float(iy + 1);
-                            const int sr = (Y - y0) + TP + ky;
-                            const float4* rx = reinterpret_cast<const float4*>(dxs + sr * SR_W + 4 * tx);
-                            const float4* ry = reinterpret_cast<const float4*>(dys + sr * SR_W + 4 * tx);
-                            const float4* rm = reinterpret_cast<const float4*>(mss + sr * SR_W + 4 * tx);
-                            float vx[12], vy[12], vm[12];
+            const float m = mm[jj];
+            if (m == 0.f) continue;
+            const float oy0 = fmaxf(cy0, ya[jj]), oy1 = fminf(cy1, yb[jj]);
+            const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
+            if (!(oh > 0.f)) continue;
 #pragma unroll
-                            for (int q = 0; q < 3; ++q) {
-                                float4 a4 = rx[q], b4 = ry[q], m4 = rm[q];
-                                vx[4 * q] = a4.x; vx[4 * q + 1] = a4.y; vx[4 * q + 2] = a4.z; vx[4 * q + 3] = a4.w;
-                                vy[4 * q] = b4.x; vy[4 * q + 1] = b4.y; vy[4 * q + 2] = b4.z; vy[4 * q + 3] = b4.w;
-                                vm[4 * q] = m4.x; vm[4 * q + 1] = m4.y; vm[4 * q + 2] = m4.z; vm[4 * q + 3] = m4.w;
-                            }
-#pragma unroll 1
-                            for (int cp = cp_lo; cp <= cp_hi; ++cp) {
-#pragma unroll
-                                for (int j = 0; j < 12; ++j) {
-                                    const int gx = x0 - TP + 4 * tx + j;
-                                    if (wrap_pass(gx, W) != cp) continue;
-                                    const float m = vm[j];
-                                    if (m == 0.f) continue;
-                                    const float ymin = __fsub_rn(vy[j], s), ymax = __fadd_rn(vy[j], s);
-                                    const float oy0 = fmaxf(cy0, ymin), oy1 = fminf(cy1, ymax);
-                                    const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
-                                    if (!(oh > 0.f)) continue;
-                                    const float xmin = __fsub_rn(vx[j], s), xmax = __fadd_rn(vx[j], s);
-                                    const int xsh = gx < 0 ? W : (gx >= W ? -W : 0);
-#pragma unroll
-                                    for (int i = 0; i < 4; ++i) {
-                                        const int X = X0 + i;
-                                        const int kx = gx - X;
-                                        if (kx < -R || kx > R) continue;
-                                        const int ix = X + xsh;
-                                        const float ox0 = fmaxf(float(ix), xmin), ox1 = fminf(float(ix + 1), xmax);
-                                        const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
-                                        const float area = __fmul_rn(ow, oh);
-                                        if (area > 0.f) {
-                                            const float frac = POW2 ? __fmul_rn(area, fp.inv_area)
-                                                                    : __fdiv_rn(area, fp.total_area);
-                                            acc[i] = __fadd_rn(acc[i], __fmul_rn(m, frac));
-                                        }
-                                    }
-                                }
-                            }
-                        }
-                    }
-                    float* out = Anext + size_t(c) * N + size_t(Y) * W;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        if (X0 + i < W) {
-                            out[X0 + i] = acc[i];
-                            nsum[h][i] = __fadd_rn(nsum[h][i], acc[i]);
-                        }
-                    }
+            for (int i = 0; i < 4; ++i) {
+                if (j - TP - i < -RN || j - TP - i > RN + 1) continue;
+                const int ix = X0 + i + xsh;
+                const float ox0 = fmaxf(float(ix), xa[jj]), ox1 = fminf(float(ix + 1), xb[jj]);
+                const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
+                const float area = __fmul_rn(ow, oh);
+                if (POW2) {
+                    // m holds mass * (1 / total_area), exact for a power-of-two
+                    // area; a zero area adds a signed zero, which leaves acc as is.
+                    acc[i] = __fadd_rn(acc[i], __fmul_rn(m, area));
+                } else if (area > 0.f) {
+                    acc[i] = __fadd_rn(acc[i], __fmul_rn(m, __fdiv_rn(area, inv_or_total)));
                 }
             }
         }
     }
-    // Spread of the next channel sum, for the next step's gather radius.
-    float vmax = -INFINITY, vmin = INFINITY;
+}
+
+template <int RN, bool POW2>
+__device__ void transport_body(float* sm, const float* __restrict__ A, const float* __restrict__ U,
+                               float* __restrict__ Anext, int c, int C, int W, int H, const FlowParams& fp,
+                               float (&out)[4]) {
+    constexpr int SRH = TT_H + 2 * RN + 1, ARH = SRH + 2, AREG = region_floats(ARH);
+    float* asum = sm;                   // ARH x AR_W: channel sum
+    float* usm = asum + AREG;           // ARH x AR_W: U_c
+    float* amc = usm + AREG;            // ARH x AR_W: A_c
+    float* sxmin = amc + AREG;          // SRH x SR_W each (16-byte aligned)
+    float* sxmax = sxmin + SR_W * SRH;
+    float* symin = sxmax + SR_W * SRH;
+    float* symax = symin + SR_W * SRH;
+    float* smass = symax + SR_W * SRH;
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int x0 = blockIdx.x * TT_W, y0 = blockIdx.y * TT_H;
+    const size_t N = size_t(W) * H;
+    const float* Uc = U + size_t(c) * N;
+    const float s = fp.s;
+
+    // channel sum, U_c and A_c over the source region plus the Sobel ring
+    for (int i = tid; i < AR_W * ARH; i += 256) {
+        const int ly = i / AR_W, lx = i - ly * AR_W;
+        const int gy = wrap_near(y0 - RN - 1 + ly, H), gx = wrap_near(x0 - TP - 1 + lx, W);
+        const size_t idx = size_t(gy) * W + gx;
+        float a = 0.f, mine = 0.f;
+        for (int k = 0; k < C; ++k) {
+            const float v = A[size_t(k) * N + idx];
+            a = __fadd_rn(a, v);
+            if (k == c) mine = v;
+        }
+        asum[i] = a;
+        amc[i] = mine;
+        usm[i] = Uc[idx];
+    }
+    __syncthreads();
+    // Per-source square bounds and (scaled) mass.  Each thread walks a column
+    // segment of SRC_CHUNK sources with a 3-row register window of the channel
+    // sum and U_c.
+    {
+        constexpr int COL0 = TP - RN, NCOL = TT_W + 2 * RN + 1;
+        constexpr int NCH = (SRH + SRC_CHUNK - 1) / SRC_CHUNK;
+        for (int item = tid; item < NCOL * NCH; item += 256) {
+            const int col = item % NCOL, ch = item / NCOL;
+            const int sx = COL0 + col, r0 = ch * SRC_CHUNK;
+            const int xw = wrap_near(x0 - TP + sx, W);
+            const float* ap = asum + r0 * AR_W + sx;  // region row r0 = source row r0 - 1
+            const float* up = usm + r0 * AR_W + sx;
+            float a0[3] = {ap[0], ap[1], ap[2]}, a1[3] = {ap[AR_W], ap[AR_W + 1], ap[AR_W + 2]};
+            float u0[3] = {up[0], up[1], up[2]}, u1[3] = {up[AR_W], up[AR_W + 1], up[AR_W + 2]};
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+            for (int r = 0; r < SRC_CHUNK; ++r) {
+                const int sy = r0 + r;
+                if (sy >= SRH) break;
+                const float* ar = ap + (r + 2) * AR_W;
+                const float* ur = up + (r + 2) * AR_W;
+                const float a2[3] = {ar[0], ar[1], ar[2]};
+                const float u2[3] = {ur[0], ur[1], ur[2]};
+                const int yw = wrap_near(y0 - RN + sy, H);
+                float mass = amc[(sy + 1) * AR_W + sx + 1];
+                if (fabsf(mass) < 1e-10f) mass = 0.f;
+                float gax, gay, gux, guy;
+                sobel2(a0[0], a0[1], a0[2], a1[0], a1[2], a2[0], a2[1], a2[2], gax, gay);
+                sobel2(u0[0], u0[1], u0[2], u1[0], u1[2], u2[0], u2[1], u2[2], gux, guy);
+                const float alpha = flow_alpha(a1[1], fp.beta_a, fp.nexp);
+                const float oma = __fsub_rn(1.0f, alpha);
+                const float fx = __fsub_rn(__fmul_rn(oma, gux), __fmul_rn(alpha, gax));
+                const float fy = __fsub_rn(__fmul_rn(oma, guy), __fmul_rn(alpha, gay));
+                const float dx = __fadd_rn(float(xw), __fmul_rn(fp.dt, fx));
+                const float dy = __fadd_rn(float(yw), __fmul_rn(fp.dt, fy));
+                const int o = sy * SR_W + sx;
+                sxmin[o] = __fsub_rn(dx, s);
+                sxmax[o] = __fadd_rn(dx, s);
+                symin[o] = __fsub_rn(dy, s);
+                symax[o] = __fadd_rn(dy, s);
+                smass[o] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            int X = x0 + 4 * tx + i, Y = y0 + ty + 16 * h;
-            if (X < W && Y < H) {
-                float v = nsum[h][i];
-                if (v != v) { vmax = NAN; vmin = NAN; }
-                else { vmax = fmaxf(vmax, v); vmin = fminf(vmin, v); }
+                for (int t = 0; t < 3; ++t) {
+                    a0[t] = a1[t]; a1[t] = a2[t];
+                    u0[t] = u1[t]; u1[t] = u2[t];
+                }
             }
         }
-    if (bound_out) block_minmax_atomic(vmax, vmin, bound_out);
+    }
+    __syncthreads();
+
+    const int Y = y0 + ty, X0 = x0 + 4 * tx;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if (Y < H && X0 < W) {
+        const int rp_lo = (y0 + TT_H + RN >= H) ? 0 : 1, rp_hi = (y0 - RN < 0) ? 2 : 1;
+        const int cp_lo = (x0 + TT_W + RN >= W) ? 0 : 1, cp_hi = (x0 - RN < 0) ? 2 : 1;
+        const bool xin = cp_lo == 1 && cp_hi == 1;
+        const int gx_base = x0 - TP + 4 * tx;
+        const float inv_or_total = POW2 ? fp.inv_area : fp.total_area;
+        for (int rp = rp_lo; rp <= rp_hi; ++rp) {
+#pragma unroll 1
+            for (int ky = -RN; ky <= RN + 1; ++ky) {
+                const int gy = Y + ky;
+                if (wrap_pass(gy, H) != rp) continue;
+                const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
+                const float cy0 = float(iy), cy1 = float(iy + 1);
+                const int off = (ty + RN + ky) * SR_W + 4 * tx;
+                if (xin) {
+                    gather_row<RN, POW2, false>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
+                                                cy0, cy1, X0, gx_base, W, 1, inv_or_total, acc);
+                } else {
+                    for (int cp = cp_lo; cp <= cp_hi; ++cp)
+                        gather_row<RN, POW2, true>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
+                                                   cy0, cy1, X0, gx_base, W, cp, inv_or_total, acc);
+                }
+            }
+        }
+        float* o = Anext + size_t(c) * N + size_t(Y) * W;
+        if (X0 + 3 < W && (W & 3) == 0) {
+            *reinterpret_cast<float4*>(o + X0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (X0 + i < W) o[X0 + i] = acc[i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = acc[i];
+}
+
+template <bool POW2>
+__global__ void __launch_bounds__(256, TRANSPORT_MIN_BLOCKS) transport_2d(const float* __restrict__ A,
+                                                                          const float* __restrict__ U,
+                                                                          float* __restrict__ Anext, int C, int W,
+                                                                          int H, FlowParams fp,
+                                                                          const int* __restrict__ bound_in,
+                                                                          int* bound_out, int* status) {
+    extern __shared__ __align__(16) float sm[];
+    const int c = blockIdx.z;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int x0 = blockIdx.x * TT_W, y0 = blockIdx.y * TT_H;
+    const size_t N = size_t(W) * H;
+    const int RN = gather_window(bound_in, C, fp, max(W, H), status);
+    float out[4] = {0.f, 0.f, 0.f, 0.f};
+    const bool fast = RN <= RN_MAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && !fp.point_mode;
+    if (fast) {
+        switch (RN) {
+            case 0: transport_body<0, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
+            case 1: transport_body<1, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
+            case 2: transport_body<2, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
+            default: transport_body<3, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
+        }
+    } else {
+        const int Y = y0 + ty;
+        const int R = RN + 1;
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int X = x0 + 4 * tx + i;
+            if (X < W && Y < H) {
+                out[i] = gather_generic_2d(A, U, c, C, W, H, X, Y, R, fp);
+                Anext[size_t(c) * N + size_t(Y) * W + X] = out[i];
+            }
+        }
+    }
+    // Spread of this channel of the next state, for the next step's window.
+    float vmax = -INFINITY, vmin = INFINITY;
+    bool bad = false;
+    const int Y = y0 + ty;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int X = x0 + 4 * tx + i;
+        if (X < W && Y < H) {
+            float v = out[i];
+            bad |= !isfinite(v);
+            vmax = fmaxf(vmax, v);
+            vmin = fminf(vmin, v);
+        }
+    }
+    if (bound_out) block_minmax_atomic(vmax, vmin, bad, bound_out + 2 * c);
 }
 
 void launch_transport_2d(const float* A, const float* U, float* Anext, int C, int W, int H, const FlowParams& fp,
                          const int* bound_in, int* bound_out, int* status, cudaStream_t st) {
-    dim3 grid((W + TT_W - 1) / TT_W, (H + TT_H - 1) / TT_H);
+    dim3 grid((W + TT_W - 1) / TT_W, (H + TT_H - 1) / TT_H, C);
     size_t smem = transport_smem_bytes();
     if (fp.area_pow2)
         transport_2d<true><<<grid, 256, smem, st>>>(A, U, Anext, C, W, H, fp, bound_in, bound_out, status);
@@ -443,39 +532,45 @@ void launch_transport_2d(const float* A, const float* U, float* Anext, int C, in
 void transport_2d_set_attributes() {
     cudaFuncSetAttribute(transport_2d<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(transport_smem_bytes()));
     cudaFuncSetAttribute(transport_2d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(transport_smem_bytes()));
+    cudaFuncSetAttribute(transport_2d<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(transport_2d<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(conv_direct_growth_2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(conv_direct_smem_bytes(MAX_DIRECT_RADIUS)));
 }
 
 // ---------------------------------------------------------------------------
-// Spread of the channel sum of a state (initial flow bound).
+// Per-channel spread of a state (initial flow bound) and slot reset.
 // ---------------------------------------------------------------------------
-__global__ void bound_reset_kernel(int* slot) {
-    slot[0] = float_to_ordered(-INFINITY);
-    slot[1] = float_to_ordered(INFINITY);
-}
-
-__global__ void __launch_bounds__(256) channel_sum_minmax(const float* __restrict__ A, int C, size_t N, int* slot) {
-    float vmax = -INFINITY, vmin = INFINITY;
-    for (size_t i = blockIdx.x * size_t(256) + threadIdx.x; i < N; i += size_t(gridDim.x) * 256) {
-        float s = 0.f;
-        for (int c = 0; c < C; ++c) s = __fadd_rn(s, A[size_t(c) * N + i]);
-        if (s != s) { vmax = NAN; vmin = NAN; break; }
-        vmax = fmaxf(vmax, s);
-        vmin = fminf(vmin, s);
+__global__ void bound_reset_kernel(int* slot, int C) {
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        slot[2 * c] = float_to_ordered(-INFINITY);
+        slot[2 * c + 1] = float_to_ordered(INFINITY);
     }
-    block_minmax_atomic(vmax, vmin, slot);
 }
 
-void launch_bound_reset(int* slot, cudaStream_t st) {
-    if (slot) bound_reset_kernel<<<1, 1, 0, st>>>(slot);
+__global__ void __launch_bounds__(256) channel_minmax(const float* __restrict__ A, size_t N, int* slot) {
+    const int c = blockIdx.y;
+    const float* a = A + size_t(c) * N;
+    float vmax = -INFINITY, vmin = INFINITY;
+    bool bad = false;
+    for (size_t i = blockIdx.x * size_t(256) + threadIdx.x; i < N; i += size_t(gridDim.x) * 256) {
+        float v = a[i];
+        bad |= !isfinite(v);
+        vmax = fmaxf(vmax, v);
+        vmin = fminf(vmin, v);
+    }
+    block_minmax_atomic(vmax, vmin, bad, slot + 2 * c);
+}
+
+void launch_bound_reset(int* slot, int C, cudaStream_t st) {
+    if (slot && C > 0) bound_reset_kernel<<<1, 32, 0, st>>>(slot, C);
 }
 
 void launch_bound_init(const float* A, int C, size_t N, int* slot, cudaStream_t st) {
-    bound_reset_kernel<<<1, 1, 0, st>>>(slot);
+    launch_bound_reset(slot, C, st);
     size_t want = (N + 255) / 256;
-    int blocks = int(want < size_t(148 * 4) ? want : size_t(148 * 4));
-    if (blocks > 0 && C > 0) channel_sum_minmax<<<blocks, 256, 0, st>>>(A, C, N, slot);
+    int blocks = int(want < size_t(148) ? want : size_t(148));
+    if (blocks > 0 && C > 0) channel_minmax<<<dim3(blocks, C), 256, 0, st>>>(A, N, slot);
 }
 
 // ---------------------------------------------------------------------------

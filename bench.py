@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-flush", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline (profiling runs)")
+    ap.add_argument("--conv", choices=["auto", "direct", "fft"], default="auto",
+                    help="convolution path (auto = the engine's measured choice)")
     return ap.parse_args()
 
 
@@ -187,7 +190,7 @@ def cpu_reference_run(cfg, state, seconds: float, max_steps: int, warmup: int = 
     st = p.run(state, warmup, threads=threads) if warmup else state
     t0 = time.perf_counter()
     n = 0
-    while n < max_steps and (time.perf_counter() - t0) < seconds:
+    while n < max_steps and (n == 0 or (time.perf_counter() - t0) < seconds):
         st = p.run(st, 1, threads=threads)
         n += 1
     dt = time.perf_counter() - t0
@@ -223,7 +226,8 @@ def main():
     from autoverse_b200 import _native as nat
     dist = dist_init()
     dev = nat.device_info()
-    p = fl.CudaPropagator(cfg)
+    p = fl.CudaPropagator(cfg, conv_mode={"auto": fl.CONV_AUTO, "direct": fl.CONV_DIRECT,
+                                          "fft": fl.CONV_FFT}[args.conv])
     mode = {fl.CONV_DIRECT: "direct", fl.CONV_FFT: "fft"}[p.conv_mode]
     p.write_state(state)
     flush = not args.no_flush
@@ -273,7 +277,7 @@ def main():
     e2e_value = WORLD * cells * args.e2e_steps / e2e_t
 
     cpu = None
-    if RANK == 0 and WORLD == 1:
+    if RANK == 0 and WORLD == 1 and not args.skip_cpu:
         n, dt, threads = cpu_reference_run(cfg, state, args.cpu_seconds, 200)
         cpu = {"value": cells * n / dt, "unit": "cell-steps/s", "cores": threads, "kind": "port",
                "sample": f"{n} steps of the same workload (time-bounded at {args.cpu_seconds:.0f} s, 1 warm-up), "
