@@ -73,6 +73,7 @@ SIGNATURES = {
     "flp_host_free": (I, [P]),
     "flp_profile_run": (I, [P, I, I, C.POINTER(F), I, C.POINTER(I), C.c_char_p, Z, C.POINTER(F)]),
     "flp_debug_affinity": (I, [P, P, Z]),
+    "flp_affinity_noalloc": (I, [S, P, P, P]),
     "flp_debug_transport": (I, [P, P, P, P, Z]),
 }
 

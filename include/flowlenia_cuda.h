@@ -144,6 +144,24 @@ FLP_API int flp_debug_affinity(flp_propagator* h, float* aff_out, size_t n);
  * mass sum, Sobel, flow, reintegration.  Writes the next state to out. */
 FLP_API int flp_debug_transport(flp_propagator* h, const float* state, const float* aff, float* out, size_t n);
 
+/* Allocation-free affinity.  No counterpart in the reference: an addition for
+ * callers that may not allocate device memory, such as code enqueued from
+ * another framework's plugin or custom operator on that framework's stream,
+ * where cudaMalloc would synchronise the device, break the caller's graph
+ * capture and fragment the framework's memory pool.  Computes the same
+ * affinity as the direct path of flp_debug_affinity -- U = sum_k w_k
+ * G(K_k * A_src) for a 2D config -- from the caller's device state
+ * (channels*N floats) into the caller's device buffer d_affinity
+ * (channels*N floats), on `stream` (NULL = the default stream).  The kernel
+ * descriptors and stencil taps go into a 1 MiB file-scope device array, held
+ * on every device that loads the library until exit; configs whose taps do
+ * not fit, or with a kernel radius above 24, are rejected with
+ * FLP_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (once per device); make that first call before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race and
+ * must be serialised by the caller.  Calls no cudaMalloc or cudaFree. */
+FLP_API int flp_affinity_noalloc(const char* config_json, const float* d_state, float* d_affinity, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
