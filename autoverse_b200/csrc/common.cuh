@@ -32,6 +32,8 @@ struct FlowParams {
     float beta_a, nexp;
     float ubound;       // max over channels of sum_k |w_k| for kernels targeting the channel
     float pos_eps;      // absolute margin (cells) for rounding of positions in the gather window
+    float inv_beta;     // 1 / beta_a when beta_a is a power of two (exact)
+    int beta_pow2;
     int area_pow2;      // 1 when the division by total_area is a multiplication
     int point_mode;     // total_area < 1e-10: nearest-cell deposit
 };
@@ -67,14 +69,6 @@ __device__ __forceinline__ int wrap_near(int c, int size) {
     while (c < 0) c += size;
     while (c >= size) c -= size;
     return c;
-}
-
-// Flow-bound slots: C pairs (max, min) of ordered ints, reset to (-inf, +inf).
-__device__ __forceinline__ void reset_bound_slots(int* slot, int C) {
-    for (int c = 0; c < C; ++c) {
-        slot[2 * c] = float_to_ordered(-INFINITY);
-        slot[2 * c + 1] = float_to_ordered(INFINITY);
-    }
 }
 
 // alpha = clamp((A/beta)^n, 0, 1) with the reference's integer-n fast paths

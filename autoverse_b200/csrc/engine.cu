@@ -20,7 +20,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/flowlenia_cuda.h"
+#include "flowlenia_cuda.h"
 #include "kernels.h"
 #include "schema.h"
 
@@ -103,7 +103,10 @@ struct flp_propagator {
     int rmax = 0;
     bool direct_ok = false;
     FlowParams fp{};
-    int* d_bound = nullptr;  // 2 state buffers x C channels x (max, min) as ordered ints
+    int* d_dmax = nullptr;   // largest |dest - x| of the step (float bits), reset by the step's first kernel
+    float* d_DX = nullptr;   // per-channel destinations and masses (C x N each)
+    float* d_DY = nullptr;
+    float* d_MS = nullptr;
     int* d_status = nullptr;
     double2* d_partial = nullptr;
     double* d_mass = nullptr;
@@ -139,7 +142,7 @@ struct flp_propagator {
     void enqueue_conv(const float* a, int* reset_slot) {
         if (K == 0) {
             // No kernels: the affinity stays zero (it is cleared at creation).
-            launch_bound_reset(reset_slot, C, st);
+            launch_zero_ints(reset_slot, 1, st);
             mark(0);
             return;
         }
@@ -147,7 +150,7 @@ struct flp_propagator {
             launch_conv_direct_2d(a, U, d_kd, K, d_taps, W, H, C, rmax, reset_slot, st);
             mark(0);
         } else {
-            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, reset_slot, C, st);
+            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, reset_slot, 1, st);
             mark(0);
             launch_fft_cols(d_S, d_KH, d_T, d_slot, K, W, H, geom, 0, 1.f, st);
             mark(1);
@@ -157,19 +160,24 @@ struct flp_propagator {
     }
 
     std::vector<std::string> stage_names() const {
-        if (K == 0) return {"bound_reset", "transport_2d"};
-        if (conv_mode == FLP_CONV_DIRECT) return {"conv_direct_growth_2d", "transport_2d"};
-        return {"fft_rows_r2c", "fft_cols_conv", "fft_rows_c2r_growth", "transport_2d"};
+        if (K == 0) return {"slot_reset", "flow_2d", "gather_2d"};
+        if (conv_mode == FLP_CONV_DIRECT) return {"conv_direct_growth_2d", "flow_2d", "gather_2d"};
+        return {"fft_rows_r2c", "fft_cols_conv", "fft_rows_c2r_growth", "flow_2d", "gather_2d"};
+    }
+
+    void enqueue_transport(const float* a, float* an) {
+        const int ns = int(stage_names().size());
+        launch_flow_2d(a, U, d_DX, d_DY, d_MS, C, W, H, fp, d_dmax, d_status, st);
+        mark(ns - 2);
+        launch_gather_2d(d_DX, d_DY, d_MS, an, C, W, H, fp, d_dmax, st);
+        mark(ns - 1);
     }
 
     void enqueue_step() {
         const float* a = A[cur];
         float* an = A[cur ^ 1];
-        int* bin = d_bound + 2 * C * cur;
-        int* bout = d_bound + 2 * C * (cur ^ 1);
-        enqueue_conv(a, bout);
-        launch_transport_2d(a, U, an, C, W, H, fp, bin, bout, d_status, st);
-        mark(int(stage_names().size()) - 1);
+        enqueue_conv(a, d_dmax);
+        enqueue_transport(a, an);
         CK(cudaGetLastError());
         cur ^= 1;
     }
@@ -182,7 +190,7 @@ struct flp_propagator {
     void free_all() {
         for (auto& g : graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-        void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_bound, d_status, d_partial, d_mass,
+        void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_dmax, d_DX, d_DY, d_MS, d_status, d_partial, d_mass,
                         d_tw, d_S, d_T, d_KH, d_srcs, d_slot};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -340,8 +348,15 @@ static FlowParams make_flow_params(const SimulationConfig& cfg) {
     fp.area_pow2 = (fp.total_area > 0.f && mant == 0.5f && std::isnormal(fp.total_area)) ? 1 : 0;
     fp.inv_area = fp.area_pow2 ? 1.0f / fp.total_area : 0.f;
     fp.beta_a = cfg.flow.beta_a;
+    {
+        int eb = 0;
+        const float mb = std::frexp(fp.beta_a, &eb);
+        fp.beta_pow2 = (fp.beta_a > 0.f && mb == 0.5f && std::isnormal(fp.beta_a) && std::isnormal(1.0f / fp.beta_a)) ? 1 : 0;
+        fp.inv_beta = fp.beta_pow2 ? 1.0f / fp.beta_a : 0.f;
+    }
     fp.nexp = cfg.flow.n;
     fp.point_mode = fp.total_area < 1e-10f ? 1 : 0;
+    if (fp.point_mode) fp.area_pow2 = 0;  // nearest-cell deposits carry the raw mass
     std::vector<float> wsum(cfg.channels, 0.f);
     for (const auto& k : cfg.kernels) wsum[k.target_channel] += std::fabs(k.weight);
     fp.ubound = 0.f;
@@ -371,7 +386,10 @@ static void create(const std::string& json, flp_propagator* h) {
     CK(cudaMemsetAsync(h->A[0], 0, CN * sizeof(float), h->st));
     CK(cudaMemsetAsync(h->A[1], 0, CN * sizeof(float), h->st));
     CK(cudaMemsetAsync(h->U, 0, CN * sizeof(float), h->st));
-    h->d_bound = dalloc<int>(4 * size_t(h->C));
+    h->d_dmax = dalloc<int>(1);
+    h->d_DX = dalloc<float>(CN);
+    h->d_DY = dalloc<float>(CN);
+    h->d_MS = dalloc<float>(CN);
     h->d_status = dalloc<int>(1);
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
     h->np = 256;
@@ -397,7 +415,6 @@ static void create(const std::string& json, flp_propagator* h) {
     if (h->K) CK(cudaMemcpy(h->d_kd, h->kd.data(), h->kd.size() * sizeof(KDesc), cudaMemcpyHostToDevice));
     setup_fft(h, ks);
     h->fp = make_flow_params(c);
-    launch_bound_init(h->A[0], h->C, h->N, h->d_bound, h->st);
     CK(cudaStreamSynchronize(h->st));
     resolve_conv_mode(h, FLP_CONV_AUTO);
 }
@@ -406,7 +423,6 @@ static void upload_state(flp_propagator* h, const float* src, size_t n) {
     const size_t CN = size_t(h->C) * h->N;
     if (n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "state size mismatch: expected " + std::to_string(CN));
     CK(cudaMemcpyAsync(h->A[h->cur], src, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
-    launch_bound_init(h->A[h->cur], h->C, h->N, h->d_bound + 2 * h->C * h->cur, h->st);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
 }
@@ -743,24 +759,22 @@ int flp_debug_transport(flp_propagator* h, const float* state, const float* aff,
     FLP_TRY({
         const size_t CN = size_t(h->C) * h->N;
         if (!state || !aff || !out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "size mismatch");
+        // The handle's own scratch planes are reused; the live state is untouched.
         float* a = dalloc<float>(CN);
-        float* u = dalloc<float>(CN);
         float* o = dalloc<float>(CN);
-        int* slots = dalloc<int>(4 * size_t(h->C));
         try {
             CK(cudaMemcpyAsync(a, state, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
-            CK(cudaMemcpyAsync(u, aff, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
-            launch_bound_init(a, h->C, h->N, slots, h->st);
-            launch_bound_reset(slots + 2 * h->C, h->C, h->st);
-            launch_transport_2d(a, u, o, h->C, h->W, h->H, h->fp, slots, slots + 2 * h->C, h->d_status, h->st);
+            CK(cudaMemcpyAsync(h->U, aff, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+            launch_zero_ints(h->d_dmax, 1, h->st);
+            h->enqueue_transport(a, o);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(out, o, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
             CK(cudaStreamSynchronize(h->st));
         } catch (...) {
-            cudaFree(a); cudaFree(u); cudaFree(o); cudaFree(slots);
+            cudaFree(a); cudaFree(o);
             throw;
         }
-        cudaFree(a); cudaFree(u); cudaFree(o); cudaFree(slots);
+        cudaFree(a); cudaFree(o);
     })
 }
 

@@ -33,13 +33,15 @@ size_t conv_direct_smem_bytes(int rmax);
 void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, const float* taps, int W, int H, int C,
                            int rmax, int* reset_slot, cudaStream_t st);
 
-// fused transport
-size_t transport_smem_bytes();
+// transport: flow (destinations) then gather
+size_t flow_smem_bytes(int C);
+size_t gather_smem_bytes();
 void transport_2d_set_attributes();
-void launch_transport_2d(const float* A, const float* U, float* Anext, int C, int W, int H, const FlowParams& fp,
-                         const int* bound_in, int* bound_out, int* status, cudaStream_t st);
-void launch_bound_init(const float* A, int C, size_t N, int* slot, cudaStream_t st);
-void launch_bound_reset(int* slot, int C, cudaStream_t st);
+void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float* MS, int C, int W, int H,
+                    const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st);
+void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
+                      const FlowParams& fp, const int* dmax_slot, cudaStream_t st);
+void launch_zero_ints(int* p, int n, cudaStream_t st);
 
 // FP64 compensated mass
 void launch_mass_fp64(const float* A, size_t n, double2* partial, int np, double* out, cudaStream_t st);

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __rest
     const int x0 = blockIdx.x * CD_TW, y0 = blockIdx.y * CD_TH;
     const size_t N = size_t(W) * H;
     if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0)
-        reset_bound_slots(reset_slot, nreset);
+        for (int i = 0; i < nreset; ++i) reset_slot[i] = 0;
     const int Pmax = CD_TW + 2 * rmax;
     float* tile = sm;                                   // (CD_TH + 2r) x (CD_TW + 2r)
     float* tsm = sm + size_t(CD_TH + 2 * rmax) * Pmax;  // taps
@@ -100,35 +100,60 @@ void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, con
                            int rmax, int* reset_slot, cudaStream_t st) {
     dim3 grid((W + CD_TW - 1) / CD_TW, (H + CD_TH - 1) / CD_TH, C);
     size_t smem = conv_direct_smem_bytes(rmax);
-    conv_direct_growth_2d<<<grid, dim3(32, 8), smem, st>>>(A, U, kd, K, taps, W, H, rmax, reset_slot, C);
+    conv_direct_growth_2d<<<grid, dim3(32, 8), smem, st>>>(A, U, kd, K, taps, W, H, rmax, reset_slot, 1);
 }
 
 // ---------------------------------------------------------------------------
-// Gather window from the flow bound.
-// |F_x|,|F_y| <= max(max|grad U|, max|grad A_sum|) since F = (1-a)gU - a gA
-// with a in [0,1]; the Sobel/8 of a field ranges over at most half its spread,
-// |U| <= sum_k |w_k| (G in [-1,1]) and the spread of A_sum is at most
-// sum_c (max A_c - min A_c).  With |dest - x| <= D, a source at x overlaps
-// cell ix only if x - ix lies in (-(D+s), D+s+1) (reintegration.rs:105-146),
-// so sources x = ix + k with k in [-RN, RN+1], RN = ceil(D+s) - 1, cover every
-// deposit.  D carries a margin for the rounding of dest and x_min/x_max.
-// bound: C pairs (max, min) as ordered ints.  Returns RN.
+// Transport in two kernels.
+//
+// flow_2d (one thread per cell, all channels): channel sum, Sobel of the sum
+// and of U_c, alpha, flow, destination dest = x + dt*F (reintegration.rs:81-82)
+// and the mass (zeroed below 1e-10, reintegration.rs:76-78), written as three
+// planes per channel; it also publishes the largest |dest - x| of any cell
+// with mass.
+//
+// gather_2d (one block per 64x16 tile and channel): with D the largest
+// displacement, a source at x overlaps cell ix only if x - ix lies in
+// (-(D+s), D+s+1) (reintegration.rs:105-146), so sources x = ix + k with
+// k in [-RN, RN+1], RN = ceil(D+s) - 1, cover every deposit.  Each
+// destination sums the overlaps of those sources in the reference's deposit
+// order (row-major over wrapped source indices), so the result is the
+// reference's scatter bit for bit.  No atomics touch the state.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int gather_window(const int* bound, int C, const FlowParams& fp, int maxside, int* status) {
-    float hi = 0.f, lo = 0.f;
-    for (int c = 0; c < C; ++c) {
-        hi += ordered_to_float(bound[2 * c]);
-        lo += ordered_to_float(bound[2 * c + 1]);
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// alpha with the reference's division mass / beta_a; a power-of-two beta_a
+// turns it into an exact multiplication.
+__device__ __forceinline__ float alpha_fp(float mass, const FlowParams& fp) {
+    if (fp.beta_pow2) {
+        const float ratio = __fmul_rn(mass, fp.inv_beta);
+        float p;
+        if (fp.nexp == 1.0f) p = ratio;
+        else if (fp.nexp == 2.0f) p = __fmul_rn(ratio, ratio);
+        else if (fp.nexp == 3.0f) p = __fmul_rn(__fmul_rn(ratio, ratio), ratio);
+        else if (fp.nexp == 4.0f) { const float r2 = __fmul_rn(ratio, ratio); p = __fmul_rn(r2, r2); }
+        else p = powf(ratio, fp.nexp);
+        if (p < 0.0f) p = 0.0f;  // f32::clamp(0, 1); NaN passes through
+        if (p > 1.0f) p = 1.0f;
+        return p;
     }
-    float spread = (hi - lo) * 1.0001f;
-    if (!(spread >= 0.f) || !isfinite(spread)) {
-        if (status && threadIdx.x == 0 && threadIdx.y == 0) atomicOr(status, STATUS_NONFINITE);
-        return 0;
-    }
-    float fb = fmaxf(fp.ubound, 0.5f * spread);
-    float Db = fp.dt * fb * 1.0001f + fp.pos_eps;
-    float rn = ceilf(Db + fp.s) - 1.0f;
-    int cap = 2 * maxside + 2;
+    return flow_alpha(mass, fp.beta_a, fp.nexp);
+}
+
+// Window from the largest displacement (dmax slot: float bits of a
+// non-negative value; NaN or +inf means unbounded).
+__device__ __forceinline__ int window_from_dmax(int bits, const FlowParams& fp, int maxside) {
+    const float md = __int_as_float(bits);
+    const float rn = ceilf(md + fp.pos_eps + fp.s) - 1.0f;
+    const int cap = 2 * maxside + 2;
     if (!(rn < float(cap))) return cap;
     return rn < 0.f ? 0 : int(rn);
 }
@@ -146,20 +171,6 @@ __device__ __forceinline__ int rotated_offset(int j, int c, int R, int size) {
     return -R + (j - (2 * R + 1 - n_lo));
 }
 
-// Overlap contribution of one source square (x_min..x_max, y_min..y_max) to
-// cell (ix, iy): reintegration.rs:129-157, in the reference's order.
-__device__ __forceinline__ float overlap_mass(float mass, float xmin, float xmax, float ymin, float ymax, int ix, int iy,
-                                              const FlowParams& fp) {
-    float ox0 = fmaxf(float(ix), xmin), ox1 = fminf(float(ix + 1), xmax);
-    float oy0 = fmaxf(float(iy), ymin), oy1 = fminf(float(iy + 1), ymax);
-    float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
-    float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
-    float area = __fmul_rn(ow, oh);
-    if (!(area > 0.f)) return 0.f;
-    float frac = fp.area_pow2 ? __fmul_rn(area, fp.inv_area) : __fdiv_rn(area, fp.total_area);
-    return __fmul_rn(mass, frac);
-}
-
 __device__ __forceinline__ int f2i_sat(float v) {
     // Rust `f32 as i32`: saturating, NaN -> 0.
     if (v != v) return 0;
@@ -168,124 +179,101 @@ __device__ __forceinline__ int f2i_sat(float v) {
     return int(v);
 }
 
-// Flow at a wrapped source cell, read straight from global memory.
-__device__ void source_dest_global(const float* __restrict__ A, const float* __restrict__ Uc, int C, int W, int H,
-                                   int xw, int yw, const FlowParams& fp, float& dest_x, float& dest_y) {
-    const size_t N = size_t(W) * H;
-    int xs[3] = {wrap_coord(xw - 1, W), xw, wrap_coord(xw + 1, W)};
-    int ys[3] = {wrap_coord(yw - 1, H), yw, wrap_coord(yw + 1, H)};
-    float as[3][3], us[3][3];
-    for (int j = 0; j < 3; ++j)
-        for (int i = 0; i < 3; ++i) {
-            size_t idx = size_t(ys[j]) * W + xs[i];
-            float s = 0.f;
-            for (int c = 0; c < C; ++c) s = __fadd_rn(s, A[size_t(c) * N + idx]);
-            as[j][i] = s;
-            us[j][i] = Uc[idx];
-        }
-    float gax, gay, gux, guy;
-    sobel2(as[0][0], as[0][1], as[0][2], as[1][0], as[1][2], as[2][0], as[2][1], as[2][2], gax, gay);
-    sobel2(us[0][0], us[0][1], us[0][2], us[1][0], us[1][2], us[2][0], us[2][1], us[2][2], gux, guy);
-    float alpha = flow_alpha(as[1][1], fp.beta_a, fp.nexp);
-    float oma = __fsub_rn(1.0f, alpha);
-    float fx = __fsub_rn(__fmul_rn(oma, gux), __fmul_rn(alpha, gax));
-    float fy = __fsub_rn(__fmul_rn(oma, guy), __fmul_rn(alpha, gay));
-    dest_x = __fadd_rn(float(xw), __fmul_rn(fp.dt, fx));
-    dest_y = __fadd_rn(float(yw), __fmul_rn(fp.dt, fy));
+// ------------------------------------------------------------- flow_2d ----
+constexpr int FL_W = 32, FL_H = 8;
+constexpr int FL_RW = FL_W + 2, FL_RH = FL_H + 2, FL_RC = FL_RW * FL_RH;  // region with the Sobel ring
+
+size_t flow_smem_bytes(int C) { return sizeof(float) * (size_t(2 * C + 1) * FL_RC); }
+
+__device__ __forceinline__ void block_max_atomic(float v, bool bad, int* slot) {
+    __shared__ float red[32];
+    const int anybad = __syncthreads_or(bad ? 1 : 0);
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = red[0];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
+        if (anybad) m = INFINITY;
+        if (m > 0.f) atomicMax(slot, __float_as_int(m));  // non-negative floats order like ints
+    }
 }
 
-// Reintegrated mass of channel c at destination (X, Y), any radius, sources
-// evaluated from global memory.  Handles the nearest-cell mode, the
-// reference's [-W, 2W] cell clamp, and radii wider than the grid.
-__device__ float gather_generic_2d(const float* __restrict__ A, const float* __restrict__ U, int c, int C, int W, int H,
-                                   int X, int Y, int R, const FlowParams& fp) {
+template <bool POW2>
+__global__ void __launch_bounds__(256) flow_2d(const float* __restrict__ A, const float* __restrict__ U,
+                                               float* __restrict__ DX, float* __restrict__ DY,
+                                               float* __restrict__ MS, int C, int W, int H, FlowParams fp,
+                                               int* dmax_slot, int* status) {
+    extern __shared__ __align__(16) float sm[];
+    float* as = sm;                    // C staged A planes
+    float* us = sm + C * FL_RC;        // C staged U planes
+    float* asum = sm + 2 * C * FL_RC;  // channel sum
+    __shared__ int colx[FL_RW], rowy[FL_RH];
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * FL_W, y0 = blockIdx.y * FL_H;
     const size_t N = size_t(W) * H;
-    const float* Ac = A + size_t(c) * N;
-    const float* Uc = U + size_t(c) * N;
-    float acc = 0.f;
-    for (int jy = 0; jy <= 2 * R; ++jy) {
-        int ky = rotated_offset(jy, Y, R, H);
-        int yw = wrap_coord(Y + ky, H);
-        int iy = yw - ky;
-        for (int jx = 0; jx <= 2 * R; ++jx) {
-            int kx = rotated_offset(jx, X, R, W);
-            int xw = wrap_coord(X + kx, W);
-            int ix = xw - kx;
-            float mass = Ac[size_t(yw) * W + xw];
-            if (fabsf(mass) < 1e-10f) continue;
-            float dx, dy;
-            source_dest_global(A, Uc, C, W, H, xw, yw, fp, dx, dy);
-            if (fp.point_mode) {
-                if (f2i_sat(roundf(dx)) == ix && f2i_sat(roundf(dy)) == iy) acc = __fadd_rn(acc, mass);
-                continue;
-            }
-            float xmin = __fsub_rn(dx, fp.s), xmax = __fadd_rn(dx, fp.s);
-            float ymin = __fsub_rn(dy, fp.s), ymax = __fadd_rn(dy, fp.s);
-            int ix_lo = max(f2i_sat(floorf(xmin)), -W), ix_hi = min(f2i_sat(ceilf(xmax)), 2 * W);
-            int iy_lo = max(f2i_sat(floorf(ymin)), -H), iy_hi = min(f2i_sat(ceilf(ymax)), 2 * H);
-            if (ix < ix_lo || ix > ix_hi || iy < iy_lo || iy > iy_hi) continue;
-            acc = __fadd_rn(acc, overlap_mass(mass, xmin, xmax, ymin, ymax, ix, iy, fp));
+    if (tid < FL_RW) colx[tid] = wrap_near(x0 - 1 + tid, W);
+    else if (tid < FL_RW + FL_RH) rowy[tid - FL_RW] = wrap_near(y0 - 1 + (tid - FL_RW), H);
+    __syncthreads();
+    for (int i = tid; i < 2 * C * FL_RC; i += 256) {
+        const int k = i / FL_RC, cell = i - k * FL_RC;
+        const int ly = cell / FL_RW, lx = cell - ly * FL_RW;
+        const size_t idx = size_t(rowy[ly]) * W + colx[lx];
+        cp_async4(sm + i, (k < C ? A + size_t(k) * N : U + size_t(k - C) * N) + idx);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = tid; i < FL_RC; i += 256) {
+        float a = 0.f;
+        for (int k = 0; k < C; ++k) a = __fadd_rn(a, as[k * FL_RC + i]);
+        asum[i] = a;
+    }
+    __syncthreads();
+    const int lx = tid & (FL_W - 1), ly = tid / FL_W;
+    const int X = x0 + lx, Y = y0 + ly;
+    float dmax = 0.f;
+    bool bad = false;
+    if (X < W && Y < H) {
+        const int o = ly * FL_RW + lx;  // top-left of the 3x3 window
+        const float* a = asum + o;
+        float gax, gay;
+        sobel2(a[0], a[1], a[2], a[FL_RW], a[FL_RW + 2], a[2 * FL_RW], a[2 * FL_RW + 1], a[2 * FL_RW + 2], gax, gay);
+        const float alpha = alpha_fp(a[FL_RW + 1], fp);
+        const float oma = __fsub_rn(1.0f, alpha);
+        const float agx = __fmul_rn(alpha, gax), agy = __fmul_rn(alpha, gay);
+        const size_t cell = size_t(Y) * W + X;
+        for (int c = 0; c < C; ++c) {
+            const float* u = us + c * FL_RC + o;
+            float gux, guy;
+            sobel2(u[0], u[1], u[2], u[FL_RW], u[FL_RW + 2], u[2 * FL_RW], u[2 * FL_RW + 1], u[2 * FL_RW + 2], gux,
+                   guy);
+            const float fx = __fsub_rn(__fmul_rn(oma, gux), agx);
+            const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
+            const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
+            const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
+            float mass = as[c * FL_RC + o + FL_RW + 1];
+            bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
+            if (fabsf(mass) < 1e-10f) mass = 0.f;
+            if (mass != 0.f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
+            DX[size_t(c) * N + cell] = dx;
+            DY[size_t(c) * N + cell] = dy;
+            MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
         }
     }
-    return acc;
+    if (status && __syncthreads_or(bad ? 1 : 0) && tid == 0) atomicOr(status, STATUS_NONFINITE);
+    block_max_atomic(dmax, bad, dmax_slot);
 }
 
-// ---------------------------------------------------------------------------
-// Fused transport.  Block = (64x16 tile, one channel), 256 threads; thread
-// (tx, ty) owns the 4-cell row strip x0+4tx.., y0+ty.  The source region is
-// the tile plus R rows above/below and TP(=4) columns left/right (columns
-// padded to keep float4 alignment); the Sobel inputs add a 1-cell ring.
-// Per source the kernel stores its square's bounds x_min, x_max, y_min, y_max
-// (reintegration.rs:105-108) and its mass; destinations then gather.
-// ---------------------------------------------------------------------------
-#ifndef TRANSPORT_MIN_BLOCKS
-#define TRANSPORT_MIN_BLOCKS 2
-#endif
-// Fused transport.  Block = (64x16 tile, one channel), 256 threads; thread
-// (tx, ty) owns the 4-cell row strip x0+4tx.., y0+ty.  Sources are the cells
-// y0-RN .. y0+15+RN+1 by x0-TP .. x0+63+TP (columns padded to keep float4
-// alignment); the Sobel inputs add a 1-cell ring.  Per source the block
-// stores its square's bounds x_min, x_max, y_min, y_max
-// (reintegration.rs:105-108) and its mass; destinations then gather.
-constexpr int TT_W = 64, TT_H = 16, TP = 4, RN_MAX = 3;
-constexpr int SR_W = TT_W + 2 * TP;              // 72 source columns
-constexpr int SR_HMAX = TT_H + 2 * RN_MAX + 1;   // up to 23 source rows
-constexpr int AR_W = SR_W + 2;                   // 74 with the Sobel ring
-constexpr int AR_HMAX = SR_HMAX + 2;             // up to 25
-constexpr int SRC_CHUNK = 8;                     // sources per thread in the sliding Sobel
-
-// Region arrays are padded to a multiple of 4 floats so that every array,
-// and hence every float4 chunk of the source arrays, is 16-byte aligned.
-__host__ __device__ constexpr int region_floats(int arh) { return ((AR_W * arh + 3) / 4) * 4; }
+// ----------------------------------------------------------- gather_2d ----
+constexpr int GT_W = 64, GT_H = 16, TP = 4, RN_MAX = 3;
+constexpr int SR_W = GT_W + 2 * TP;             // 72 source columns (float4-aligned padding)
+constexpr int SR_HMAX = GT_H + 2 * RN_MAX + 1;  // up to 23 source rows
 static_assert(SR_W % 4 == 0, "source rows must stay 16-byte aligned");
 
-size_t transport_smem_bytes() { return sizeof(float) * (3 * region_floats(AR_HMAX) + 5 * SR_W * SR_HMAX); }
+size_t gather_smem_bytes() { return sizeof(float) * 5 * SR_W * SR_HMAX; }
 
 __device__ __forceinline__ int wrap_pass(int g, int size) { return g >= size ? 0 : (g < 0 ? 2 : 1); }
-
-// Block max/min into an ordered-int slot pair.  A non-finite value anywhere
-// in the block publishes +inf as the max, so the next gather_window sees a
-// non-finite spread and raises STATUS_NONFINITE.
-__device__ __forceinline__ void block_minmax_atomic(float vmax, float vmin, bool bad, int* slot) {
-    __shared__ float red_max[32], red_min[32];
-    const int anybad = __syncthreads_or(bad ? 1 : 0);
-    for (int o = 16; o > 0; o >>= 1) {
-        vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-        vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-    }
-    int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    int warp = tid >> 5, lane = tid & 31;
-    if (lane == 0) { red_max[warp] = vmax; red_min[warp] = vmin; }
-    __syncthreads();
-    if (tid == 0) {
-        int nw = (blockDim.x * blockDim.y) >> 5;
-        float mx = red_max[0], mn = red_min[0];
-        for (int w = 1; w < nw; ++w) { mx = fmaxf(mx, red_max[w]); mn = fminf(mn, red_min[w]); }
-        if (anybad) mx = INFINITY;
-        atomicMax(slot + 0, float_to_ordered(mx));
-        atomicMin(slot + 1, float_to_ordered(mn));
-    }
-}
 
 // One source row of the gather for the thread's 4 destinations X0..X0+3.
 // Source column j of the strip window is x0-TP+4tx+j; its offset from
@@ -296,7 +284,7 @@ template <int RN, bool POW2, bool CHECK>
 __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, const float* __restrict__ rxmax,
                                            const float* __restrict__ rymin, const float* __restrict__ rymax,
                                            const float* __restrict__ rm, float cy0, float cy1, int X0, int gx_base,
-                                           int W, int cp, float inv_or_total, float (&acc)[4]) {
+                                           int W, int cp, float total_area, float (&acc)[4]) {
     constexpr int JLO = TP - RN, JHI = TP + 3 + RN + 1;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -320,10 +308,12 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
                 xsh = gx < 0 ? W : (gx >= W ? -W : 0);
             }
             const float m = mm[jj];
-            if (m == 0.f) continue;
             const float oy0 = fmaxf(cy0, ya[jj]), oy1 = fminf(cy1, yb[jj]);
             const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
-            if (!(oh > 0.f)) continue;
+            // POW2: a zero mass or a zero height adds a signed zero, which
+            // leaves acc (never -0: it starts at +0) unchanged, so the loop
+            // runs branch-free; the division path keeps the reference's skip.
+            if (!POW2 && (m == 0.f || !(oh > 0.f))) continue;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 if (j - TP - i < -RN || j - TP - i > RN + 1) continue;
@@ -336,7 +326,7 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
                     // area; a zero area adds a signed zero, which leaves acc as is.
                     acc[i] = __fadd_rn(acc[i], __fmul_rn(m, area));
                 } else if (area > 0.f) {
-                    acc[i] = __fadd_rn(acc[i], __fmul_rn(m, __fdiv_rn(area, inv_or_total)));
+                    acc[i] = __fadd_rn(acc[i], __fmul_rn(m, __fdiv_rn(area, total_area)));
                 }
             }
         }
@@ -344,233 +334,186 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
 }
 
 template <int RN, bool POW2>
-__device__ void transport_body(float* sm, const float* __restrict__ A, const float* __restrict__ U,
-                               float* __restrict__ Anext, int c, int C, int W, int H, const FlowParams& fp,
-                               float (&out)[4]) {
-    constexpr int SRH = TT_H + 2 * RN + 1, ARH = SRH + 2, AREG = region_floats(ARH);
-    float* asum = sm;                   // ARH x AR_W: channel sum
-    float* usm = asum + AREG;           // ARH x AR_W: U_c
-    float* amc = usm + AREG;            // ARH x AR_W: A_c
-    float* sxmin = amc + AREG;          // SRH x SR_W each (16-byte aligned)
+__device__ void gather_body(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
+                            const float* __restrict__ MS, float* __restrict__ out, int W, int H, const FlowParams& fp,
+                            float (&acc)[4]) {
+    constexpr int SRH = GT_H + 2 * RN + 1;
+    float* sxmin = sm;                  // SRH x SR_W each
     float* sxmax = sxmin + SR_W * SRH;
     float* symin = sxmax + SR_W * SRH;
     float* symax = symin + SR_W * SRH;
     float* smass = symax + SR_W * SRH;
+    __shared__ int colx[SR_W], rowy[SRH];
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
-    const int x0 = blockIdx.x * TT_W, y0 = blockIdx.y * TT_H;
-    const size_t N = size_t(W) * H;
-    const float* Uc = U + size_t(c) * N;
+    const int x0 = blockIdx.x * GT_W, y0 = blockIdx.y * GT_H;
     const float s = fp.s;
-
-    // channel sum, U_c and A_c over the source region plus the Sobel ring
-    for (int i = tid; i < AR_W * ARH; i += 256) {
-        const int ly = i / AR_W, lx = i - ly * AR_W;
-        const int gy = wrap_near(y0 - RN - 1 + ly, H), gx = wrap_near(x0 - TP - 1 + lx, W);
-        const size_t idx = size_t(gy) * W + gx;
-        float a = 0.f, mine = 0.f;
-        for (int k = 0; k < C; ++k) {
-            const float v = A[size_t(k) * N + idx];
-            a = __fadd_rn(a, v);
-            if (k == c) mine = v;
-        }
-        asum[i] = a;
-        amc[i] = mine;
-        usm[i] = Uc[idx];
+    if (tid < SR_W) colx[tid] = wrap_near(x0 - TP + tid, W);
+    else if (tid < SR_W + SRH) rowy[tid - SR_W] = wrap_near(y0 - RN + (tid - SR_W), H);
+    __syncthreads();
+    // stage destinations and masses (dx -> xmin in place, dy -> ymin in place)
+    for (int i = tid; i < 3 * SR_W * SRH; i += 256) {
+        const int k = i / (SR_W * SRH), cell = i - k * (SR_W * SRH);
+        const int sy = cell / SR_W, sx = cell - sy * SR_W;
+        const size_t idx = size_t(rowy[sy]) * W + colx[sx];
+        float* dst = k == 0 ? sxmin + cell : (k == 1 ? symin + cell : smass + cell);
+        cp_async4(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = tid; i < SR_W * SRH; i += 256) {
+        const float dx = sxmin[i], dy = symin[i];
+        sxmin[i] = __fsub_rn(dx, s);
+        sxmax[i] = __fadd_rn(dx, s);
+        symin[i] = __fsub_rn(dy, s);
+        symax[i] = __fadd_rn(dy, s);
     }
     __syncthreads();
-    // Per-source square bounds and (scaled) mass.  Each thread walks a column
-    // segment of SRC_CHUNK sources with a 3-row register window of the channel
-    // sum and U_c.
-    {
-        constexpr int COL0 = TP - RN, NCOL = TT_W + 2 * RN + 1;
-        constexpr int NCH = (SRH + SRC_CHUNK - 1) / SRC_CHUNK;
-        for (int item = tid; item < NCOL * NCH; item += 256) {
-            const int col = item % NCOL, ch = item / NCOL;
-            const int sx = COL0 + col, r0 = ch * SRC_CHUNK;
-            const int xw = wrap_near(x0 - TP + sx, W);
-            const float* ap = asum + r0 * AR_W + sx;  // region row r0 = source row r0 - 1
-            const float* up = usm + r0 * AR_W + sx;
-            float a0[3] = {ap[0], ap[1], ap[2]}, a1[3] = {ap[AR_W], ap[AR_W + 1], ap[AR_W + 2]};
-            float u0[3] = {up[0], up[1], up[2]}, u1[3] = {up[AR_W], up[AR_W + 1], up[AR_W + 2]};
-#pragma unroll
-            for (int r = 0; r < SRC_CHUNK; ++r) {
-                const int sy = r0 + r;
-                if (sy >= SRH) break;
-                const float* ar = ap + (r + 2) * AR_W;
-                const float* ur = up + (r + 2) * AR_W;
-                const float a2[3] = {ar[0], ar[1], ar[2]};
-                const float u2[3] = {ur[0], ur[1], ur[2]};
-                const int yw = wrap_near(y0 - RN + sy, H);
-                float mass = amc[(sy + 1) * AR_W + sx + 1];
-                if (fabsf(mass) < 1e-10f) mass = 0.f;
-                float gax, gay, gux, guy;
-                sobel2(a0[0], a0[1], a0[2], a1[0], a1[2], a2[0], a2[1], a2[2], gax, gay);
-                sobel2(u0[0], u0[1], u0[2], u1[0], u1[2], u2[0], u2[1], u2[2], gux, guy);
-                const float alpha = flow_alpha(a1[1], fp.beta_a, fp.nexp);
-                const float oma = __fsub_rn(1.0f, alpha);
-                const float fx = __fsub_rn(__fmul_rn(oma, gux), __fmul_rn(alpha, gax));
-                const float fy = __fsub_rn(__fmul_rn(oma, guy), __fmul_rn(alpha, gay));
-                const float dx = __fadd_rn(float(xw), __fmul_rn(fp.dt, fx));
-                const float dy = __fadd_rn(float(yw), __fmul_rn(fp.dt, fy));
-                const int o = sy * SR_W + sx;
-                sxmin[o] = __fsub_rn(dx, s);
-                sxmax[o] = __fadd_rn(dx, s);
-                symin[o] = __fsub_rn(dy, s);
-                symax[o] = __fadd_rn(dy, s);
-                smass[o] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
-#pragma unroll
-                for (int t = 0; t < 3; ++t) {
-                    a0[t] = a1[t]; a1[t] = a2[t];
-                    u0[t] = u1[t]; u1[t] = u2[t];
-                }
-            }
-        }
-    }
-    __syncthreads();
-
     const int Y = y0 + ty, X0 = x0 + 4 * tx;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    if (Y < H && X0 < W) {
-        const int rp_lo = (y0 + TT_H + RN >= H) ? 0 : 1, rp_hi = (y0 - RN < 0) ? 2 : 1;
-        const int cp_lo = (x0 + TT_W + RN >= W) ? 0 : 1, cp_hi = (x0 - RN < 0) ? 2 : 1;
-        const bool xin = cp_lo == 1 && cp_hi == 1;
-        const int gx_base = x0 - TP + 4 * tx;
-        const float inv_or_total = POW2 ? fp.inv_area : fp.total_area;
-        for (int rp = rp_lo; rp <= rp_hi; ++rp) {
+    if (Y >= H || X0 >= W) return;
+    const int rp_lo = (y0 + GT_H + RN >= H) ? 0 : 1, rp_hi = (y0 - RN < 0) ? 2 : 1;
+    const int cp_lo = (x0 + GT_W + RN >= W) ? 0 : 1, cp_hi = (x0 - RN < 0) ? 2 : 1;
+    const bool xin = cp_lo == 1 && cp_hi == 1;
+    const int gx_base = x0 - TP + 4 * tx;
+    for (int rp = rp_lo; rp <= rp_hi; ++rp) {
 #pragma unroll 1
-            for (int ky = -RN; ky <= RN + 1; ++ky) {
-                const int gy = Y + ky;
-                if (wrap_pass(gy, H) != rp) continue;
-                const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
-                const float cy0 = float(iy), cy1 = float(iy + 1);
-                const int off = (ty + RN + ky) * SR_W + 4 * tx;
-                if (xin) {
-                    gather_row<RN, POW2, false>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
-                                                cy0, cy1, X0, gx_base, W, 1, inv_or_total, acc);
-                } else {
-                    for (int cp = cp_lo; cp <= cp_hi; ++cp)
-                        gather_row<RN, POW2, true>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
-                                                   cy0, cy1, X0, gx_base, W, cp, inv_or_total, acc);
-                }
+        for (int ky = -RN; ky <= RN + 1; ++ky) {
+            const int gy = Y + ky;
+            if (wrap_pass(gy, H) != rp) continue;
+            const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
+            const float cy0 = float(iy), cy1 = float(iy + 1);
+            const int off = (ty + RN + ky) * SR_W + 4 * tx;
+            if (xin) {
+                gather_row<RN, POW2, false>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off, cy0,
+                                            cy1, X0, gx_base, W, 1, fp.total_area, acc);
+            } else {
+                for (int cp = cp_lo; cp <= cp_hi; ++cp)
+                    gather_row<RN, POW2, true>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
+                                               cy0, cy1, X0, gx_base, W, cp, fp.total_area, acc);
             }
         }
-        float* o = Anext + size_t(c) * N + size_t(Y) * W;
-        if (X0 + 3 < W && (W & 3) == 0) {
-            *reinterpret_cast<float4*>(o + X0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
-        } else {
+    }
+    float* o = out + size_t(Y) * W;
+    if (X0 + 3 < W && (W & 3) == 0) {
+        *reinterpret_cast<float4*>(o + X0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (X0 + i < W) o[X0 + i] = acc[i];
+        for (int i = 0; i < 4; ++i)
+            if (X0 + i < W) o[X0 + i] = acc[i];
+    }
+}
+
+// Reintegrated mass at destination (X, Y) for any window, sources read from
+// the destination planes in global memory.  Handles the nearest-cell mode,
+// the reference's [-W, 2W] cell clamp, and windows wider than the grid.
+template <bool POW2>
+__device__ float gather_generic_2d(const float* __restrict__ DX, const float* __restrict__ DY,
+                                   const float* __restrict__ MS, int W, int H, int X, int Y, int R,
+                                   const FlowParams& fp) {
+    float acc = 0.f;
+    for (int jy = 0; jy <= 2 * R; ++jy) {
+        const int ky = rotated_offset(jy, Y, R, H);
+        const int yw = wrap_coord(Y + ky, H);
+        const int iy = yw - ky;
+        for (int jx = 0; jx <= 2 * R; ++jx) {
+            const int kx = rotated_offset(jx, X, R, W);
+            const int xw = wrap_coord(X + kx, W);
+            const int ix = xw - kx;
+            const size_t src = size_t(yw) * W + xw;
+            const float m = MS[src];
+            if (m == 0.f) continue;
+            const float dx = DX[src], dy = DY[src];
+            if (fp.point_mode) {
+                if (f2i_sat(roundf(dx)) == ix && f2i_sat(roundf(dy)) == iy) acc = __fadd_rn(acc, m);
+                continue;
+            }
+            const float xmin = __fsub_rn(dx, fp.s), xmax = __fadd_rn(dx, fp.s);
+            const float ymin = __fsub_rn(dy, fp.s), ymax = __fadd_rn(dy, fp.s);
+            const int ix_lo = max(f2i_sat(floorf(xmin)), -W), ix_hi = min(f2i_sat(ceilf(xmax)), 2 * W);
+            const int iy_lo = max(f2i_sat(floorf(ymin)), -H), iy_hi = min(f2i_sat(ceilf(ymax)), 2 * H);
+            if (ix < ix_lo || ix > ix_hi || iy < iy_lo || iy > iy_hi) continue;
+            const float ox0 = fmaxf(float(ix), xmin), ox1 = fminf(float(ix + 1), xmax);
+            const float oy0 = fmaxf(float(iy), ymin), oy1 = fminf(float(iy + 1), ymax);
+            const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
+            const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
+            const float area = __fmul_rn(ow, oh);
+            if (!(area > 0.f)) continue;
+            acc = __fadd_rn(acc, POW2 ? __fmul_rn(m, area) : __fmul_rn(m, __fdiv_rn(area, fp.total_area)));
         }
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) out[i] = acc[i];
+    return acc;
 }
 
 template <bool POW2>
-__global__ void __launch_bounds__(256, TRANSPORT_MIN_BLOCKS) transport_2d(const float* __restrict__ A,
-                                                                          const float* __restrict__ U,
-                                                                          float* __restrict__ Anext, int C, int W,
-                                                                          int H, FlowParams fp,
-                                                                          const int* __restrict__ bound_in,
-                                                                          int* bound_out, int* status) {
+__global__ void __launch_bounds__(256, 3) gather_2d(const float* __restrict__ DX, const float* __restrict__ DY,
+                                                 const float* __restrict__ MS, float* __restrict__ Anext, int W,
+                                                 int H, FlowParams fp, const int* __restrict__ dmax_slot) {
     extern __shared__ __align__(16) float sm[];
     const int c = blockIdx.z;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int x0 = blockIdx.x * TT_W, y0 = blockIdx.y * TT_H;
     const size_t N = size_t(W) * H;
-    const int RN = gather_window(bound_in, C, fp, max(W, H), status);
-    float out[4] = {0.f, 0.f, 0.f, 0.f};
+    const int RN = window_from_dmax(*dmax_slot, fp, max(W, H));
+    const float* dxc = DX + size_t(c) * N;
+    const float* dyc = DY + size_t(c) * N;
+    const float* msc = MS + size_t(c) * N;
+    float* out = Anext + size_t(c) * N;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
     const bool fast = RN <= RN_MAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && !fp.point_mode;
     if (fast) {
         switch (RN) {
-            case 0: transport_body<0, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
-            case 1: transport_body<1, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
-            case 2: transport_body<2, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
-            default: transport_body<3, POW2>(sm, A, U, Anext, c, C, W, H, fp, out); break;
+            case 0: gather_body<0, POW2>(sm, dxc, dyc, msc, out, W, H, fp, acc); break;
+            case 1: gather_body<1, POW2>(sm, dxc, dyc, msc, out, W, H, fp, acc); break;
+            case 2: gather_body<2, POW2>(sm, dxc, dyc, msc, out, W, H, fp, acc); break;
+            default: gather_body<3, POW2>(sm, dxc, dyc, msc, out, W, H, fp, acc); break;
         }
-    } else {
-        const int Y = y0 + ty;
-        const int R = RN + 1;
-#pragma unroll 1
-        for (int i = 0; i < 4; ++i) {
-            const int X = x0 + 4 * tx + i;
-            if (X < W && Y < H) {
-                out[i] = gather_generic_2d(A, U, c, C, W, H, X, Y, R, fp);
-                Anext[size_t(c) * N + size_t(Y) * W + X] = out[i];
-            }
-        }
+        return;
     }
-    // Spread of this channel of the next state, for the next step's window.
-    float vmax = -INFINITY, vmin = INFINITY;
-    bool bad = false;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int x0 = blockIdx.x * GT_W, y0 = blockIdx.y * GT_H;
     const int Y = y0 + ty;
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < 4; ++i) {
         const int X = x0 + 4 * tx + i;
-        if (X < W && Y < H) {
-            float v = out[i];
-            bad |= !isfinite(v);
-            vmax = fmaxf(vmax, v);
-            vmin = fminf(vmin, v);
-        }
+        if (X < W && Y < H) out[size_t(Y) * W + X] = gather_generic_2d<POW2>(dxc, dyc, msc, W, H, X, Y, RN + 1, fp);
     }
-    if (bound_out) block_minmax_atomic(vmax, vmin, bad, bound_out + 2 * c);
 }
 
-void launch_transport_2d(const float* A, const float* U, float* Anext, int C, int W, int H, const FlowParams& fp,
-                         const int* bound_in, int* bound_out, int* status, cudaStream_t st) {
-    dim3 grid((W + TT_W - 1) / TT_W, (H + TT_H - 1) / TT_H, C);
-    size_t smem = transport_smem_bytes();
+void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float* MS, int C, int W, int H,
+                    const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
+    dim3 grid((W + FL_W - 1) / FL_W, (H + FL_H - 1) / FL_H);
     if (fp.area_pow2)
-        transport_2d<true><<<grid, 256, smem, st>>>(A, U, Anext, C, W, H, fp, bound_in, bound_out, status);
+        flow_2d<true><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
     else
-        transport_2d<false><<<grid, 256, smem, st>>>(A, U, Anext, C, W, H, fp, bound_in, bound_out, status);
+        flow_2d<false><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
+}
+
+void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
+                      const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
+    dim3 grid((W + GT_W - 1) / GT_W, (H + GT_H - 1) / GT_H, C);
+    if (fp.area_pow2)
+        gather_2d<true><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, Anext, W, H, fp, dmax_slot);
+    else
+        gather_2d<false><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, Anext, W, H, fp, dmax_slot);
 }
 
 void transport_2d_set_attributes() {
-    cudaFuncSetAttribute(transport_2d<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(transport_smem_bytes()));
-    cudaFuncSetAttribute(transport_2d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(transport_smem_bytes()));
-    cudaFuncSetAttribute(transport_2d<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    cudaFuncSetAttribute(transport_2d<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    auto set = [](const void* f, size_t bytes) {
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    };
+    set((const void*)flow_2d<true>, flow_smem_bytes(64));
+    set((const void*)flow_2d<false>, flow_smem_bytes(64));
+    set((const void*)gather_2d<true>, gather_smem_bytes());
+    set((const void*)gather_2d<false>, gather_smem_bytes());
     cudaFuncSetAttribute(conv_direct_growth_2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(conv_direct_smem_bytes(MAX_DIRECT_RADIUS)));
 }
 
-// ---------------------------------------------------------------------------
-// Per-channel spread of a state (initial flow bound) and slot reset.
-// ---------------------------------------------------------------------------
-__global__ void bound_reset_kernel(int* slot, int C) {
-    for (int c = threadIdx.x; c < C; c += blockDim.x) {
-        slot[2 * c] = float_to_ordered(-INFINITY);
-        slot[2 * c + 1] = float_to_ordered(INFINITY);
-    }
+__global__ void zero_ints_kernel(int* p, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 0;
 }
 
-__global__ void __launch_bounds__(256) channel_minmax(const float* __restrict__ A, size_t N, int* slot) {
-    const int c = blockIdx.y;
-    const float* a = A + size_t(c) * N;
-    float vmax = -INFINITY, vmin = INFINITY;
-    bool bad = false;
-    for (size_t i = blockIdx.x * size_t(256) + threadIdx.x; i < N; i += size_t(gridDim.x) * 256) {
-        float v = a[i];
-        bad |= !isfinite(v);
-        vmax = fmaxf(vmax, v);
-        vmin = fminf(vmin, v);
-    }
-    block_minmax_atomic(vmax, vmin, bad, slot + 2 * c);
-}
-
-void launch_bound_reset(int* slot, int C, cudaStream_t st) {
-    if (slot && C > 0) bound_reset_kernel<<<1, 32, 0, st>>>(slot, C);
-}
-
-void launch_bound_init(const float* A, int C, size_t N, int* slot, cudaStream_t st) {
-    launch_bound_reset(slot, C, st);
-    size_t want = (N + 255) / 256;
-    int blocks = int(want < size_t(148) ? want : size_t(148));
-    if (blocks > 0 && C > 0) channel_minmax<<<dim3(blocks, C), 256, 0, st>>>(A, N, slot);
+void launch_zero_ints(int* p, int n, cudaStream_t st) {
+    if (p && n > 0) zero_ints_kernel<<<1, 32, 0, st>>>(p, n);
 }
 
 // ---------------------------------------------------------------------------

@@ -24,7 +24,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/flowlenia_cuda.h"
+#include "flowlenia_cuda.h"
 #include "kernels.h"
 #include "schema.h"
 

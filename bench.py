@@ -97,7 +97,8 @@ def stage_bytes(cfg, stage):
         "fft_rows_r2c": nsrc * N * 4 + nsrc * spec,
         "fft_cols_conv": K * spec * 3,
         "fft_rows_c2r_growth": K * spec + C * N * 4,
-        "transport_2d": 3 * C * N * 4,
+        "flow_2d": 2 * C * N * 4 + 3 * C * N * 4,
+        "gather_2d": 3 * C * N * 4 + C * N * 4,
         "conv_direct_growth_2d": nsrc * N * 4 + C * N * 4,
     }.get(stage)
 

@@ -94,6 +94,7 @@ def test_transport_tiny_world_wraps_many_times():
 
 AFF_CASES = {
     "blob64_R10": lambda: blob_case(),
+    "species80x60_untemplated": lambda: species_case(80, 60, C=2, R=7, seed=14),
     "blob256_R13": lambda: blob_case(256, R=13, steps_in=2),
     "species96x64": lambda: species_case(),
     "species128_R15": lambda: species_case(128, 128, R=15, seed=8),
@@ -197,5 +198,5 @@ def test_profile_run_reports_stages():
     with fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT) as p:
         p.write_state(st)
         prof = p.profile_run(3, flush_l2=True)
-    assert set(prof["stages"]) == {"fft_rows_r2c", "fft_cols_conv", "fft_rows_c2r_growth", "transport_2d"}
+    assert set(prof["stages"]) == {"fft_rows_r2c", "fft_cols_conv", "fft_rows_c2r_growth", "flow_2d", "gather_2d"}
     assert prof["step_ms"] > 0
