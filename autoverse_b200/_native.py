@@ -74,6 +74,17 @@ SIGNATURES = {
     "flp_profile_run": (I, [P, I, I, C.POINTER(F), I, C.POINTER(I), C.c_char_p, Z, C.POINTER(F)]),
     "flp_debug_affinity": (I, [P, P, Z]),
     "flp_affinity_noalloc": (I, [S, P, P, P]),
+    "flp_batch_create": (I, [C.POINTER(C.c_char_p), I, PP]),
+    "flp_batch_destroy": (I, [P]),
+    "flp_batch_state_from_seed": (I, [P, I, S]),
+    "flp_batch_write_world": (I, [P, I, P, Z]),
+    "flp_batch_read_world": (I, [P, I, P, Z, C.POINTER(F), C.POINTER(U64)]),
+    "flp_batch_run": (I, [P, U64]),
+    "flp_batch_synchronize": (I, [P]),
+    "flp_batch_total_mass": (I, [P, P, I]),
+    "flp_batch_info": (I, [P, C.POINTER(I), C.POINTER(Z), C.POINTER(Z)]),
+    "flp_batch_stream": (P, [P]),
+    "flp_batch_profile_run": (I, [P, I, I, C.POINTER(F), C.POINTER(F)]),
     "flp_debug_transport": (I, [P, P, P, P, Z]),
 }
 

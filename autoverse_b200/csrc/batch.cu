@@ -1,0 +1,841 @@
+// Batched engine: many independent 2D worlds of uneven sizes, channel counts
+// and parameters advanced together (the use the evolution search makes of the
+// reference, one CpuPropagator per candidate: src/compute/evolution/search.rs:152-172,
+// fitness.rs:26-88).
+//
+// All worlds share pooled buffers; a device descriptor per world gives its
+// sizes, parameters and offsets.  A step is five persistent kernels, one per
+// stage (row R2C, column convolution, row C2R + growth, flow, gather).  The
+// CTAs of each kernel pull (world, tile) items from that stage's device work
+// queue (an atomic counter over a precomputed item list, largest worlds
+// first) and dispatch at run time into the same compile-time item functions
+// the single-world kernels use, so a world gives bit-identical results in
+// either engine.  Each stage resets the next stage's counter; run(n) replays
+// a captured CUDA graph of the step loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "fft_items.cuh"
+#include "flowlenia_cuda.h"
+#include "kernels.h"
+#include "schema.h"
+#include "transport_items.cuh"
+
+namespace flp {
+
+extern thread_local std::string g_last_error;
+
+namespace {
+
+constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
+constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
+constexpr int NSTAGE = 5;
+constexpr int BATCH_GRAPH_STEPS = 8;
+
+int row_class(int M) {
+    for (int i = 0; i < int(sizeof(ROW_SIZES) / sizeof(int)); ++i)
+        if (ROW_SIZES[i] == M) return i;
+    return -1;
+}
+int col_class(int H) {
+    for (int i = 0; i < int(sizeof(COL_SIZES) / sizeof(int)); ++i)
+        if (COL_SIZES[i] == H) return i;
+    return -1;
+}
+int row_nr(int M) {
+    switch (M) {
+#define X(n) case n: return RowCfg<n>::NR;
+        FLP_ROW_SIZES(X)
+#undef X
+    }
+    return 1;
+}
+int col_nc(int H) {
+    switch (H) {
+#define X(n) case n: return ColCfg<n>::NC;
+        FLP_COL_SIZES(X)
+#undef X
+    }
+    return 1;
+}
+
+struct BWorld {
+    int W, H, C, K, nsrc, mcls, hcls, pad;
+    long long offA;  // float offset of channel 0 in the state / U / DX / DY / MS pools
+    long long offS;  // float2 offset in the source-spectrum pool
+    long long offT;  // float2 offset in the product and kernel-spectrum pools
+    int offKd;       // first kernel descriptor (and spectrum slot) of the world
+    int offSrc;      // first source-channel entry
+    int twM, twW, twH;
+    int pad2;
+    FlowParams fp;
+};
+
+constexpr int NCLS = 9;  // size classes per FFT pass
+// Queue index: FFT stages s in {0,1,2} use queue s*NCLS + class; flow and
+// gather use queues 3*NCLS and 3*NCLS+1.
+constexpr int NQUEUE = 3 * NCLS + 2;
+
+struct Pools {
+    const BWorld* worlds;
+    const int2* items;       // all queues back to back
+    const int* q_off;        // NQUEUE+1 offsets into items (device)
+    int* counters;           // NQUEUE work-queue counters, zeroed at the start of each step
+    int* dmax;      // per-world largest displacement (float bits)
+    int* status;
+    int n_worlds;
+    const float* A;
+    float* Anext;
+    float* U;
+    float* DX;
+    float* DY;
+    float* MS;
+    float2* S;
+    float2* T;
+    const float2* KH;
+    const KDesc* kd;
+    const int* srcs;
+    const int* slots;
+    const float2* tw;
+};
+
+// Claim the next item of a queue; -1 when the queue is drained.
+__device__ __forceinline__ int next_item(int* counter, int n) {
+    __shared__ int s_item;
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    return it < n ? it : -1;
+}
+
+// Zero every queue counter and every world's displacement slot.
+__global__ void k_batch_reset(Pools p) {
+    for (int i = threadIdx.x; i < NQUEUE; i += blockDim.x) p.counters[i] = 0;
+    for (int i = threadIdx.x; i < p.n_worlds; i += blockDim.x) p.dmax[i] = 0;
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const int base = p.q_off[q], n = p.q_off[q + 1] - base;
+    for (;;) {
+        const int it = next_item(p.counters + q, n);
+        if (it < 0) break;
+        const int2 item = p.items[base + it];
+        const BWorld w = p.worlds[item.x];
+        const int slot = item.y >> 16, g = item.y & 0xFFFF;
+        const int c = p.srcs[w.offSrc + slot];
+        const size_t N = size_t(2 * M) * w.H;
+        float2* Sc = p.S + w.offS + size_t(slot) * (M + 1) * w.H;
+        r2c_rows_item<M>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * RowCfg<M>::NR, p.tw + w.twM, p.tw + w.twW);
+    }
+}
+
+template <int H>
+__global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const int base = p.q_off[q], n = p.q_off[q + 1] - base;
+    for (;;) {
+        const int it = next_item(p.counters + q, n);
+        if (it < 0) break;
+        const int2 item = p.items[base + it];
+        const BWorld w = p.worlds[item.x];
+        const int k = item.y >> 16, g = item.y & 0xFFFF;
+        const int Wc = w.W / 2 + 1;
+        const int slot = p.slots[w.offKd + k];
+        const int kx0 = g * ColCfg<H>::NC;
+        const int nl = min(ColCfg<H>::NC, Wc - kx0);
+        cols_conv_item<H>(fsm, p.S + w.offS + (size_t(slot) * Wc + kx0) * H, p.KH + w.offT + (size_t(k) * Wc + kx0) * H,
+                          p.T + w.offT + (size_t(k) * Wc + kx0) * H, nl, 0, 1.f, p.tw + w.twH);
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const int base = p.q_off[q], n = p.q_off[q + 1] - base;
+    for (;;) {
+        const int it = next_item(p.counters + q, n);
+        if (it < 0) break;
+        const int2 item = p.items[base + it];
+        const BWorld w = p.worlds[item.x];
+        const int c = item.y >> 16, g = item.y & 0xFFFF;
+        float* Uc = p.U + w.offA + size_t(c) * (2 * M) * w.H;
+        c2r_growth_item<M>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H, g * RowCfg<M>::NR, p.tw + w.twM,
+                           p.tw + w.twW);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_flow(Pools p) {
+    extern __shared__ __align__(16) float sm[];
+    constexpr int q = 3 * NCLS;
+    const int base = p.q_off[q], n = p.q_off[q + 1] - base;
+    for (;;) {
+        const int it = next_item(p.counters + q, n);
+        if (it < 0) break;
+        const int2 item = p.items[base + it];
+        const BWorld w = p.worlds[item.x];
+        const int tiles_x = (w.W + FL_W - 1) / FL_W;
+        const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * FL_H;
+        if (w.fp.area_pow2)
+            flow_item<true>(sm, p.A + w.offA, p.U + w.offA, p.DX + w.offA, p.DY + w.offA, p.MS + w.offA, w.C, w.W,
+                            w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+        else
+            flow_item<false>(sm, p.A + w.offA, p.U + w.offA, p.DX + w.offA, p.DY + w.offA, p.MS + w.offA, w.C, w.W,
+                             w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) k_batch_gather(Pools p) {
+    extern __shared__ __align__(16) float sm[];
+    constexpr int q = 3 * NCLS + 1;
+    const int base = p.q_off[q], n = p.q_off[q + 1] - base;
+    for (;;) {
+        const int it = next_item(p.counters + q, n);
+        if (it < 0) break;
+        const int2 item = p.items[base + it];
+        const BWorld w = p.worlds[item.x];
+        const int c = item.y >> 16, t = item.y & 0xFFFF;
+        const int tiles_x = (w.W + GT_W - 1) / GT_W;
+        const int x0 = (t % tiles_x) * GT_W, y0 = (t / tiles_x) * GT_H;
+        const size_t off = size_t(w.offA) + size_t(c) * w.W * w.H;
+        const int bits = p.dmax[item.x];
+        if (w.fp.area_pow2)
+            gather_item<true>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
+        else
+            gather_item<false>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
+    }
+}
+
+// FP64 compensated mass per world: one block per world.
+__global__ void __launch_bounds__(256) k_batch_mass(const BWorld* worlds, const float* A, double* out) {
+    const BWorld w = worlds[blockIdx.x];
+    const size_t n = size_t(w.C) * w.W * w.H;
+    const float* a = A + w.offA;
+    double s = 0.0, c = 0.0;
+    for (size_t i = threadIdx.x; i < n; i += 256) {
+        const double x = double(a[i]);
+        const double t = s + x;
+        if (fabs(s) >= fabs(x)) c += (s - t) + x;
+        else c += (x - t) + s;
+        s = t;
+    }
+    __shared__ double ss[256], cs[256];
+    ss[threadIdx.x] = s;
+    cs[threadIdx.x] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S = 0.0, Cc = 0.0;
+        for (int i = 0; i < 256; ++i) {
+            const double x = ss[i];
+            const double t = S + x;
+            if (fabs(S) >= fabs(x)) Cc += (S - t) + x;
+            else Cc += (x - t) + S;
+            S = t;
+            Cc += cs[i];
+        }
+        out[blockIdx.x] = S + Cc;
+    }
+}
+
+template <class T>
+T* dalloc_b(size_t n) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return static_cast<T*>(p);
+}
+
+void ckb(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+std::once_flag g_battr_once;
+
+// Per-class launch helpers (class index -> template instantiation).
+const void* r2c_fn(int cls) {
+    switch (ROW_SIZES[cls]) {
+#define X(n) case n: return (const void*)k_batch_r2c<n>;
+        FLP_ROW_SIZES(X)
+#undef X
+    }
+    return nullptr;
+}
+const void* c2r_fn(int cls) {
+    switch (ROW_SIZES[cls]) {
+#define X(n) case n: return (const void*)k_batch_c2r<n>;
+        FLP_ROW_SIZES(X)
+#undef X
+    }
+    return nullptr;
+}
+const void* cols_fn(int cls) {
+    switch (COL_SIZES[cls]) {
+#define X(n) case n: return (const void*)k_batch_cols<n>;
+        FLP_COL_SIZES(X)
+#undef X
+    }
+    return nullptr;
+}
+size_t r2c_smem(int cls) {
+    switch (ROW_SIZES[cls]) {
+#define X(n) case n: return RowCfg<n>::smem_r2c;
+        FLP_ROW_SIZES(X)
+#undef X
+    }
+    return 0;
+}
+size_t c2r_smem(int cls) {
+    switch (ROW_SIZES[cls]) {
+#define X(n) case n: return RowCfg<n>::smem_c2r;
+        FLP_ROW_SIZES(X)
+#undef X
+    }
+    return 0;
+}
+size_t cols_smem(int cls) {
+    switch (COL_SIZES[cls]) {
+#define X(n) case n: return ColCfg<n>::smem;
+        FLP_COL_SIZES(X)
+#undef X
+    }
+    return 0;
+}
+
+}  // namespace
+}  // namespace flp
+
+using namespace flp;
+
+struct flp_batch {
+    std::vector<SimulationConfig> cfgs;
+    std::vector<BWorld> hw;
+    int n = 0;
+    size_t cells_total = 0;  // sum of C*N
+    cudaStream_t st = nullptr;
+    BWorld* d_worlds = nullptr;
+    int2* d_items = nullptr;
+    int* d_qoff = nullptr;
+    int n_q[NQUEUE] = {0};
+    int* d_counters = nullptr;
+    int* d_dmax = nullptr;
+    int* d_status = nullptr;
+    float* A[2] = {nullptr, nullptr};
+    float *U = nullptr, *DX = nullptr, *DY = nullptr, *MS = nullptr;
+    float2 *S = nullptr, *T = nullptr, *KH = nullptr, *tw = nullptr;
+    KDesc* d_kd = nullptr;
+    int *d_srcs = nullptr, *d_slots = nullptr;
+    double* d_mass = nullptr;
+    int cur = 0;
+    const void* q_fn[NQUEUE] = {nullptr};
+    int q_grid[NQUEUE] = {0};
+    size_t q_smem[NQUEUE] = {0};
+    std::vector<float> time;
+    std::vector<uint64_t> steps;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t ev[NSTAGE + 1] = {nullptr};
+    void* flush_buf = nullptr;
+    size_t flush_bytes = 0;
+
+    Pools pools() const {
+        Pools p{};
+        p.worlds = d_worlds;
+        p.items = d_items;
+        p.q_off = d_qoff;
+        p.counters = d_counters;
+        p.dmax = d_dmax;
+        p.status = d_status;
+        p.n_worlds = n;
+        p.A = A[cur];
+        p.Anext = A[cur ^ 1];
+        p.U = U; p.DX = DX; p.DY = DY; p.MS = MS;
+        p.S = S; p.T = T; p.KH = KH;
+        p.kd = d_kd; p.srcs = d_srcs; p.slots = d_slots; p.tw = tw;
+        return p;
+    }
+
+    void launch_queue(int q, Pools& p) {
+        if (!n_q[q]) return;
+        if (q < 3 * NCLS) {
+            int qq = q;
+            void* args[] = {&p, &qq};
+            ckb(cudaLaunchKernel(q_fn[q], dim3(q_grid[q]), dim3(256), args, q_smem[q], st), "batch launch");
+        } else {
+            void* args[] = {&p};
+            ckb(cudaLaunchKernel(q_fn[q], dim3(q_grid[q]), dim3(256), args, q_smem[q], st), "batch launch");
+        }
+    }
+
+    // reset, then per stage the size-class kernels of that stage
+    void enqueue_step(bool timed = false) {
+        Pools p = pools();
+        k_batch_reset<<<1, 256, 0, st>>>(p);
+        if (timed) ckb(cudaEventRecord(ev[0], st), "event");
+        for (int stage = 0; stage < 3; ++stage) {
+            for (int cls = 0; cls < NCLS; ++cls) launch_queue(stage * NCLS + cls, p);
+            if (timed) ckb(cudaEventRecord(ev[stage + 1], st), "event");
+        }
+        launch_queue(3 * NCLS, p);
+        if (timed) ckb(cudaEventRecord(ev[4], st), "event");
+        launch_queue(3 * NCLS + 1, p);
+        if (timed) ckb(cudaEventRecord(ev[5], st), "event");
+        ckb(cudaGetLastError(), "batch launch");
+        cur ^= 1;
+    }
+
+    void advance(uint64_t k) {
+        for (int w = 0; w < n; ++w) {
+            for (uint64_t i = 0; i < k; ++i) time[w] += cfgs[w].dt;
+            steps[w] += k;
+        }
+    }
+
+    void free_all() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, MS, S, T,
+                        KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf};
+        for (void* q : ptrs)
+            if (q) cudaFree(q);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace flp {
+namespace {
+
+void batch_create(flp_batch* b, const char* const* jsons, int n) {
+    if (n <= 0) throw std::invalid_argument("need at least one world");
+    std::call_once(g_battr_once, [] {
+        auto set = [](const void* f, size_t bytes) {
+            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+            cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        };
+        for (int c = 0; c < NCLS; ++c) {
+            set(r2c_fn(c), r2c_smem(c));
+            set(c2r_fn(c), c2r_smem(c));
+            set(cols_fn(c), cols_smem(c));
+        }
+        set((const void*)k_batch_flow, flow_smem_bytes_inl(64));
+        set((const void*)k_batch_gather, gather_smem_bytes_inl());
+        transport_2d_set_attributes();
+        fft2d_set_attributes(200 * 1024);
+    });
+    b->n = n;
+    ckb(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
+    for (auto& e : b->ev) ckb(cudaEventCreate(&e), "event");
+    // ---- per-world layout
+    std::vector<KDesc> kd;
+    std::vector<int> srcs, slots;
+    std::vector<float2> tw;
+    std::vector<std::pair<int, int>> tw_index;  // (L, offset) tables exp(-2 pi i t / L), t < L
+    auto twiddles = [&](int L) {
+        for (auto& e : tw_index)
+            if (e.first == L) return e.second;
+        const int off = int(tw.size());
+        for (int t = 0; t < L; ++t) {
+            const double ang = -2.0 * M_PI * double(t) / double(L);
+            tw.push_back(make_float2(float(std::cos(ang)), float(std::sin(ang))));
+        }
+        tw_index.push_back({L, off});
+        return off;
+    };
+    long long offA = 0, offS = 0, offT = 0;
+    int cmax = 1;
+    std::vector<std::vector<KernelStencil>> stencils(n);
+    for (int w = 0; w < n; ++w) {
+        if (!jsons[w]) throw ConfigError("null config for world " + std::to_string(w));
+        SimulationConfig c = parse_config(jsons[w]);
+        if (c.is_3d()) throw ConfigError("world " + std::to_string(w) + ": the batched engine serves 2D worlds");
+        BWorld d{};
+        d.W = c.width; d.H = c.height; d.C = c.channels; d.K = int(c.kernels.size());
+        d.mcls = (d.W % 2 == 0) ? row_class(d.W / 2) : -1;
+        d.hcls = col_class(d.H);
+        if (d.mcls < 0 || d.hcls < 0)
+            throw ConfigError("world " + std::to_string(w) + ": batched sides must be even widths with W/2 in {16..256} and H in {32..512} of factors 2 and 3");
+        cmax = std::max(cmax, d.C);
+        d.offA = offA;
+        offA += (long long)d.C * d.W * d.H;
+        d.offKd = int(kd.size());
+        d.offSrc = int(srcs.size());
+        std::vector<int> my_src;
+        for (int k = 0; k < d.K; ++k) {
+            const KernelConfig& kc = c.kernels[k];
+            stencils[w].push_back(build_kernel(kc, c.kernel_radius, 2));
+            (void)pad_kernel(stencils[w].back(), d.W, d.H, 1);  // radius check
+            KDesc kdsc{};
+            kdsc.src = kc.source_channel;
+            kdsc.tgt = kc.target_channel;
+            kdsc.r = stencils[w].back().radius;
+            kdsc.weight = kc.weight;
+            kdsc.mu = kc.mu;
+            const float sigma_sq_2 = 2.0f * kc.sigma * kc.sigma;
+            kdsc.inv2s2 = 1.0f / sigma_sq_2;
+            kd.push_back(kdsc);
+            auto it = std::find(my_src.begin(), my_src.end(), kc.source_channel);
+            int slot;
+            if (it == my_src.end()) { slot = int(my_src.size()); my_src.push_back(kc.source_channel); }
+            else slot = int(it - my_src.begin());
+            slots.push_back(slot);
+        }
+        d.nsrc = int(my_src.size());
+        srcs.insert(srcs.end(), my_src.begin(), my_src.end());
+        const long long spec = (long long)(d.W / 2 + 1) * d.H;
+        d.offS = offS;
+        offS += spec * std::max(d.nsrc, 1);
+        d.offT = offT;
+        offT += spec * std::max(d.K, 1);
+        d.twM = twiddles(d.W / 2);
+        d.twW = twiddles(d.W);
+        d.twH = twiddles(d.H);
+        // flow parameters (same derivation as the single-world engine)
+        FlowParams fp{};
+        fp.dt = c.dt;
+        fp.s = c.flow.distribution_size;
+        const float two_s = 2.0f * fp.s;
+        fp.total_area = two_s * two_s;
+        int e = 0;
+        const float mant = std::frexp(fp.total_area, &e);
+        fp.area_pow2 = (fp.total_area > 0.f && mant == 0.5f && std::isnormal(fp.total_area)) ? 1 : 0;
+        fp.inv_area = fp.area_pow2 ? 1.0f / fp.total_area : 0.f;
+        fp.beta_a = c.flow.beta_a;
+        int eb = 0;
+        const float mb = std::frexp(fp.beta_a, &eb);
+        fp.beta_pow2 = (fp.beta_a > 0.f && mb == 0.5f && std::isnormal(fp.beta_a) && std::isnormal(1.0f / fp.beta_a)) ? 1 : 0;
+        fp.inv_beta = fp.beta_pow2 ? 1.0f / fp.beta_a : 0.f;
+        fp.nexp = c.flow.n;
+        fp.point_mode = fp.total_area < 1e-10f ? 1 : 0;
+        if (fp.point_mode) fp.area_pow2 = 0;
+        const float maxside = float(std::max(c.width, c.height));
+        fp.pos_eps = 8.0f * maxside * 1.1920929e-07f + 1e-4f;
+        d.fp = fp;
+        b->hw.push_back(d);
+        b->cfgs.push_back(c);
+    }
+    b->cells_total = size_t(offA);
+    b->time.assign(n, 0.f);
+    b->steps.assign(n, 0);
+    // ---- pools
+    const size_t CN = size_t(offA);
+    b->A[0] = dalloc_b<float>(CN);
+    b->A[1] = dalloc_b<float>(CN);
+    b->U = dalloc_b<float>(CN);
+    b->DX = dalloc_b<float>(CN);
+    b->DY = dalloc_b<float>(CN);
+    b->MS = dalloc_b<float>(CN);
+    ckb(cudaMemsetAsync(b->A[0], 0, CN * sizeof(float), b->st), "memset");
+    ckb(cudaMemsetAsync(b->A[1], 0, CN * sizeof(float), b->st), "memset");
+    ckb(cudaMemsetAsync(b->U, 0, CN * sizeof(float), b->st), "memset");
+    b->S = dalloc_b<float2>(size_t(offS));
+    b->T = dalloc_b<float2>(size_t(offT));
+    b->KH = dalloc_b<float2>(size_t(offT));
+    b->tw = dalloc_b<float2>(tw.size());
+    b->d_kd = dalloc_b<KDesc>(kd.size());
+    b->d_srcs = dalloc_b<int>(srcs.size());
+    b->d_slots = dalloc_b<int>(slots.size());
+    b->d_worlds = dalloc_b<BWorld>(n);
+    b->d_counters = dalloc_b<int>(NQUEUE);
+    b->d_dmax = dalloc_b<int>(n);
+    b->d_status = dalloc_b<int>(1);
+    b->d_mass = dalloc_b<double>(n);
+    ckb(cudaMemsetAsync(b->d_counters, 0, NQUEUE * sizeof(int), b->st), "memset");
+    ckb(cudaMemsetAsync(b->d_status, 0, sizeof(int), b->st), "memset");
+    ckb(cudaMemcpy(b->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice), "copy");
+    if (!kd.empty()) ckb(cudaMemcpy(b->d_kd, kd.data(), kd.size() * sizeof(KDesc), cudaMemcpyHostToDevice), "copy");
+    if (!srcs.empty()) ckb(cudaMemcpy(b->d_srcs, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
+    if (!slots.empty()) ckb(cudaMemcpy(b->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
+    ckb(cudaMemcpy(b->d_worlds, b->hw.data(), n * sizeof(BWorld), cudaMemcpyHostToDevice), "copy");
+    // ---- kernel spectra, world by world, with the single-world FFT passes
+    for (int w = 0; w < n; ++w) {
+        const BWorld& d = b->hw[w];
+        if (d.K == 0) continue;
+        FftGeom g;
+        make_plan(d.W / 2, g.pm);
+        make_plan(d.H, g.ph);
+        g.twM = b->tw + d.twM;
+        g.twW = b->tw + d.twW;
+        g.twH = b->tw + d.twH;
+        std::vector<float> padded(size_t(d.K) * d.W * d.H);
+        for (int k = 0; k < d.K; ++k) {
+            std::vector<float> pk = pad_kernel(stencils[w][k], d.W, d.H, 1);
+            std::copy(pk.begin(), pk.end(), padded.begin() + size_t(k) * d.W * d.H);
+        }
+        float* d_pad = dalloc_b<float>(padded.size());
+        float2* d_tmp = dalloc_b<float2>(size_t(d.K) * (d.W / 2 + 1) * d.H);
+        ckb(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, b->st), "copy");
+        launch_fft_r2c(d_pad, d_tmp, nullptr, d.K, d.W, d.H, g, nullptr, 0, b->st);
+        launch_fft_cols(d_tmp, nullptr, b->KH + d.offT, nullptr, d.K, d.W, d.H, g, 1,
+                        float(1.0 / (double(d.W) * double(d.H))), b->st);
+        ckb(cudaGetLastError(), "kernel spectra");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        cudaFree(d_pad);
+        cudaFree(d_tmp);
+    }
+    // ---- work queues, largest worlds first
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return size_t(b->hw[a].W) * b->hw[a].H > size_t(b->hw[c].W) * b->hw[c].H;
+    });
+    std::vector<int2> items[NQUEUE];
+    for (int w : order) {
+        const BWorld& d = b->hw[w];
+        const int nr = row_nr(d.W / 2), nc = col_nc(d.H), Wc = d.W / 2 + 1;
+        for (int s2 = 0; s2 < d.nsrc; ++s2)
+            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[0 * NCLS + d.mcls].push_back(make_int2(w, (s2 << 16) | g));
+        for (int k = 0; k < d.K; ++k)
+            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (k << 16) | g));
+        for (int c = 0; c < d.C; ++c)
+            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
+        const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + FL_H - 1) / FL_H);
+        for (int t = 0; t < ftiles; ++t) items[3 * NCLS].push_back(make_int2(w, t));
+        const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + GT_H - 1) / GT_H);
+        for (int c = 0; c < d.C; ++c)
+            for (int t = 0; t < gtiles; ++t) items[3 * NCLS + 1].push_back(make_int2(w, (c << 16) | t));
+    }
+    std::vector<int2> all;
+    std::vector<int> qoff(NQUEUE + 1, 0);
+    for (int q = 0; q < NQUEUE; ++q) {
+        qoff[q] = int(all.size());
+        all.insert(all.end(), items[q].begin(), items[q].end());
+        b->n_q[q] = int(items[q].size());
+    }
+    qoff[NQUEUE] = int(all.size());
+    b->d_items = dalloc_b<int2>(all.size());
+    b->d_qoff = dalloc_b<int>(qoff.size());
+    if (!all.empty()) ckb(cudaMemcpy(b->d_items, all.data(), all.size() * sizeof(int2), cudaMemcpyHostToDevice), "copy");
+    ckb(cudaMemcpy(b->d_qoff, qoff.data(), qoff.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
+    // ---- persistent grids: one wave of resident CTAs per queue
+    int dev = 0, sms = 0;
+    ckb(cudaGetDevice(&dev), "device");
+    ckb(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
+    for (int q = 0; q < NQUEUE; ++q) {
+        const int stage = q < 3 * NCLS ? q / NCLS : (q == 3 * NCLS ? 3 : 4);
+        const int cls = q % NCLS;
+        switch (stage) {
+            case 0: b->q_fn[q] = r2c_fn(cls); b->q_smem[q] = r2c_smem(cls); break;
+            case 1: b->q_fn[q] = cols_fn(cls); b->q_smem[q] = cols_smem(cls); break;
+            case 2: b->q_fn[q] = c2r_fn(cls); b->q_smem[q] = c2r_smem(cls); break;
+            case 3: b->q_fn[q] = (const void*)k_batch_flow; b->q_smem[q] = flow_smem_bytes_inl(cmax); break;
+            default: b->q_fn[q] = (const void*)k_batch_gather; b->q_smem[q] = gather_smem_bytes_inl(); break;
+        }
+        if (!b->n_q[q]) continue;
+        int per_sm = 0;
+        ckb(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->q_fn[q], 256, b->q_smem[q]), "occupancy");
+        b->q_grid[q] = std::max(1, std::min(per_sm * sms, b->n_q[q]));
+    }
+    ckb(cudaStreamSynchronize(b->st), "sync");
+}
+
+void batch_build_graph(flp_batch* b) {
+    const int c0 = b->cur;
+    cudaGraph_t g = nullptr;
+    ckb(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
+    try {
+        for (int i = 0; i < BATCH_GRAPH_STEPS; ++i) b->enqueue_step();
+    } catch (...) {
+        cudaStreamEndCapture(b->st, &g);
+        if (g) cudaGraphDestroy(g);
+        b->cur = c0;
+        throw;
+    }
+    ckb(cudaStreamEndCapture(b->st, &g), "capture");
+    b->cur = c0;
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    ckb(e, "graph instantiate");
+    b->graph[c0] = ge;
+}
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+}  // namespace
+}  // namespace flp
+
+#define BATCH_TRY(...)                                           \
+    try {                                                        \
+        __VA_ARGS__;                                             \
+        return FLP_OK;                                           \
+    } catch (const flp::ConfigError& e) {                        \
+        return flp::fail(FLP_ERR_INVALID_CONFIG, e.what());      \
+    } catch (const std::invalid_argument& e) {                   \
+        return flp::fail(FLP_ERR_INVALID_ARGUMENT, e.what());    \
+    } catch (const std::exception& e) {                          \
+        return flp::fail(FLP_ERR_CUDA, e.what());                \
+    }
+
+#define BATCH_HANDLE(b) \
+    if (!(b)) return flp::fail(FLP_ERR_INVALID_ARGUMENT, "null batch handle");
+
+extern "C" {
+
+int flp_batch_create(const char* const* config_jsons, int n_worlds, flp_batch** out) {
+    if (!config_jsons || !out) return fail(FLP_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    flp_batch* b = new flp_batch();
+    try {
+        batch_create(b, config_jsons, n_worlds);
+    } catch (...) {
+        b->free_all();
+        delete b;
+        BATCH_TRY(throw)
+    }
+    *out = b;
+    return FLP_OK;
+}
+
+int flp_batch_destroy(flp_batch* b) {
+    if (!b) return FLP_OK;
+    cudaStreamSynchronize(b->st);
+    b->free_all();
+    delete b;
+    return FLP_OK;
+}
+
+int flp_batch_write_world(flp_batch* b, int world, const float* state, size_t n) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (world < 0 || world >= b->n || !state) throw std::invalid_argument("bad world index or null state");
+        const BWorld& d = b->hw[world];
+        const size_t cn = size_t(d.C) * d.W * d.H;
+        if (n != cn) throw std::invalid_argument("state size mismatch: expected " + std::to_string(cn));
+        ckb(cudaMemcpyAsync(b->A[b->cur] + d.offA, state, cn * sizeof(float), cudaMemcpyHostToDevice, b->st), "copy");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        b->time[world] = 0.f;
+        b->steps[world] = 0;
+    })
+}
+
+int flp_batch_state_from_seed(flp_batch* b, int world, const char* seed_json) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (world < 0 || world >= b->n || !seed_json) throw std::invalid_argument("bad world index or null seed");
+        std::vector<float> g = generate_seed(seed_json, b->cfgs[world]);
+        const BWorld& d = b->hw[world];
+        ckb(cudaMemcpyAsync(b->A[b->cur] + d.offA, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice, b->st),
+            "copy");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        b->time[world] = 0.f;
+        b->steps[world] = 0;
+    })
+}
+
+int flp_batch_read_world(flp_batch* b, int world, float* out, size_t n, float* time, uint64_t* step) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (world < 0 || world >= b->n || !out) throw std::invalid_argument("bad world index or null output");
+        const BWorld& d = b->hw[world];
+        const size_t cn = size_t(d.C) * d.W * d.H;
+        if (n != cn) throw std::invalid_argument("state size mismatch: expected " + std::to_string(cn));
+        ckb(cudaMemcpyAsync(out, b->A[b->cur] + d.offA, cn * sizeof(float), cudaMemcpyDeviceToHost, b->st), "copy");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        if (time) *time = b->time[world];
+        if (step) *step = b->steps[world];
+    })
+}
+
+int flp_batch_run(flp_batch* b, uint64_t n) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        while (n >= uint64_t(BATCH_GRAPH_STEPS)) {
+            if (!b->graph[b->cur]) batch_build_graph(b);
+            ckb(cudaGraphLaunch(b->graph[b->cur], b->st), "graph launch");
+            b->advance(BATCH_GRAPH_STEPS);
+            n -= BATCH_GRAPH_STEPS;
+        }
+        for (uint64_t i = 0; i < n; ++i) {
+            b->enqueue_step();
+            b->advance(1);
+        }
+    })
+}
+
+int flp_batch_synchronize(flp_batch* b) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        int status = 0;
+        ckb(cudaMemcpy(&status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost), "copy");
+        if (status) {
+            ckb(cudaMemset(b->d_status, 0, sizeof(int)), "memset");
+            if (status & STATUS_NONFINITE) {
+                g_last_error = "non-finite mass in a world";
+                return FLP_ERR_NONFINITE;
+            }
+        }
+    })
+}
+
+int flp_batch_total_mass(flp_batch* b, double* per_world, int n) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (!per_world || n != b->n) throw std::invalid_argument("output needs one double per world");
+        k_batch_mass<<<b->n, 256, 0, b->st>>>(b->d_worlds, b->A[b->cur], b->d_mass);
+        ckb(cudaGetLastError(), "mass");
+        ckb(cudaMemcpyAsync(per_world, b->d_mass, n * sizeof(double), cudaMemcpyDeviceToHost, b->st), "copy");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+    })
+}
+
+int flp_batch_info(flp_batch* b, int* n_worlds, size_t* cell_channels, size_t* cells) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (n_worlds) *n_worlds = b->n;
+        if (cell_channels) *cell_channels = b->cells_total;
+        if (cells) {
+            size_t s = 0;
+            for (const auto& d : b->hw) s += size_t(d.W) * d.H;
+            *cells = s;
+        }
+    })
+}
+
+void* flp_batch_stream(flp_batch* b) { return b ? static_cast<void*>(b->st) : nullptr; }
+
+int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms, float* step_ms) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (steps < 0) throw std::invalid_argument("negative step count");
+        if (flush_l2 && !b->flush_buf) {
+            int dev = 0, l2 = 0;
+            ckb(cudaGetDevice(&dev), "device");
+            ckb(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "attr");
+            b->flush_bytes = std::max<size_t>(size_t(2) * size_t(l2), size_t(64) << 20);
+            ckb(cudaMalloc(&b->flush_buf, b->flush_bytes), "flush buffer");
+        }
+        double acc[NSTAGE] = {0}, tot = 0;
+        for (int s = 0; s < steps; ++s) {
+            if (flush_l2) ckb(cudaMemsetAsync(b->flush_buf, s & 0xFF, b->flush_bytes, b->st), "flush");
+            b->enqueue_step(true);
+            b->advance(1);
+            ckb(cudaEventSynchronize(b->ev[NSTAGE]), "sync");
+            for (int i = 0; i < NSTAGE; ++i) {
+                float ms = 0.f;
+                ckb(cudaEventElapsedTime(&ms, b->ev[i], b->ev[i + 1]), "elapsed");
+                acc[i] += ms;
+            }
+            float ms = 0.f;
+            ckb(cudaEventElapsedTime(&ms, b->ev[0], b->ev[NSTAGE]), "elapsed");
+            tot += ms;
+        }
+        if (stage_ms)
+            for (int i = 0; i < NSTAGE; ++i) stage_ms[i] = float(acc[i]);
+        if (step_ms) *step_ms = float(tot);
+    })
+}
+
+}  // extern "C"

@@ -28,6 +28,8 @@ struct FftGeom {
     const float2* twH = nullptr;  // exp(-2 pi i t / H),     t < H
 };
 
+bool make_plan(int L, FftPlan& p);
+
 // direct convolution + growth
 size_t conv_direct_smem_bytes(int rmax);
 void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, const float* taps, int W, int H, int C,

@@ -76,6 +76,35 @@ def patches_as_custom_seed(state: np.ndarray, width: int, height: int) -> dict:
     return {"pattern": {"type": "Custom", "values": vals}}
 
 
+BATCH_SIDES = (64, 96, 128, 192, 256, 384, 512)
+
+
+def batched_worlds(n=4096, sides=BATCH_SIDES, seed=DEFAULT_SEED):
+    """Independent 2D worlds for batched runs: width and height drawn
+    independently from `sides`, 1-2 channels, K = C*C kernels (every
+    source->target pair) with 1-2 rings of the multispecies distributions,
+    kernel_radius ~ U{8..20}, mu ~ U(0.1,0.3), sigma ~ U(0.01,0.05),
+    dt ~ U(0.1,0.3), weight ~ U(0.3,1); one Gaussian blob per channel with
+    radius ~ U(0.05,0.15).  Returns [(config, seed), ...]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        W = int(rng.choice(sides))
+        H = int(rng.choice(sides))
+        C = int(rng.integers(1, 3))
+        R = int(rng.integers(8, 21))
+        ks = []
+        for src in range(C):
+            for tgt in range(C):
+                ks.append(kernel(src, tgt, random_rings(rng, 1, 2), weight=float(rng.uniform(0.3, 1.0)),
+                                 mu=float(rng.uniform(0.1, 0.3)), sigma=float(rng.uniform(0.01, 0.05))))
+        cfg = config(W, H, C, ks, dt=float(rng.uniform(0.1, 0.3)), kernel_radius=R)
+        blobs = [{"center": [float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7))],
+                  "radius": float(rng.uniform(0.05, 0.15)), "amplitude": 1.0, "channel": c} for c in range(C)]
+        out.append((cfg, {"pattern": {"type": "MultiBlob", "blobs": blobs}}))
+    return out
+
+
 def sphere3d(size=128, R=10, mu=0.15, sigma=0.017, radius=0.12, dt=0.2):
     cfg = config(size, size, 1, [kernel(mu=mu, sigma=sigma)], dt=dt, kernel_radius=R, depth=size)
     seed = {"pattern": {"type": "GaussianSphere", "center": [0.5, 0.5, 0.5], "radius": radius, "amplitude": 1.0,

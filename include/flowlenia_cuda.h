@@ -144,6 +144,34 @@ FLP_API int flp_debug_affinity(flp_propagator* h, float* aff_out, size_t n);
  * mass sum, Sobel, flow, reintegration.  Writes the next state to out. */
 FLP_API int flp_debug_transport(flp_propagator* h, const float* state, const float* aff, float* out, size_t n);
 
+/* ---- Batched worlds ----------------------------------------------------
+ * Many independent 2D worlds of uneven sizes, channel counts and parameters,
+ * advanced together by persistent kernels that pull (world, tile) items from
+ * device work queues; replaces running one CpuPropagator per candidate as the
+ * reference's evolution search does (src/compute/evolution/search.rs:152-172,
+ * src/compute/evolution/fitness.rs:26-88).  Each world follows
+ * CpuPropagator::step (src/compute/propagator.rs:239-420) and gives the same
+ * bits as a single-world flp_propagator with the same config.  Widths must
+ * be even with W/2 in {16,24,32,48,64,96,128,192,256} and heights in
+ * {32,48,64,96,128,192,256,384,512}. */
+typedef struct flp_batch flp_batch;
+
+FLP_API int flp_batch_create(const char* const* config_jsons, int n_worlds, flp_batch** out);
+FLP_API int flp_batch_destroy(flp_batch* b);
+/* SimulationState::from_seed for one world (time and step reset to 0). */
+FLP_API int flp_batch_state_from_seed(flp_batch* b, int world, const char* seed_json);
+FLP_API int flp_batch_write_world(flp_batch* b, int world, const float* state, size_t n);
+FLP_API int flp_batch_read_world(flp_batch* b, int world, float* out, size_t n, float* time, uint64_t* step);
+/* CpuPropagator::run for every world at once; replays a captured CUDA graph. */
+FLP_API int flp_batch_run(flp_batch* b, uint64_t n);
+FLP_API int flp_batch_synchronize(flp_batch* b);
+/* FP64 compensated total mass of every world (n = number of worlds). */
+FLP_API int flp_batch_total_mass(flp_batch* b, double* per_world, int n);
+FLP_API int flp_batch_info(flp_batch* b, int* n_worlds, size_t* cell_channels, size_t* cells);
+FLP_API void* flp_batch_stream(flp_batch* b);
+/* As flp_profile_run: 5 stages (r2c, cols, c2r, flow, gather). */
+FLP_API int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms, float* step_ms);
+
 /* Allocation-free affinity.  No counterpart in the reference: an addition for
  * callers that may not allocate device memory, such as code enqueued from
  * another framework's plugin or custom operator on that framework's stream,
