@@ -77,7 +77,9 @@ static std::once_flag g_attr_once;
 static void set_attributes_once() {
     std::call_once(g_attr_once, [] {
         transport_2d_set_attributes();
+        transport_3d_set_attributes();
         fft2d_set_attributes(200 * 1024);
+        fft3d_set_attributes(200 * 1024);
     });
 }
 
@@ -107,6 +109,7 @@ struct flp_propagator {
     float* d_DX = nullptr;   // per-channel destinations and masses (C x N each)
     float* d_DY = nullptr;
     float* d_MS = nullptr;
+    float* d_DZ = nullptr;   // 3D only
     int* d_status = nullptr;
     double2* d_partial = nullptr;
     double* d_mass = nullptr;
@@ -146,7 +149,20 @@ struct flp_propagator {
             mark(0);
             return;
         }
-        if (conv_mode == FLP_CONV_DIRECT) {
+        if (dims == 3) {
+            // x rows are the D*H rows of the grid; spectra are [kx][z][y]
+            const int Wc = W / 2 + 1;
+            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, D * H, geom, reset_slot, 1, st);
+            mark(0);
+            launch_fft_lines(d_S, nullptr, d_S, nullptr, nsrc, Wc * D, H, geom, 1, 1.f, st);
+            mark(1);
+            launch_fft_z(d_S, d_KH, d_T, d_slot, K, W, H, D, geom.twD, 0, 1.f, st);
+            mark(2);
+            launch_fft_lines(d_T, nullptr, d_T, nullptr, K, Wc * D, H, geom, 2, 1.f, st);
+            mark(3);
+            launch_fft_c2r_growth(d_T, U, d_kd, K, W, D * H, C, geom, st);
+            mark(4);
+        } else if (conv_mode == FLP_CONV_DIRECT) {
             launch_conv_direct_2d(a, U, d_kd, K, d_taps, W, H, C, rmax, reset_slot, st);
             mark(0);
         } else {
@@ -160,6 +176,10 @@ struct flp_propagator {
     }
 
     std::vector<std::string> stage_names() const {
+        if (dims == 3) {
+            if (K == 0) return {"slot_reset", "flow_3d", "gather_3d"};
+            return {"fft_x_r2c", "fft_y_fwd", "fft_z_conv", "fft_y_inv", "fft_x_c2r_growth", "flow_3d", "gather_3d"};
+        }
         if (K == 0) return {"slot_reset", "flow_2d", "gather_2d"};
         if (conv_mode == FLP_CONV_DIRECT) return {"conv_direct_growth_2d", "flow_2d", "gather_2d"};
         return {"fft_rows_r2c", "fft_cols_conv", "fft_rows_c2r_growth", "flow_2d", "gather_2d"};
@@ -167,6 +187,13 @@ struct flp_propagator {
 
     void enqueue_transport(const float* a, float* an) {
         const int ns = int(stage_names().size());
+        if (dims == 3) {
+            launch_flow_3d(a, U, d_DX, d_DY, d_DZ, d_MS, C, W, H, D, fp, d_dmax, d_status, st);
+            mark(ns - 2);
+            launch_gather_3d(d_DX, d_DY, d_DZ, d_MS, an, C, W, H, D, fp, d_dmax, st);
+            mark(ns - 1);
+            return;
+        }
         launch_flow_2d(a, U, d_DX, d_DY, d_MS, C, W, H, fp, d_dmax, d_status, st);
         mark(ns - 2);
         launch_gather_2d(d_DX, d_DY, d_MS, an, C, W, H, fp, d_dmax, st);
@@ -190,7 +217,7 @@ struct flp_propagator {
     void free_all() {
         for (auto& g : graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-        void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_dmax, d_DX, d_DY, d_MS, d_status, d_partial, d_mass,
+        void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_dmax, d_DX, d_DY, d_MS, d_DZ, d_status, d_partial, d_mass,
                         d_tw, d_S, d_T, d_KH, d_srcs, d_slot};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -294,6 +321,65 @@ static void setup_fft(flp_propagator* h, const std::vector<KernelStencil>& ks) {
     h->fft_ok = true;
 }
 
+static void setup_fft3d(flp_propagator* h, const std::vector<KernelStencil>& ks) {
+    const int W = h->W, H = h->H, D = h->D;
+    h->fft_ok = false;
+    if (W % 2 != 0 || !fft_row_templated(W / 2) || !fft_col_templated(H) || !fft_z_templated(D))
+        throw FlpError(FLP_ERR_UNSUPPORTED,
+                       "3D worlds need an even width with W/2 in {16..256}, H in {32..512}, D in {32..256} (factors 2, 3)");
+    FftGeom g;
+    make_plan(W / 2, g.pm);
+    make_plan(H, g.ph);
+    const int M = W / 2, Wc = M + 1;
+    std::vector<float2> tw;
+    upload_twiddles(tw, M, M);
+    upload_twiddles(tw, W, Wc);
+    upload_twiddles(tw, H, H);
+    upload_twiddles(tw, D, D);
+    h->d_tw = dalloc<float2>(tw.size());
+    CK(cudaMemcpy(h->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    g.twM = h->d_tw;
+    g.twW = h->d_tw + M;
+    g.twH = h->d_tw + M + Wc;
+    g.twD = h->d_tw + M + Wc + H;
+    h->geom = g;
+    std::vector<int> srcs, slot(h->K);
+    for (int k = 0; k < h->K; ++k) {
+        auto it = std::find(srcs.begin(), srcs.end(), h->kd[k].src);
+        if (it == srcs.end()) { slot[k] = int(srcs.size()); srcs.push_back(h->kd[k].src); }
+        else slot[k] = int(it - srcs.begin());
+    }
+    h->nsrc = int(srcs.size());
+    h->d_srcs = dalloc<int>(srcs.size());
+    h->d_slot = dalloc<int>(slot.size());
+    if (!srcs.empty()) CK(cudaMemcpy(h->d_srcs, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!slot.empty()) CK(cudaMemcpy(h->d_slot, slot.data(), slot.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const size_t spec = size_t(Wc) * H * D;
+    h->d_S = dalloc<float2>(spec * std::max(h->nsrc, 1));
+    h->d_T = dalloc<float2>(spec * std::max(h->K, 1));
+    h->d_KH = dalloc<float2>(spec * std::max(h->K, 1));
+    if (h->K) {
+        // K^ = FFT3(wrap-padded stencil) / (W*H*D), in the [kx][z][y] layout
+        std::vector<float> padded(size_t(h->K) * W * H * D);
+        for (int k = 0; k < h->K; ++k) {
+            std::vector<float> p = pad_kernel(ks[k], W, H, D);
+            std::copy(p.begin(), p.end(), padded.begin() + size_t(k) * W * H * D);
+        }
+        float* d_pad = dalloc<float>(padded.size());
+        float2* d_tmp = dalloc<float2>(spec * h->K);
+        CK(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
+        launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, D * H, g, nullptr, 0, h->st);
+        launch_fft_lines(d_tmp, nullptr, d_tmp, nullptr, h->K, Wc * D, H, g, 1, 1.f, h->st);
+        launch_fft_z(d_tmp, nullptr, h->d_KH, nullptr, h->K, W, H, D, g.twD, 1,
+                     float(1.0 / (double(W) * double(H) * double(D))), h->st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->st));
+        cudaFree(d_pad);
+        cudaFree(d_tmp);
+    }
+    h->fft_ok = true;
+}
+
 static float time_conv(flp_propagator* h, int mode, int reps) {
     int saved = h->conv_mode;
     h->conv_mode = mode;
@@ -341,8 +427,11 @@ static FlowParams make_flow_params(const SimulationConfig& cfg) {
     FlowParams fp{};
     fp.dt = cfg.dt;
     fp.s = cfg.flow.distribution_size;
+    // Square area (2s)^2 in 2D (reintegration.rs:117); cube volume (2s)^3 in
+    // 3D (reintegration3d.rs:137), both evaluated left to right in f32.
     float two_s = 2.0f * fp.s;
     fp.total_area = two_s * two_s;
+    if (cfg.is_3d()) fp.total_area = fp.total_area * two_s;
     int e = 0;
     float mant = std::frexp(fp.total_area, &e);
     fp.area_pow2 = (fp.total_area > 0.f && mant == 0.5f && std::isnormal(fp.total_area)) ? 1 : 0;
@@ -371,7 +460,6 @@ static FlowParams make_flow_params(const SimulationConfig& cfg) {
 static void create(const std::string& json, flp_propagator* h) {
     h->cfg = parse_config(json);
     const SimulationConfig& c = h->cfg;
-    if (c.is_3d()) throw FlpError(FLP_ERR_UNSUPPORTED, "3D worlds are served by the 3D engine");
     h->W = c.width; h->H = c.height; h->D = c.depth; h->C = c.channels; h->K = int(c.kernels.size());
     h->dims = c.is_3d() ? 3 : 2;
     h->N = c.grid_size();
@@ -390,6 +478,7 @@ static void create(const std::string& json, flp_propagator* h) {
     h->d_DX = dalloc<float>(CN);
     h->d_DY = dalloc<float>(CN);
     h->d_MS = dalloc<float>(CN);
+    if (h->dims == 3) h->d_DZ = dalloc<float>(CN);
     h->d_status = dalloc<int>(1);
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
     h->np = 256;
@@ -410,10 +499,16 @@ static void create(const std::string& json, flp_propagator* h) {
         d.inv2s2 = 1.0f / sigma_sq_2;
         h->kd[k] = d;
     }
-    setup_direct(h, ks);
+    if (h->dims == 2) {
+        setup_direct(h, ks);
+    } else {
+        for (int k = 0; k < h->K; ++k) h->kd[k].r = ks[k].radius;
+        h->direct_ok = false;  // 3D convolves through the FFT path only
+    }
     h->d_kd = dalloc<KDesc>(h->kd.size());
     if (h->K) CK(cudaMemcpy(h->d_kd, h->kd.data(), h->kd.size() * sizeof(KDesc), cudaMemcpyHostToDevice));
-    setup_fft(h, ks);
+    if (h->dims == 2) setup_fft(h, ks);
+    else setup_fft3d(h, ks);
     h->fp = make_flow_params(c);
     CK(cudaStreamSynchronize(h->st));
     resolve_conv_mode(h, FLP_CONV_AUTO);
@@ -759,7 +854,8 @@ int flp_debug_transport(flp_propagator* h, const float* state, const float* aff,
     FLP_TRY({
         const size_t CN = size_t(h->C) * h->N;
         if (!state || !aff || !out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "size mismatch");
-        // The handle's own scratch planes are reused; the live state is untouched.
+        // The handle's own scratch planes are reused; the live state is untouched
+        // (3D worlds go through the same entry: enqueue_transport dispatches).
         float* a = dalloc<float>(CN);
         float* o = dalloc<float>(CN);
         try {

@@ -360,20 +360,24 @@ void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W,
                                                                     reset_slot, nreset);
 }
 
-void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
-                     const FftGeom& g, int mode, float scale, cudaStream_t st) {
-    int Wc = W / 2 + 1;
-#define X(n)                                                                                              \
-    if (H == n) {                                                                                         \
-        dim3 grid((Wc + ColCfg<n>::NC - 1) / ColCfg<n>::NC, K);                                           \
-        k_cols_t<n><<<grid, 256, ColCfg<n>::smem, st>>>(S, KH, T, slot_of_kernel, Wc, mode, scale, g.twH); \
-        return;                                                                                           \
+void launch_fft_lines(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int nlines,
+                      int H, const FftGeom& g, int mode, float scale, cudaStream_t st) {
+#define X(n)                                                                                                   \
+    if (H == n) {                                                                                              \
+        dim3 grid((nlines + ColCfg<n>::NC - 1) / ColCfg<n>::NC, K);                                            \
+        k_cols_t<n><<<grid, 256, ColCfg<n>::smem, st>>>(S, KH, T, slot_of_kernel, nlines, mode, scale, g.twH); \
+        return;                                                                                                \
     }
     FLP_COL_SIZES(X)
 #undef X
-    dim3 grid((Wc + g.NC - 1) / g.NC, K);
-    fft_cols_conv<<<grid, 256, fft_cols_smem(H, g.NC), st>>>(S, KH, T, slot_of_kernel, Wc, H, g.NC, g.ph, g.twH,
+    dim3 grid((nlines + g.NC - 1) / g.NC, K);
+    fft_cols_conv<<<grid, 256, fft_cols_smem(H, g.NC), st>>>(S, KH, T, slot_of_kernel, nlines, H, g.NC, g.ph, g.twH,
                                                               mode, scale);
+}
+
+void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
+                     const FftGeom& g, int mode, float scale, cudaStream_t st) {
+    launch_fft_lines(S, KH, T, slot_of_kernel, K, W / 2 + 1, H, g, mode, scale, st);
 }
 
 void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,

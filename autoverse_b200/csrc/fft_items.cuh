@@ -233,7 +233,8 @@ __device__ void r2c_rows_item(float2* sm, const float* __restrict__ x, float2* _
 }
 
 // nl (<= NC) contiguous columns of length H: forward FFT, then either scale
-// (mode 1) or multiply by the kernel spectrum and inverse FFT (mode 0).
+// (mode 1) or multiply by the kernel spectrum and inverse FFT (mode 0); mode 2
+// is the inverse FFT alone.
 template <int H>
 __device__ void cols_conv_item(float2* sm, const float2* __restrict__ src, const float2* __restrict__ kh,
                                float2* __restrict__ dst, int nl, int mode, float scale,
@@ -250,6 +251,16 @@ __device__ void cols_conv_item(float2* sm, const float2* __restrict__ src, const
         a[l * LS + pad8(y)] = l < nl ? src[i] : make_float2(0.f, 0.f);
     }
     __syncthreads();
+    if (mode == 2) {
+        float2* R2 = ct_fft<H, NC, true>(a, b, twH);
+#pragma unroll 4
+        for (int i = tid; i < nl * H; i += 256) {
+            const int l = i / H, y = i - l * H;
+            dst[i] = R2[l * LS + pad8(y)];
+        }
+        __syncthreads();
+        return;
+    }
     float2* F = ct_fft<H, NC, false>(a, b, twH);
     float2* G = (F == a) ? b : a;
     if (mode == 1) {
@@ -273,6 +284,64 @@ __device__ void cols_conv_item(float2* sm, const float2* __restrict__ src, const
     for (int i = tid; i < nl * H; i += 256) {
         const int l = i / H, y = i - l * H;
         dst[i] = R[l * LS + pad8(y)];
+    }
+    __syncthreads();
+}
+
+// Lines along z of a [z][y] block (element (z, y) at z*H + y): NZ adjacent
+// y's starting at y0 (ny of them valid), each a line of D points.  mode 0:
+// forward FFT, multiply by the kernel spectrum (same layout), inverse FFT;
+// mode 1: forward FFT scaled.  Loads and stores move NZ contiguous complex
+// values per z.
+template <int D>
+struct ZCfg {
+    static constexpr int NZ = D >= 512 ? 4 : (2048 / D);
+    static constexpr int LS = CtPlan<D>::LS;
+    static constexpr size_t buf = size_t(NZ) * LS;
+    static constexpr size_t smem = sizeof(float2) * (D + 2 * buf);
+};
+
+template <int D>
+__device__ void zconv_item(float2* sm, const float2* __restrict__ src, const float2* __restrict__ kh,
+                           float2* __restrict__ dst, int H, int y0, int ny, int mode, float scale,
+                           const float2* __restrict__ twD_g) {
+    constexpr int NZ = ZCfg<D>::NZ, LS = ZCfg<D>::LS;
+    float2* twD = sm;
+    float2* a = twD + D;
+    float2* b = a + ZCfg<D>::buf;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < D; i += 256) twD[i] = twD_g[i];
+#pragma unroll 4
+    for (int i = tid; i < NZ * D; i += 256) {
+        const int z = i / NZ, l = i - z * NZ;
+        a[l * LS + pad8(z)] = l < ny ? src[size_t(z) * H + y0 + l] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* F = ct_fft<D, NZ, false>(a, b, twD);
+    float2* G = (F == a) ? b : a;
+    if (mode == 1) {
+        for (int i = tid; i < NZ * D; i += 256) {
+            const int z = i / NZ, l = i - z * NZ;
+            if (l < ny) {
+                const float2 f = F[l * LS + pad8(z)];
+                dst[size_t(z) * H + y0 + l] = make_float2(f.x * scale, f.y * scale);
+            }
+        }
+        __syncthreads();
+        return;
+    }
+#pragma unroll 4
+    for (int i = tid; i < NZ * D; i += 256) {
+        const int z = i / NZ, l = i - z * NZ;
+        float2& f = F[l * LS + pad8(z)];
+        f = l < ny ? cmul(f, kh[size_t(z) * H + y0 + l]) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* R = ct_fft<D, NZ, true>(F, G, twD);
+#pragma unroll 4
+    for (int i = tid; i < NZ * D; i += 256) {
+        const int z = i / NZ, l = i - z * NZ;
+        if (l < ny) dst[size_t(z) * H + y0 + l] = R[l * LS + pad8(z)];
     }
     __syncthreads();
 }

@@ -26,6 +26,7 @@ struct FftGeom {
     const float2* twM = nullptr;  // exp(-2 pi i t / (W/2)), t < W/2
     const float2* twW = nullptr;  // exp(-2 pi i t / W),     t <= W/2
     const float2* twH = nullptr;  // exp(-2 pi i t / H),     t < H
+    const float2* twD = nullptr;  // exp(-2 pi i t / D),     t < D (3D only)
 };
 
 bool make_plan(int L, FftPlan& p);
@@ -56,7 +57,26 @@ void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W,
                     int* reset_slot, int nreset, cudaStream_t st);
 void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
                      const FftGeom& g, int mode, float scale, cudaStream_t st);
+void launch_fft_lines(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int nlines,
+                      int H, const FftGeom& g, int mode, float scale, cudaStream_t st);
 void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,
                            cudaStream_t st);
+
+// 3D FFT path: z-axis pass (the x and y passes reuse the 2D row and column passes)
+bool fft_row_templated(int M);
+bool fft_col_templated(int H);
+bool fft_z_templated(int D);
+void fft3d_set_attributes(size_t max_bytes);
+void launch_fft_z(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int nlines_k, int W, int H,
+                  int D, const float2* twD, int mode, float scale, cudaStream_t st);
+
+// 3D transport
+size_t flow3d_smem_bytes(int C);
+size_t gather3d_smem_bytes();
+void transport_3d_set_attributes();
+void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
+                    int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st);
+void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
+                      int H, int D, const FlowParams& fp, const int* dmax_slot, cudaStream_t st);
 
 }  // namespace flp

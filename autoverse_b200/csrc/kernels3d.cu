@@ -1,0 +1,304 @@
+// 3D transport kernels (replace CpuPropagator3D::step's stencil and
+// reintegration, src/compute/propagator3d.rs:181-256):
+//   * flow_3d — channel sum, the 3x3x3 Sobel of the sum and of U_c in the
+//     reference's evaluation order (gradient3d.rs:106-138), alpha, the flow
+//     F = (1-a) grad U - a grad A (flow3d.rs:64-72) and dest = x + dt*F
+//     (reintegration3d.rs:82-84), one thread per cell;
+//   * gather_3d — cube reintegration in gather form (reintegration3d.rs:109-198):
+//     each destination sums the overlap volumes of the sources in the window
+//     [-RN, RN+1]^3 in the reference's deposit order (z, then y, then x over
+//     wrapped source indices), bit-identical to the reference's scatter.
+#include "common.cuh"
+#include "kernels.h"
+#include "transport_items.cuh"
+
+namespace flp {
+
+// ------------------------------------------------------------- flow_3d ----
+constexpr int F3_W = 32, F3_H = 8;
+constexpr int F3_RW = F3_W + 2, F3_RH = F3_H + 2, F3_PL = F3_RW * F3_RH, F3_RC = 3 * F3_PL;
+
+size_t flow3d_smem_bytes(int C) { return sizeof(float) * (size_t(2 * C + 1) * F3_RC); }
+
+// 3D Sobel of a field at the centre of a 3x3x3 window w[z][y][x] (region
+// indices), gradient3d.rs:106-138: each line sum (a + 2b) + c, each gradient
+// ((l_m + 2 l_0) + l_p) / 32, all in f32 without contraction.
+struct Win3 {
+    const float* p;  // element (dz, dy, dx) at p[dz*F3_PL + dy*F3_RW + dx], dz,dy,dx in 0..2
+    __device__ float at(int z, int y, int x) const { return p[z * F3_PL + y * F3_RW + x]; }
+};
+__device__ __forceinline__ float line3(float a, float b, float c) { return __fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, b)), c); }
+__device__ __forceinline__ float diff3(float lm, float lp) { return __fadd_rn(-lm, lp); }
+__device__ __forceinline__ float comb3(float m, float z, float p) {
+    return __fmul_rn(__fadd_rn(__fadd_rn(m, __fmul_rn(2.0f, z)), p), 0.03125f);
+}
+__device__ __forceinline__ void sobel3(const Win3& w, float& gx, float& gy, float& gz) {
+    // x gradient: for each z layer, -(column x-1 over y) + (column x+1 over y)
+    float l[3];
+    for (int z = 0; z < 3; ++z)
+        l[z] = diff3(line3(w.at(z, 0, 0), w.at(z, 1, 0), w.at(z, 2, 0)), line3(w.at(z, 0, 2), w.at(z, 1, 2), w.at(z, 2, 2)));
+    gx = comb3(l[0], l[1], l[2]);
+    // y gradient: for each z layer, -(row y-1 over x) + (row y+1 over x)
+    for (int z = 0; z < 3; ++z)
+        l[z] = diff3(line3(w.at(z, 0, 0), w.at(z, 0, 1), w.at(z, 0, 2)), line3(w.at(z, 2, 0), w.at(z, 2, 1), w.at(z, 2, 2)));
+    gy = comb3(l[0], l[1], l[2]);
+    // z gradient: for each x column, -(layer z-1 over y) + (layer z+1 over y)
+    for (int x = 0; x < 3; ++x)
+        l[x] = diff3(line3(w.at(0, 0, x), w.at(0, 1, x), w.at(0, 2, x)), line3(w.at(2, 0, x), w.at(2, 1, x), w.at(2, 2, x)));
+    gz = comb3(l[0], l[1], l[2]);
+}
+
+template <bool POW2>
+__global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, const float* __restrict__ U,
+                                               float* __restrict__ DX, float* __restrict__ DY,
+                                               float* __restrict__ DZ, float* __restrict__ MS, int C, int W, int H,
+                                               int D, FlowParams fp, int* dmax_slot, int* status) {
+    extern __shared__ __align__(16) float sm[];
+    float* as = sm;                    // C staged A blocks (3 planes each)
+    float* us = sm + C * F3_RC;        // C staged U blocks
+    float* asum = sm + 2 * C * F3_RC;  // channel sum
+    __shared__ int colx[F3_RW], rowy[F3_RH], plz[3];
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * F3_W, y0 = blockIdx.y * F3_H, z = blockIdx.z;
+    const size_t N = size_t(W) * H * D;
+    if (tid < F3_RW) colx[tid] = wrap_near(x0 - 1 + tid, W);
+    else if (tid < F3_RW + F3_RH) rowy[tid - F3_RW] = wrap_near(y0 - 1 + (tid - F3_RW), H);
+    else if (tid < F3_RW + F3_RH + 3) plz[tid - F3_RW - F3_RH] = wrap_near(z - 1 + (tid - F3_RW - F3_RH), D);
+    __syncthreads();
+    for (int i = tid; i < 2 * C * F3_RC; i += 256) {
+        const int k = i / F3_RC, cell = i - k * F3_RC;
+        const int pz = cell / F3_PL, r = cell - pz * F3_PL;
+        const int ly = r / F3_RW, lx = r - ly * F3_RW;
+        const size_t idx = (size_t(plz[pz]) * H + rowy[ly]) * W + colx[lx];
+        cp_async4(sm + i, (k < C ? A + size_t(k) * N : U + size_t(k - C) * N) + idx);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = tid; i < F3_RC; i += 256) {
+        float a = 0.f;
+        for (int k = 0; k < C; ++k) a = __fadd_rn(a, as[k * F3_RC + i]);
+        asum[i] = a;
+    }
+    __syncthreads();
+    const int lx = tid & (F3_W - 1), ly = tid / F3_W;
+    const int X = x0 + lx, Y = y0 + ly;
+    float dmax = 0.f;
+    bool bad = false;
+    if (X < W && Y < H) {
+        const int o = ly * F3_RW + lx;  // (0,0,0) corner of the window
+        float gax, gay, gaz;
+        sobel3(Win3{asum + o}, gax, gay, gaz);
+        const float alpha = alpha_fp(asum[F3_PL + o + F3_RW + 1], fp);
+        const float oma = __fsub_rn(1.0f, alpha);
+        const float agx = __fmul_rn(alpha, gax), agy = __fmul_rn(alpha, gay), agz = __fmul_rn(alpha, gaz);
+        const size_t cell = (size_t(z) * H + Y) * W + X;
+        for (int c = 0; c < C; ++c) {
+            float gux, guy, guz;
+            sobel3(Win3{us + c * F3_RC + o}, gux, guy, guz);
+            const float fx = __fsub_rn(__fmul_rn(oma, gux), agx);
+            const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
+            const float fz = __fsub_rn(__fmul_rn(oma, guz), agz);
+            const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
+            const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
+            const float dz = __fadd_rn(float(z), __fmul_rn(fp.dt, fz));
+            float mass = as[c * F3_RC + F3_PL + o + F3_RW + 1];
+            bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy) && isfinite(dz));
+            if (fabsf(mass) < 1e-10f) mass = 0.f;
+            if (mass != 0.f)
+                dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fmaxf(fabsf(dy - float(Y)), fabsf(dz - float(z)))));
+            DX[size_t(c) * N + cell] = dx;
+            DY[size_t(c) * N + cell] = dy;
+            DZ[size_t(c) * N + cell] = dz;
+            MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
+        }
+    }
+    if (status && __syncthreads_or(bad ? 1 : 0) && tid == 0) atomicOr(status, STATUS_NONFINITE);
+    block_max_atomic(dmax, bad, dmax_slot);
+}
+
+// ----------------------------------------------------------- gather_3d ----
+constexpr int G3_W = 32, G3_H = 8, G3_RNMAX = 2;
+constexpr int G3_SW = G3_W + 2 * G3_RNMAX + 1, G3_SH = G3_H + 2 * G3_RNMAX + 1, G3_SD = 2 * G3_RNMAX + 2;
+constexpr int G3_CELLS = G3_SW * G3_SH * G3_SD;
+
+size_t gather3d_smem_bytes() { return sizeof(float) * 4 * G3_CELLS; }
+
+// Overlap of one source cube with cell (ix, iy, iz): reintegration3d.rs:155-185.
+template <bool POW2>
+__device__ __forceinline__ float cube_term(float m, float dx, float dy, float dz, int ix, int iy, int iz,
+                                           const FlowParams& fp) {
+    const float s = fp.s;
+    const float ox0 = fmaxf(float(ix), __fsub_rn(dx, s)), ox1 = fminf(float(ix + 1), __fadd_rn(dx, s));
+    const float oy0 = fmaxf(float(iy), __fsub_rn(dy, s)), oy1 = fminf(float(iy + 1), __fadd_rn(dy, s));
+    const float oz0 = fmaxf(float(iz), __fsub_rn(dz, s)), oz1 = fminf(float(iz + 1), __fadd_rn(dz, s));
+    const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
+    const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
+    const float od = fmaxf(__fsub_rn(oz1, oz0), 0.f);
+    const float vol = __fmul_rn(__fmul_rn(ow, oh), od);
+    if (POW2) return __fmul_rn(m, vol);  // m holds mass / total_volume (exact); a zero volume adds a signed zero
+    if (!(vol > 0.f)) return 0.f;
+    return __fmul_rn(m, __fdiv_rn(vol, fp.total_area));
+}
+
+// Offsets k in the window [-RN, RN+1] (NW = 2RN+2 of them) in the order that
+// makes the wrapped coordinates (c + k) mod size ascend; valid when NW <= size.
+__device__ __forceinline__ int rot_window(int j, int c, int RN, int size) {
+    const int NW = 2 * RN + 2;
+    const int n_hi = max(0, c + RN + 2 - size);  // k with c + k >= size
+    const int n_lo = max(0, RN - c);             // k with c + k < 0
+    if (j < n_hi) return RN + 2 - n_hi + j;
+    if (j < NW - n_lo) return -RN + n_lo + (j - n_hi);
+    return -RN + (j - (NW - n_lo));
+}
+
+// One 32x8 block of destinations in plane Z of one channel.
+template <int RN, bool POW2>
+__device__ void gather3d_plane(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
+                               const float* __restrict__ DZ, const float* __restrict__ MS, float* __restrict__ out,
+                               int W, int H, int D, int Z, const FlowParams& fp) {
+    constexpr int SW = G3_W + 2 * RN + 1, SH = G3_H + 2 * RN + 1, SD = 2 * RN + 2, PL = SW * SH, NC = PL * SD;
+    float* sx = sm;
+    float* sy = sx + NC;
+    float* sz = sy + NC;
+    float* smm = sz + NC;
+    __shared__ int colx[G3_SW], rowy[G3_SH], plz[G3_SD];
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * G3_W, y0 = blockIdx.y * G3_H;
+    if (tid < SW) colx[tid] = wrap_near(x0 - RN + tid, W);
+    else if (tid < SW + SH) rowy[tid - SW] = wrap_near(y0 - RN + (tid - SW), H);
+    else if (tid < SW + SH + SD) plz[tid - SW - SH] = wrap_near(Z - RN + (tid - SW - SH), D);
+    __syncthreads();
+    for (int i = tid; i < 4 * NC; i += 256) {
+        const int k = i / NC, cell = i - k * NC;
+        const int pz = cell / PL, r = cell - pz * PL;
+        const int ly = r / SW, lx = r - ly * SW;
+        const size_t idx = (size_t(plz[pz]) * H + rowy[ly]) * W + colx[lx];
+        const float* src = k == 0 ? DX : (k == 1 ? DY : (k == 2 ? DZ : MS));
+        cp_async4(sm + i, src + idx);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lx = tid & (G3_W - 1), ly = tid / G3_W;
+    const int X = x0 + lx, Y = y0 + ly;
+    if (X >= W || Y >= H) return;
+    float acc = 0.f;
+    // Offsets k = source - destination in [-RN, RN+1] per axis, visited so the
+    // wrapped source indices ascend (z outer, then y, then x).
+    constexpr int NW = 2 * RN + 2;
+    for (int jz = 0; jz < NW; ++jz) {
+        const int kz = rot_window(jz, Z, RN, D);
+        const int gz = Z + kz;
+        const int iz = Z + (gz < 0 ? D : (gz >= D ? -D : 0));
+        for (int jy = 0; jy < NW; ++jy) {
+            const int ky = rot_window(jy, Y, RN, H);
+            const int gy = Y + ky;
+            const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
+            const int rowbase = (kz + RN) * PL + (ly + ky + RN) * SW;
+#pragma unroll
+            for (int jx = 0; jx < NW; ++jx) {
+                const int kx = rot_window(jx, X, RN, W);
+                const int gx = X + kx;
+                const int ix = X + (gx < 0 ? W : (gx >= W ? -W : 0));
+                const int o = rowbase + lx + kx + RN;
+                const float m = smm[o];
+                if (!POW2 && m == 0.f) continue;
+                acc = __fadd_rn(acc, cube_term<POW2>(m, sx[o], sy[o], sz[o], ix, iy, iz, fp));
+            }
+        }
+    }
+    out[(size_t(Z) * H + Y) * W + X] = acc;
+}
+
+// Generic per-destination gather from global memory for any window; also the
+// nearest-cell mode and the reference's [-W, 2W] cell clamps.
+template <bool POW2>
+__device__ float gather3d_generic(const float* __restrict__ DX, const float* __restrict__ DY,
+                                  const float* __restrict__ DZ, const float* __restrict__ MS, int W, int H, int D,
+                                  int X, int Y, int Z, int R, const FlowParams& fp) {
+    float acc = 0.f;
+    for (int jz = 0; jz <= 2 * R; ++jz) {
+        const int kz = rotated_offset(jz, Z, R, D);
+        const int zw = wrap_coord(Z + kz, D), iz = zw - kz;
+        for (int jy = 0; jy <= 2 * R; ++jy) {
+            const int ky = rotated_offset(jy, Y, R, H);
+            const int yw = wrap_coord(Y + ky, H), iy = yw - ky;
+            for (int jx = 0; jx <= 2 * R; ++jx) {
+                const int kx = rotated_offset(jx, X, R, W);
+                const int xw = wrap_coord(X + kx, W), ix = xw - kx;
+                const size_t src = (size_t(zw) * H + yw) * W + xw;
+                const float m = MS[src];
+                if (m == 0.f) continue;
+                const float dx = DX[src], dy = DY[src], dz = DZ[src];
+                if (fp.point_mode) {
+                    if (f2i_sat(roundf(dx)) == ix && f2i_sat(roundf(dy)) == iy && f2i_sat(roundf(dz)) == iz)
+                        acc = __fadd_rn(acc, m);
+                    continue;
+                }
+                const float s = fp.s;
+                const int ix_lo = max(f2i_sat(floorf(__fsub_rn(dx, s))), -W), ix_hi = min(f2i_sat(ceilf(__fadd_rn(dx, s))), 2 * W);
+                const int iy_lo = max(f2i_sat(floorf(__fsub_rn(dy, s))), -H), iy_hi = min(f2i_sat(ceilf(__fadd_rn(dy, s))), 2 * H);
+                const int iz_lo = max(f2i_sat(floorf(__fsub_rn(dz, s))), -D), iz_hi = min(f2i_sat(ceilf(__fadd_rn(dz, s))), 2 * D);
+                if (ix < ix_lo || ix > ix_hi || iy < iy_lo || iy > iy_hi || iz < iz_lo || iz > iz_hi) continue;
+                const float t = cube_term<POW2>(m, dx, dy, dz, ix, iy, iz, fp);
+                if (t != 0.f) acc = __fadd_rn(acc, t);
+            }
+        }
+    }
+    return acc;
+}
+
+template <bool POW2>
+__global__ void __launch_bounds__(256) gather_3d(const float* __restrict__ DX, const float* __restrict__ DY,
+                                                 const float* __restrict__ DZ, const float* __restrict__ MS,
+                                                 float* __restrict__ Anext, int C, int W, int H, int D, FlowParams fp,
+                                                 const int* __restrict__ dmax_slot) {
+    extern __shared__ __align__(16) float sm[];
+    const int c = blockIdx.z / D;
+    const int Z = blockIdx.z - c * D;
+    const size_t N = size_t(W) * H * D, off = size_t(c) * N;
+    const int RN = window_from_dmax(*dmax_slot, fp, max(max(W, H), D));
+    const bool fast = RN <= G3_RNMAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && 2 * RN + 2 <= D && !fp.point_mode;
+    if (fast) {
+        switch (RN) {
+            case 0: gather3d_plane<0, POW2>(sm, DX + off, DY + off, DZ + off, MS + off, Anext + off, W, H, D, Z, fp); break;
+            case 1: gather3d_plane<1, POW2>(sm, DX + off, DY + off, DZ + off, MS + off, Anext + off, W, H, D, Z, fp); break;
+            default: gather3d_plane<2, POW2>(sm, DX + off, DY + off, DZ + off, MS + off, Anext + off, W, H, D, Z, fp); break;
+        }
+        return;
+    }
+    const int X = blockIdx.x * G3_W + (threadIdx.x & (G3_W - 1)), Y = blockIdx.y * G3_H + (threadIdx.x / G3_W);
+    if (X < W && Y < H)
+        Anext[off + (size_t(Z) * H + Y) * W + X] =
+            gather3d_generic<POW2>(DX + off, DY + off, DZ + off, MS + off, W, H, D, X, Y, Z, RN + 1, fp);
+}
+
+void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
+                    int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
+    dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, D);
+    if (fp.area_pow2)
+        flow_3d<true><<<grid, 256, flow3d_smem_bytes(C), st>>>(A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+    else
+        flow_3d<false><<<grid, 256, flow3d_smem_bytes(C), st>>>(A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+}
+
+void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
+                      int H, int D, const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
+    dim3 grid((W + G3_W - 1) / G3_W, (H + G3_H - 1) / G3_H, C * D);
+    if (fp.area_pow2)
+        gather_3d<true><<<grid, 256, gather3d_smem_bytes(), st>>>(DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
+    else
+        gather_3d<false><<<grid, 256, gather3d_smem_bytes(), st>>>(DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
+}
+
+void transport_3d_set_attributes() {
+    auto set = [](const void* f, size_t bytes) {
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    };
+    set((const void*)flow_3d<true>, flow3d_smem_bytes(32));
+    set((const void*)flow_3d<false>, flow3d_smem_bytes(32));
+    set((const void*)gather_3d<true>, gather3d_smem_bytes());
+    set((const void*)gather_3d<false>, gather3d_smem_bytes());
+}
+
+}  // namespace flp

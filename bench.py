@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline (profiling runs)")
     ap.add_argument("--conv", choices=["auto", "direct", "fft"], default="auto",
                     help="convolution path (auto = the engine's measured choice)")
+    ap.add_argument("--batch-worlds", type=int, default=4096, help="worlds in the batched measurement (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -198,6 +200,67 @@ def cpu_reference_run(cfg, state, seconds: float, max_steps: int, warmup: int = 
     return n, dt, threads
 
 
+def measure_batched(args, dist):
+    """Batched worlds: `--batch-worlds` independent worlds (sides from
+    {64..512} per axis, 1-2 channels, K = C*C, radius 8..20, per-world growth
+    and flow parameters), timed as one persistent-kernel step loop; plus the
+    batched/plain ratio on 1024 small uneven worlds (sides 64..128), plain
+    being one device-resident propagator per world stepped in turn."""
+    import autoverse_b200 as fl
+    from autoverse_b200 import workloads as wl
+    worlds = wl.batched_worlds(args.batch_worlds, seed=wl.DEFAULT_SEED + RANK)
+    b = fl.BatchedPropagator([c for c, _ in worlds])
+    for i, (_, sd) in enumerate(worlds):
+        b.load_seed(i, sd)
+    info = b.info()
+    b.profile_run(3, flush_l2=False)
+    if dist:
+        dist.barrier()
+    prof = b.profile_run(args.batch_steps, flush_l2=False)
+    b.synchronize()
+    t = reduce_max(dist, prof["step_ms"] / 1e3)
+    out = {"workload": f"{args.batch_worlds} worlds, sides {{64..512}} per axis, C in {{1,2}}, K=C*C, R~U{{8..20}}, "
+                       "mu~U(0.1,0.3), sigma~U(0.01,0.05), dt~U(0.1,0.3), Gaussian-blob seeds",
+           "cells_per_gpu": info["cells"], "cell_channels_per_gpu": info["cell_channels"], "steps": args.batch_steps,
+           "value": WORLD * info["cells"] * args.batch_steps / t, "unit": "cell-steps/s",
+           "ms_per_step": 1e3 * t / args.batch_steps,
+           "stage_ms_per_step": {k: v / args.batch_steps for k, v in prof["stages"].items()},
+           "gpu_launches_per_step": 1 + 3 * 7 + 2, "l2": "working set above L2 (pooled state and spectra)"}
+    b.close()
+    # batched vs plain on small uneven worlds
+    small = wl.batched_worlds(1024, sides=(64, 96, 128), seed=wl.DEFAULT_SEED + 17)
+    b = fl.BatchedPropagator([c for c, _ in small])
+    for i, (_, sd) in enumerate(small):
+        b.load_seed(i, sd)
+    b.profile_run(3, flush_l2=False)
+    steps = 40
+    pb = b.profile_run(steps, flush_l2=False)
+    v_b = b.info()["cells"] * steps / (pb["step_ms"] / 1e3)
+    b.close()
+    props = []
+    for cfg, sd in small[:48]:
+        p = fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT)
+        p.load_seed(sd)
+        p.run_device(16)
+        props.append(p)
+    for p in props:
+        p.synchronize()
+    t0 = time.perf_counter()
+    for p in props:
+        p.run_device(steps)
+    for p in props:
+        p.synchronize()
+    t_plain = time.perf_counter() - t0
+    v_p = sum(c["width"] * c["height"] for c, _ in small[:48]) * steps / t_plain
+    for p in props:
+        p.close()
+    out["small_worlds_batched_over_plain"] = {
+        "batched": v_b, "plain": v_p, "ratio": v_b / v_p,
+        "workload": "1024 worlds with sides {64,96,128} per axis (plain: 48 of them, one propagator each, "
+                    "graph-replayed, stepped in turn; host wall time around device-synchronised runs)"}
+    return out
+
+
 def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
@@ -277,6 +340,8 @@ def main():
     e2e_t = reduce_max(dist, time.perf_counter() - t0)
     e2e_value = WORLD * cells * args.e2e_steps / e2e_t
 
+    batched = measure_batched(args, dist) if args.batch_worlds > 0 else None
+
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
         n, dt, threads = cpu_reference_run(cfg, state, args.cpu_seconds, 200)
@@ -305,6 +370,7 @@ def main():
         "gpu_launches": prof["launches_per_step"] * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "batched": batched,
     }
     print(json.dumps(line), flush=True)
 
