@@ -125,6 +125,7 @@ struct flp_propagator {
     int* d_slot = nullptr;
     int nsrc = 0;
     int conv_mode = FLP_CONV_DIRECT;
+    bool conv_pending = true;  // the autotuner runs before the first convolution unless a mode is set first
     float time = 0.f;
     uint64_t step = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -511,7 +512,14 @@ static void create(const std::string& json, flp_propagator* h) {
     else setup_fft3d(h, ks);
     h->fp = make_flow_params(c);
     CK(cudaStreamSynchronize(h->st));
+    h->conv_pending = true;
+}
+
+// Runs the direct-vs-FFT autotuner on first use, outside any graph capture.
+static void ensure_conv_mode(flp_propagator* h) {
+    if (!h->conv_pending) return;
     resolve_conv_mode(h, FLP_CONV_AUTO);
+    h->conv_pending = false;
 }
 
 static void upload_state(flp_propagator* h, const float* src, size_t n) {
@@ -544,6 +552,7 @@ static void build_graph(flp_propagator* h) {
 }
 
 static void run_steps(flp_propagator* h, uint64_t n) {
+    ensure_conv_mode(h);
     while (n >= uint64_t(GRAPH_STEPS)) {
         if (!h->graph[h->cur]) build_graph(h);
         CK(cudaGraphLaunch(h->graph[h->cur], h->st));
@@ -718,6 +727,7 @@ int flp_read_state(flp_propagator* h, float* out, size_t n, float* time, uint64_
 int flp_step(flp_propagator* h) {
     FLP_CHECK_HANDLE(h);
     FLP_TRY({
+        ensure_conv_mode(h);
         h->enqueue_step();
         h->advance_clock(1);
     })
@@ -776,6 +786,7 @@ int flp_get_info(flp_propagator* h, flp_info* out) {
         if (!out) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "null output");
         out->width = h->W; out->height = h->H; out->depth = h->D;
         out->channels = h->C; out->n_kernels = h->K;
+        ensure_conv_mode(h);
         out->conv_mode = h->conv_mode;
         out->time = h->time;
         out->step = h->step;
@@ -792,6 +803,7 @@ int flp_set_conv_mode(flp_propagator* h, int mode) {
         }
         CK(cudaStreamSynchronize(h->st));
         resolve_conv_mode(h, mode);
+        h->conv_pending = false;
         invalidate_graphs(h);
     })
 }
@@ -833,6 +845,7 @@ int flp_profile_run(flp_propagator* h, int steps, int flush_l2, float* stage_ms,
     FLP_CHECK_HANDLE(h);
     FLP_TRY({
         if (steps < 0) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "negative step count");
+        ensure_conv_mode(h);
         profile_run(h, steps, flush_l2, stage_ms, max_stages, n_stages, names, names_len, step_ms);
     })
 }
@@ -842,6 +855,7 @@ int flp_debug_affinity(flp_propagator* h, float* aff_out, size_t n) {
     FLP_TRY({
         const size_t CN = size_t(h->C) * h->N;
         if (!aff_out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "size mismatch");
+        ensure_conv_mode(h);
         h->enqueue_conv(h->A[h->cur], nullptr);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(aff_out, h->U, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));

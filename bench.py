@@ -208,7 +208,12 @@ def measure_batched(args, dist):
     being one device-resident propagator per world stepped in turn."""
     import autoverse_b200 as fl
     from autoverse_b200 import workloads as wl
-    worlds = wl.batched_worlds(args.batch_worlds, seed=wl.DEFAULT_SEED + RANK)
+    from autoverse_b200 import sharding
+    # weak scaling: batch_worlds per GPU; the global list is LPT-partitioned by
+    # estimated step cost, every rank deriving the same partition locally
+    everything = wl.batched_worlds(args.batch_worlds * WORLD)
+    share = sharding.lpt_partition([sharding.world_cost(c) for c, _ in everything], WORLD)[RANK]
+    worlds = [everything[i] for i in share]
     b = fl.BatchedPropagator([c for c, _ in worlds])
     for i, (_, sd) in enumerate(worlds):
         b.load_seed(i, sd)
@@ -219,10 +224,10 @@ def measure_batched(args, dist):
     prof = b.profile_run(args.batch_steps, flush_l2=False)
     b.synchronize()
     t = reduce_max(dist, prof["step_ms"] / 1e3)
-    out = {"workload": f"{args.batch_worlds} worlds, sides {{64..512}} per axis, C in {{1,2}}, K=C*C, R~U{{8..20}}, "
+    out = {"workload": f"{args.batch_worlds} worlds per GPU (LPT-sharded by step cost), sides {{64..512}} per axis, C in {{1,2}}, K=C*C, R~U{{8..20}}, "
                        "mu~U(0.1,0.3), sigma~U(0.01,0.05), dt~U(0.1,0.3), Gaussian-blob seeds",
            "cells_per_gpu": info["cells"], "cell_channels_per_gpu": info["cell_channels"], "steps": args.batch_steps,
-           "value": WORLD * info["cells"] * args.batch_steps / t, "unit": "cell-steps/s",
+           "value": sum(c["width"] * c["height"] for c, _ in everything) * args.batch_steps / t, "unit": "cell-steps/s",
            "ms_per_step": 1e3 * t / args.batch_steps,
            "stage_ms_per_step": {k: v / args.batch_steps for k, v in prof["stages"].items()},
            "gpu_launches_per_step": 1 + 3 * 7 + 2, "l2": "working set above L2 (pooled state and spectra)"}
