@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["multispecies512", "blob256"], default="multispecies512")
+    ap.add_argument("--workload", choices=["multispecies512", "blob256", "sphere128"], default="multispecies512")
     ap.add_argument("--e2e-steps", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-flush", action="store_true")
@@ -69,6 +69,13 @@ def workload(name):
         desc = {"workload": "multispecies 512x512 torus, 3 channels, 9 kernels (all src->tgt pairs, 1-3 rings), "
                             "R=15, dt=0.2, beta_a=1, n=2, s=1, 20 U(0,1) 40x40 patches per channel",
                 "width": 512, "height": 512, "channels": 3, "kernels": 9, "kernel_radius": 15}
+    elif name == "sphere128":
+        from oracle import oracle as O
+        cfg, seed = wl.sphere3d(128)
+        state = O.seed_generate(seed, cfg)
+        desc = {"workload": "3D sphere 128^3 torus, 1 channel, 1 spherical-shell kernel (ring 1.0/0.5/0.15), R=10, "
+                            "mu=0.15, sigma=0.017, dt=0.2, Gaussian sphere r=0.12",
+                "width": 128, "height": 128, "depth": 128, "channels": 1, "kernels": 1, "kernel_radius": 10}
     else:
         from oracle import oracle as O
         cfg, seed = wl.single_blob(256)
@@ -91,13 +98,21 @@ def hbm_peak():
 def stage_bytes(cfg, stage):
     """Algorithmic HBM bytes of one launch of each stage."""
     W, H, C = cfg["width"], cfg["height"], cfg["channels"]
+    D = cfg.get("depth", 1)
     K = len(cfg["kernels"])
-    N = W * H
+    N = W * H * D
     nsrc = len({k["source_channel"] for k in cfg["kernels"]})
-    spec = (W // 2 + 1) * H * 8
+    spec = (W // 2 + 1) * H * D * 8
     return {
+        "fft_x_r2c": nsrc * N * 4 + nsrc * spec,
+        "fft_y_fwd": 2 * nsrc * spec,
+        "fft_z_conv": (nsrc + 2 * K) * spec,
+        "fft_y_inv": 2 * K * spec,
+        "fft_x_c2r_growth": K * spec + C * N * 4,
+        "flow_3d": 2 * C * N * 4 + 4 * C * N * 4,
+        "gather_3d": 4 * C * N * 4 + C * N * 4,
         "fft_rows_r2c": nsrc * N * 4 + nsrc * spec,
-        "fft_cols_conv": K * spec * 3,
+        "fft_cols_conv": (nsrc + 2 * K) * spec,
         "fft_rows_c2r_growth": K * spec + C * N * 4,
         "flow_2d": 2 * C * N * 4 + 3 * C * N * 4,
         "gather_2d": 3 * C * N * 4 + C * N * 4,
@@ -270,7 +285,7 @@ def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
     W, H, C = cfg["width"], cfg["height"], cfg["channels"]
-    cells = W * H
+    cells = W * H * cfg.get("depth", 1)
     metric = "cell-steps/s"
 
     if args.impl == "reference":
