@@ -110,3 +110,31 @@ def sphere3d(size=128, R=10, mu=0.15, sigma=0.017, radius=0.12, dt=0.2):
     seed = {"pattern": {"type": "GaussianSphere", "center": [0.5, 0.5, 0.5], "radius": radius, "amplitude": 1.0,
                         "channel": 0}}
     return cfg, seed
+
+
+
+def adjoint_worlds(n=64, size=256, channels=2, R=13, seed=DEFAULT_SEED):
+    """Worlds for differentiation: `channels` channels, K = C*C kernels (every
+    source->target pair) with 1-3 rings and the multispecies parameter
+    distributions, beta_a=1, n=2, s=1, dt=0.2, and a seed of one Gaussian blob
+    per channel (centre ~U(0.35,0.65), radius ~U(0.06,0.12)).
+    Returns [(config, seed), ...]; the loss target is `shifted(state0)`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        ks = []
+        for src in range(channels):
+            for tgt in range(channels):
+                ks.append(kernel(src, tgt, random_rings(rng), weight=float(rng.uniform(0.3, 1.0)),
+                                 mu=float(rng.uniform(0.1, 0.3)), sigma=float(rng.uniform(0.01, 0.05))))
+        cfg = config(size, size, channels, ks, dt=0.2, kernel_radius=R)
+        blobs = [{"center": [float(rng.uniform(0.35, 0.65)), float(rng.uniform(0.35, 0.65))],
+                  "radius": float(rng.uniform(0.06, 0.12)), "amplitude": 1.0, "channel": c} for c in range(channels)]
+        out.append((cfg, {"pattern": {"type": "MultiBlob", "blobs": blobs}}))
+    return out
+
+
+def shifted(state: np.ndarray, width: int, height: int, shift: int = 20) -> np.ndarray:
+    """The state moved `shift` cells along +x on the torus (the adjoint loss target)."""
+    C = state.shape[0]
+    return np.ascontiguousarray(np.roll(state.reshape(C, height, width), shift, axis=2).reshape(C, -1))

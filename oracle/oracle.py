@@ -117,8 +117,9 @@ def validate_config(cfg: dict) -> None:
             raise ValueError(f"InvalidChannelIndex kernel {i}")
 
 
-def _pack_kernels(cfg: dict, f64: bool):
+def _pack_kernels(cfg: dict, f64: bool, exact: bool = False):
     dt = _dt(f64)
+    f32 = float if exact else globals()["f32"]
     ks = cfg["kernels"]
     kp = np.zeros((max(len(ks), 1), 6), dtype=dt)
     rc = np.zeros(max(len(ks), 1), dtype=np.int32)
@@ -136,7 +137,9 @@ def _pack_kernels(cfg: dict, f64: bool):
 class OraclePropagator:
     """CpuPropagator / CpuPropagator3D restated in C (f32, or f64 twin)."""
 
-    def __init__(self, cfg: dict | str, f64: bool = False):
+    def __init__(self, cfg: dict | str, f64: bool = False, exact_params: bool = False):
+        """exact_params (f64 only): take the config's numbers as given instead of
+        rounding them to f32 first (finite differences of the FP64 twin)."""
         cfg = normalize_config(cfg)
         validate_config(cfg)
         self.cfg = cfg
@@ -145,12 +148,14 @@ class OraclePropagator:
         self.C = cfg["channels"]
         self.N = self.W * self.H * self.D
         self.dims = 3 if self.D > 1 else 2
-        kp, rc, ra = _pack_kernels(cfg, f64)
+        exact = bool(exact_params and f64)
+        kp, rc, ra = _pack_kernels(cfg, f64, exact)
         self._keep = (kp, rc, ra)
         fl = cfg["flow"]
-        self._h = _fn(f64, "prop_new")(self.W, self.H, self.D, self.C, f32(cfg["dt"]), cfg["kernel_radius"],
-                                      len(cfg["kernels"]), _ptr(kp), _ptr(rc), _ptr(ra), f32(fl["beta_a"]),
-                                      f32(fl["n"]), f32(fl["distribution_size"]))
+        num = float if exact else f32
+        self._h = _fn(f64, "prop_new")(self.W, self.H, self.D, self.C, num(cfg["dt"]), cfg["kernel_radius"],
+                                      len(cfg["kernels"]), _ptr(kp), _ptr(rc), _ptr(ra), num(fl["beta_a"]),
+                                      num(fl["n"]), num(fl["distribution_size"]))
 
     def __del__(self):
         h = getattr(self, "_h", None)
