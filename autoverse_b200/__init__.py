@@ -4,8 +4,9 @@ Hand-written sm_100a CUDA kernels behind a C ABI (include/flowlenia_cuda.h),
 with a Python mirror of the reference crate's propagator surface.
 """
 from ._native import CONV_AUTO, CONV_DIRECT, CONV_FFT, ConfigError, FlpError
+from .adjoint import AdjointBatch, FlowLeniaFunction
 from .batch import BatchedPropagator
 from .propagator import CudaPropagator, SimulationConfig, SimulationState
 
-__all__ = ["BatchedPropagator", "CudaPropagator", "SimulationConfig", "SimulationState", "ConfigError", "FlpError", "CONV_AUTO",
+__all__ = ["AdjointBatch", "FlowLeniaFunction", "BatchedPropagator", "CudaPropagator", "SimulationConfig", "SimulationState", "ConfigError", "FlpError", "CONV_AUTO",
            "CONV_DIRECT", "CONV_FFT"]

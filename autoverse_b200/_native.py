@@ -75,6 +75,15 @@ SIGNATURES = {
     "flp_debug_affinity": (I, [P, P, Z]),
     "flp_affinity_noalloc": (I, [S, P, P, P]),
     "flp_batch_create": (I, [C.POINTER(C.c_char_p), I, PP]),
+    "flp_adj_create": (I, [C.POINTER(C.c_char_p), I, PP]),
+    "flp_adj_destroy": (I, [P]),
+    "flp_adj_write_state": (I, [P, I, P, Z]),
+    "flp_adj_state_from_seed": (I, [P, I, S]),
+    "flp_adj_forward": (I, [P, I, I]),
+    "flp_adj_read_final": (I, [P, I, P, Z]),
+    "flp_adj_param_count": (I, [P, I, C.POINTER(I)]),
+    "flp_adj_backward": (I, [P, P, Z, P, Z, P, Z]),
+    "flp_adj_timings": (I, [P, C.POINTER(F), C.POINTER(F)]),
     "flp_batch_destroy": (I, [P]),
     "flp_batch_state_from_seed": (I, [P, I, S]),
     "flp_batch_write_world": (I, [P, I, P, Z]),

@@ -498,27 +498,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         d.twM = twiddles(d.W / 2);
         d.twW = twiddles(d.W);
         d.twH = twiddles(d.H);
-        // flow parameters (same derivation as the single-world engine)
-        FlowParams fp{};
-        fp.dt = c.dt;
-        fp.s = c.flow.distribution_size;
-        const float two_s = 2.0f * fp.s;
-        fp.total_area = two_s * two_s;
-        int e = 0;
-        const float mant = std::frexp(fp.total_area, &e);
-        fp.area_pow2 = (fp.total_area > 0.f && mant == 0.5f && std::isnormal(fp.total_area)) ? 1 : 0;
-        fp.inv_area = fp.area_pow2 ? 1.0f / fp.total_area : 0.f;
-        fp.beta_a = c.flow.beta_a;
-        int eb = 0;
-        const float mb = std::frexp(fp.beta_a, &eb);
-        fp.beta_pow2 = (fp.beta_a > 0.f && mb == 0.5f && std::isnormal(fp.beta_a) && std::isnormal(1.0f / fp.beta_a)) ? 1 : 0;
-        fp.inv_beta = fp.beta_pow2 ? 1.0f / fp.beta_a : 0.f;
-        fp.nexp = c.flow.n;
-        fp.point_mode = fp.total_area < 1e-10f ? 1 : 0;
-        if (fp.point_mode) fp.area_pow2 = 0;
-        const float maxside = float(std::max(c.width, c.height));
-        fp.pos_eps = 8.0f * maxside * 1.1920929e-07f + 1e-4f;
-        d.fp = fp;
+        d.fp = flow_params_of(c);
         b->hw.push_back(d);
         b->cfgs.push_back(c);
     }

@@ -30,7 +30,6 @@ struct FlowParams {
     float total_area;   // (2s)*(2s) (or (2s)^3 in 3D), f32 as the reference computes it
     float inv_area;     // exact reciprocal when total_area is a power of two
     float beta_a, nexp;
-    float ubound;       // max over channels of sum_k |w_k| for kernels targeting the channel
     float pos_eps;      // absolute margin (cells) for rounding of positions in the gather window
     float inv_beta;     // 1 / beta_a when beta_a is a power of two (exact)
     int beta_pow2;

@@ -424,7 +424,7 @@ static void resolve_conv_mode(flp_propagator* h, int requested) {
     g_tune_cache[key] = h->conv_mode;
 }
 
-static FlowParams make_flow_params(const SimulationConfig& cfg) {
+FlowParams flow_params_of(const SimulationConfig& cfg) {
     FlowParams fp{};
     fp.dt = cfg.dt;
     fp.s = cfg.flow.distribution_size;
@@ -447,10 +447,6 @@ static FlowParams make_flow_params(const SimulationConfig& cfg) {
     fp.nexp = cfg.flow.n;
     fp.point_mode = fp.total_area < 1e-10f ? 1 : 0;
     if (fp.point_mode) fp.area_pow2 = 0;  // nearest-cell deposits carry the raw mass
-    std::vector<float> wsum(cfg.channels, 0.f);
-    for (const auto& k : cfg.kernels) wsum[k.target_channel] += std::fabs(k.weight);
-    fp.ubound = 0.f;
-    for (float w : wsum) fp.ubound = std::max(fp.ubound, w);
     // dest = x + dt*F and x_min/x_max are rounded at the scale of the largest
     // coordinate; allow a few ulps of it plus a fixed slack.
     const float maxside = float(std::max(std::max(cfg.width, cfg.height), cfg.depth));
@@ -510,7 +506,7 @@ static void create(const std::string& json, flp_propagator* h) {
     if (h->K) CK(cudaMemcpy(h->d_kd, h->kd.data(), h->kd.size() * sizeof(KDesc), cudaMemcpyHostToDevice));
     if (h->dims == 2) setup_fft(h, ks);
     else setup_fft3d(h, ks);
-    h->fp = make_flow_params(c);
+    h->fp = flow_params_of(c);
     CK(cudaStreamSynchronize(h->st));
     h->conv_pending = true;
 }

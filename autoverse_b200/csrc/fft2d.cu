@@ -19,6 +19,8 @@
 
 #include <math.h>
 
+#include <stdexcept>
+
 namespace flp {
 
 // Transforms `nlines` lines of length p.L held in `a`; element (line, i) sits
@@ -305,6 +307,18 @@ __global__ void __launch_bounds__(256) k_c2r_t(const float2* __restrict__ T, flo
     c2r_growth_item<M>(fsm, T, kd, K, c, U + size_t(c) * W * H, H, blockIdx.x * RowCfg<M>::NR, twM, twW);
 }
 
+template <int M>
+__global__ void __launch_bounds__(256) k_c2r_raw_t(const float2* __restrict__ T, float* __restrict__ out,
+                                                   const int* __restrict__ planes, int H, float scale, int accumulate,
+                                                   const float2* __restrict__ twM, const float2* __restrict__ twW) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const int slot = blockIdx.y;
+    const int plane = planes ? planes[slot] : slot;
+    constexpr int W = 2 * M, Wc = M + 1;
+    c2r_raw_item<M>(fsm, T + size_t(slot) * Wc * H, out + size_t(plane) * W * H, H, blockIdx.x * RowCfg<M>::NR,
+                    scale, accumulate != 0, twM, twW);
+}
+
 bool fft_row_templated(int M) {
 #define X(n) if (M == n) return true;
     FLP_ROW_SIZES(X)
@@ -335,7 +349,7 @@ void fft2d_set_attributes(size_t max_bytes) {
     set((const void*)fft_rows_r2c);
     set((const void*)fft_cols_conv);
     set((const void*)fft_rows_c2r_growth);
-#define X(n) set((const void*)k_r2c_t<n>); set((const void*)k_c2r_t<n>);
+#define X(n) set((const void*)k_r2c_t<n>); set((const void*)k_c2r_t<n>); set((const void*)k_c2r_raw_t<n>);
     FLP_ROW_SIZES(X)
 #undef X
 #define X(n) set((const void*)k_cols_t<n>);
@@ -394,6 +408,21 @@ void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, in
     dim3 grid((H + g.NR - 1) / g.NR, C);
     fft_rows_c2r_growth<<<grid, 256, fft_rows_smem(W, g.NR, true), st>>>(T, U, kd, K, W, H, g.NR, g.pm, g.twM,
                                                                           g.twW);
+}
+
+void launch_fft_c2r_raw(const float2* T, float* out, const int* planes, int nslots, int W, int H, float scale,
+                        bool accumulate, const FftGeom& g, cudaStream_t st) {
+    const int M = W / 2;
+#define X(n)                                                                                                  \
+    if (M == n) {                                                                                             \
+        dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, nslots);                                           \
+        k_c2r_raw_t<n><<<grid, 256, RowCfg<n>::smem_r2c, st>>>(T, out, planes, H, scale, accumulate ? 1 : 0, \
+                                                                g.twM, g.twW);                                \
+        return;                                                                                               \
+    }
+    FLP_ROW_SIZES(X)
+#undef X
+    throw std::runtime_error("inverse row pass without growth needs W/2 in {16..256}");
 }
 
 }  // namespace flp

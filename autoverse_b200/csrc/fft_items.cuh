@@ -407,6 +407,52 @@ __device__ void c2r_growth_item(float2* sm, const float2* __restrict__ T, const 
     __syncthreads();
 }
 
+// NR rows of one spectrum slot: inverse real FFT, times `scale`, written to
+// (or, with accumulate, added to) the rows of `out`.  Same arithmetic as the
+// growth epilogue's inverse, without the growth.
+template <int M>
+__device__ void c2r_raw_item(float2* sm, const float2* __restrict__ t, float* __restrict__ out, int H, int y0,
+                             float scale, bool accumulate, const float2* __restrict__ twM_g,
+                             const float2* __restrict__ twW_g) {
+    constexpr int NR = RowCfg<M>::NR, LS = RowCfg<M>::LS, Wc = M + 1, W = 2 * M;
+    float2* twM = sm;
+    float2* twW = twM + M;
+    float2* a = twW + Wc;
+    float2* b = a + RowCfg<M>::buf;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < M; i += 256) twM[i] = twM_g[i];
+    for (int i = tid; i < Wc; i += 256) twW[i] = twW_g[i];
+#pragma unroll 4
+    for (int i = tid; i < NR * Wc; i += 256) {
+        const int r = i % NR, kk = i / NR;
+        const int y = y0 + r;
+        a[r * LS + kk] = y < H ? t[size_t(kk) * H + y] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int i = tid; i < NR * M; i += 256) {
+        const int r = i / M, kk = i - r * M;
+        const float2 xk = a[r * LS + kk];
+        const float2 xm = cconj(a[r * LS + M - kk]);
+        const float2 e = cadd(xk, xm);
+        const float2 o = cmul(csub(xk, xm), cconj(twW[kk]));
+        b[r * LS + pad8(kk)] = make_float2(e.x - o.y, e.y + o.x);
+    }
+    __syncthreads();
+    const float2* z = ct_fft<M, NR, true>(b, a, twM);
+#pragma unroll 4
+    for (int i = tid; i < NR * W; i += 256) {
+        const int r = i / W, x = i - r * W;
+        const int y = y0 + r;
+        if (y >= H) continue;
+        const float2 v = z[r * LS + pad8(x >> 1)];
+        const float val = __fmul_rn((x & 1) ? v.y : v.x, scale);
+        float* o = out + size_t(y) * W + x;
+        *o = accumulate ? __fadd_rn(*o, val) : val;
+    }
+    __syncthreads();
+}
+
 #define FLP_ROW_SIZES(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256)
 #define FLP_COL_SIZES(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
 

@@ -31,6 +31,11 @@ struct FftGeom {
 
 bool make_plan(int L, FftPlan& p);
 
+// Flow and reintegration parameters of one world (engine.cu), shared by the
+// single-world, batched and differentiable engines.
+struct SimulationConfig;
+FlowParams flow_params_of(const SimulationConfig& cfg);
+
 // direct convolution + growth
 size_t conv_direct_smem_bytes(int rmax);
 void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, const float* taps, int W, int H, int C,
@@ -61,6 +66,10 @@ void launch_fft_lines(const float2* S, const float2* KH, float2* T, const int* s
                       int H, const FftGeom& g, int mode, float scale, cudaStream_t st);
 void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,
                            cudaStream_t st);
+// Inverse row pass without growth: slot j -> plane planes[j] (or j), times
+// scale, written or accumulated.  Templated row lengths only.
+void launch_fft_c2r_raw(const float2* T, float* out, const int* planes, int nslots, int W, int H, float scale,
+                        bool accumulate, const FftGeom& g, cudaStream_t st);
 
 // 3D FFT path: z-axis pass (the x and y passes reuse the 2D row and column passes)
 bool fft_row_templated(int M);

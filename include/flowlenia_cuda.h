@@ -172,6 +172,39 @@ FLP_API void* flp_batch_stream(flp_batch* b);
 /* As flp_profile_run: 5 stages (r2c, cols, c2r, flow, gather). */
 FLP_API int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms, float* step_ms);
 
+/* ---- Differentiable step (adjoint) ------------------------------------
+ * No counterpart in the reference (its propagators are forward only).  A
+ * batch of same-shape 2D worlds -- equal width, height, channels (<= 8),
+ * kernel count, per-kernel source/target channels and distribution_size;
+ * every other parameter may differ per world -- run forward T steps keeping
+ * the state every k steps, then a hand-written reverse sweep (recomputing
+ * each k-step segment from its checkpoint) turns dL/dA_T into dL/dA_0 and
+ * dL/d(parameters).  The forward pass is bit-identical to flp_run on each
+ * world.  Host buffers hold all worlds back to back, world-major, each world
+ * [channel][y][x].  The parameter vector of one world is
+ *   beta_a, then per kernel: weight, mu, sigma, then per ring of that
+ *   kernel: amplitude, distance, width
+ * and the worlds' vectors are concatenated in world order. */
+typedef struct flp_adjoint flp_adjoint;
+
+FLP_API int flp_adj_create(const char* const* config_jsons, int n_worlds, flp_adjoint** out);
+FLP_API int flp_adj_destroy(flp_adjoint* h);
+/* Initial state A_0 of one world (channels*W*H floats, host memory). */
+FLP_API int flp_adj_write_state(flp_adjoint* h, int world, const float* state, size_t n);
+FLP_API int flp_adj_state_from_seed(flp_adjoint* h, int world, const char* seed_json);
+/* T steps from A_0, keeping A_0, A_k, A_2k, ... on the device. */
+FLP_API int flp_adj_forward(flp_adjoint* h, int steps, int checkpoint_every);
+/* A_T of one world after flp_adj_forward. */
+FLP_API int flp_adj_read_final(flp_adjoint* h, int world, float* out, size_t n);
+FLP_API int flp_adj_param_count(flp_adjoint* h, int world, int* count);
+/* dl_dfinal: dL/dA_T of all worlds (n = n_worlds*channels*W*H floats);
+ * dl_dinitial (same size) and dl_dparams (sum of the param counts) receive
+ * the gradients; either may be NULL. */
+FLP_API int flp_adj_backward(flp_adjoint* h, const float* dl_dfinal, size_t n, float* dl_dinitial, size_t n_initial,
+                             double* dl_dparams, size_t n_params);
+/* Device time of the last forward and backward passes (CUDA events). */
+FLP_API int flp_adj_timings(flp_adjoint* h, float* forward_ms, float* backward_ms);
+
 /* Allocation-free affinity.  No counterpart in the reference: an addition for
  * callers that may not allocate device memory, such as code enqueued from
  * another framework's plugin or custom operator on that framework's stream,
