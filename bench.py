@@ -59,6 +59,9 @@ def parse_args():
                     help="convolution path (auto = the engine's measured choice)")
     ap.add_argument("--batch-worlds", type=int, default=4096, help="worlds in the batched measurement (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--adjoint-worlds", type=int, default=64, help="worlds in the adjoint measurement (0 = skip)")
+    ap.add_argument("--adjoint-steps", type=int, default=64)
+    ap.add_argument("--adjoint-every", type=int, default=8)
     return ap.parse_args()
 
 
@@ -281,12 +284,50 @@ def measure_batched(args, dist):
     return out
 
 
+def measure_adjoint(args, dist):
+    """Differentiable step: `--adjoint-worlds` worlds of 256x256, 2 channels,
+    4 kernels (every source->target pair, 1-3 rings, multispecies parameter
+    distributions), R=13; forward T steps keeping every k-th state, then the
+    reverse sweep for L = sum (A_T - target)^2, target = A_0 shifted 20 cells
+    along x.  Device time of each pass from CUDA events on the engine's stream,
+    median of 3 after one warm-up pass."""
+    import autoverse_b200 as fl
+    from autoverse_b200 import workloads as wl
+    worlds = wl.adjoint_worlds(args.adjoint_worlds, size=256, R=13, seed=wl.DEFAULT_SEED + RANK)
+    b = fl.AdjointBatch([c for c, _ in worlds])
+    tgt = []
+    for i, (c, sd) in enumerate(worlds):
+        a0 = fl.SimulationState.from_seed(sd, c).channels
+        b.write_state(i, a0)
+        tgt.append(wl.shifted(a0, 256, 256, 20))
+    tgt = np.stack(tgt)
+    T, k = args.adjoint_steps, args.adjoint_every
+    fw, bw = [], []
+    for it in range(4):  # pass 0 is the warm-up
+        b.forward(T, k)
+        fin = np.stack([b.read_final(i) for i in range(b.n_worlds)])
+        b.backward(2.0 * (fin - tgt))
+        f, g = b.timings()
+        if it:
+            fw.append(f)
+            bw.append(g)
+    b.close()
+    f = reduce_max(dist, float(np.median(fw)))
+    g = reduce_max(dist, float(np.median(bw)))
+    cells = args.adjoint_worlds * 256 * 256 * T * WORLD
+    return {"workload": f"{args.adjoint_worlds} worlds per GPU of 256x256, C=2, K=4, R=13, T={T}, checkpoint every {k}, "
+                        "loss sum (A_T - shift_x(A_0, 20))^2, gradients for A_0, beta_a, weight, mu, sigma and ring "
+                        "amplitude/distance/width",
+            "forward_ms": f, "backward_ms": g, "backward_over_forward": g / f,
+            "forward_cell_steps_per_s": cells / (f / 1e3), "backward_cell_steps_per_s": cells / (g / 1e3)}
+
+
 def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
     W, H, C = cfg["width"], cfg["height"], cfg["channels"]
     cells = W * H * cfg.get("depth", 1)
-    metric = "cell-steps/s"
+    metric = "cell-steps/s on 1 B200, batched vs plain at \u22641e-5 err; backward/forward ratio"
 
     if args.impl == "reference":
         dist = dist_init()
@@ -361,6 +402,7 @@ def main():
     e2e_value = WORLD * cells * args.e2e_steps / e2e_t
 
     batched = measure_batched(args, dist) if args.batch_worlds > 0 else None
+    adjoint = measure_adjoint(args, dist) if args.adjoint_worlds > 0 else None
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
@@ -391,6 +433,9 @@ def main():
         "clocks": clocks,
         "cpu_baseline": cpu,
         "batched": batched,
+        "batched_over_plain": batched["small_worlds_batched_over_plain"]["ratio"] if batched else None,
+        "adjoint": adjoint,
+        "backward_over_forward": adjoint["backward_over_forward"] if adjoint else None,
     }
     print(json.dumps(line), flush=True)
 
