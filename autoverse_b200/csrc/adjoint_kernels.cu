@@ -22,7 +22,7 @@
 namespace flp {
 
 // ------------------------------------------------------ forward, batched ----
-template <bool POW2>
+template <int CV, bool POW2>
 __global__ void __launch_bounds__(256) k_flow_worlds(const float* __restrict__ A, const float* __restrict__ U,
                                                      float* __restrict__ DX, float* __restrict__ DY,
                                                      float* __restrict__ MS, int C, int W, int H,
@@ -31,8 +31,12 @@ __global__ void __launch_bounds__(256) k_flow_worlds(const float* __restrict__ A
     const int w = blockIdx.z;
     const size_t off = size_t(w) * C * W * H;
     const FlowParams fp = fps[w];
-    flow_item<POW2>(sm, A + off, U + off, DX + off, DY + off, MS + off, C, W, H, fp, blockIdx.x * FL_W,
-                    blockIdx.y * FL_H, dmax + w, status);
+    if constexpr (CV == 0)
+        flow_item<POW2>(sm, A + off, U + off, DX + off, DY + off, MS + off, C, W, H, fp, blockIdx.x * FL_W,
+                        blockIdx.y * FL_H, dmax + w, status);
+    else
+        flow_rows_item<CV, POW2>(A + off, U + off, DX + off, DY + off, MS + off, W, H, fp, blockIdx.x * 32,
+                                 blockIdx.y * FR_H, dmax + w, status);
 }
 
 template <bool POW2>
@@ -50,11 +54,18 @@ __global__ void __launch_bounds__(256, 3) k_gather_worlds(const float* __restric
 
 void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, float* MS, int B, int C, int W, int H,
                         const FlowParams* fps, bool pow2, int* dmax, int* status, cudaStream_t st) {
-    dim3 grid((W + FL_W - 1) / FL_W, (H + FL_H - 1) / FL_H, B);
-    if (pow2)
-        k_flow_worlds<true><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fps, dmax, status);
-    else
-        k_flow_worlds<false><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fps, dmax, status);
+    const int cv = C <= 4 ? C : 0;
+    const int th = cv ? FR_H : FL_H;
+    const dim3 grid((W + FL_W - 1) / FL_W, (H + th - 1) / th, B);
+    const size_t smem = cv ? 0 : flow_smem_bytes(C);
+#define FW_CASE(v)                                                                                             \
+    if (cv == v) {                                                                                             \
+        if (pow2) k_flow_worlds<v, true><<<grid, 256, smem, st>>>(A, U, DX, DY, MS, C, W, H, fps, dmax, status);  \
+        else k_flow_worlds<v, false><<<grid, 256, smem, st>>>(A, U, DX, DY, MS, C, W, H, fps, dmax, status);      \
+        return;                                                                                                \
+    }
+    FW_CASE(0) FW_CASE(1) FW_CASE(2) FW_CASE(3) FW_CASE(4)
+#undef FW_CASE
 }
 
 void launch_gather_worlds(const float* DX, const float* DY, const float* MS, float* An, int B, int C, int W, int H,
@@ -417,8 +428,8 @@ void adjoint_set_attributes() {
     auto set = [](const void* f, size_t bytes) {
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     };
-    set((const void*)k_flow_worlds<true>, flow_smem_bytes(ADJ_MAX_CHANNELS));
-    set((const void*)k_flow_worlds<false>, flow_smem_bytes(ADJ_MAX_CHANNELS));
+    set((const void*)k_flow_worlds<0, true>, flow_smem_bytes(ADJ_MAX_CHANNELS));
+    set((const void*)k_flow_worlds<0, false>, flow_smem_bytes(ADJ_MAX_CHANNELS));
     set((const void*)k_gather_worlds<true>, gather_smem_bytes());
     set((const void*)k_gather_worlds<false>, gather_smem_bytes());
     set((const void*)k_adj_flow, sizeof(float) * (2 * ADJ_MAX_CHANNELS + 1) * FL_RC);

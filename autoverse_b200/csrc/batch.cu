@@ -79,9 +79,14 @@ struct BWorld {
 };
 
 constexpr int NCLS = 9;  // size classes per FFT pass
-// Queue index: FFT stages s in {0,1,2} use queue s*NCLS + class; flow and
-// gather use queues 3*NCLS and 3*NCLS+1.
-constexpr int NQUEUE = 3 * NCLS + 2;
+// Queue index: FFT stages s in {0,1,2} use queue s*NCLS + class; the flow
+// uses one queue per channel count (QF + C for C = 1..4, QF for the rest,
+// each with its own compiled kernel); the gather uses QG.
+constexpr int NFLOWQ = 5;
+constexpr int QF = 3 * NCLS;
+constexpr int QG = QF + NFLOWQ;
+constexpr int NQUEUE = QG + 1;
+inline int flow_queue(int C) { return QF + (C <= 4 ? C : 0); }
 
 struct Pools {
     const BWorld* worlds;
@@ -174,9 +179,9 @@ __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_batch_flow(Pools p) {
+template <int CV>
+__global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
     extern __shared__ __align__(16) float sm[];
-    constexpr int q = 3 * NCLS;
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
     for (;;) {
         const int it = next_item(p.counters + q, n);
@@ -184,19 +189,23 @@ __global__ void __launch_bounds__(256) k_batch_flow(Pools p) {
         const int2 item = p.items[base + it];
         const BWorld w = p.worlds[item.x];
         const int tiles_x = (w.W + FL_W - 1) / FL_W;
-        const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * FL_H;
-        if (w.fp.area_pow2)
-            flow_item<true>(sm, p.A + w.offA, p.U + w.offA, p.DX + w.offA, p.DY + w.offA, p.MS + w.offA, w.C, w.W,
-                            w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
-        else
-            flow_item<false>(sm, p.A + w.offA, p.U + w.offA, p.DX + w.offA, p.DY + w.offA, p.MS + w.offA, w.C, w.W,
-                             w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+        const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * (CV ? FR_H : FL_H);
+        const float* A = p.A + w.offA;
+        const float* U = p.U + w.offA;
+        float *DX = p.DX + w.offA, *DY = p.DY + w.offA, *MS = p.MS + w.offA;
+        if constexpr (CV == 0) {
+            if (w.fp.area_pow2) flow_item<true>(sm, A, U, DX, DY, MS, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+            else flow_item<false>(sm, A, U, DX, DY, MS, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+        } else {
+            if (w.fp.area_pow2) flow_rows_item<CV, true>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+            else flow_rows_item<CV, false>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+        }
     }
 }
 
 __global__ void __launch_bounds__(256, 3) k_batch_gather(Pools p) {
     extern __shared__ __align__(16) float sm[];
-    constexpr int q = 3 * NCLS + 1;
+    constexpr int q = QG;
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
     for (;;) {
         const int it = next_item(p.counters + q, n);
@@ -364,7 +373,7 @@ struct flp_batch {
 
     void launch_queue(int q, Pools& p) {
         if (!n_q[q]) return;
-        if (q < 3 * NCLS) {
+        if (q < QG) {
             int qq = q;
             void* args[] = {&p, &qq};
             ckb(cudaLaunchKernel(q_fn[q], dim3(q_grid[q]), dim3(256), args, q_smem[q], st), "batch launch");
@@ -383,9 +392,9 @@ struct flp_batch {
             for (int cls = 0; cls < NCLS; ++cls) launch_queue(stage * NCLS + cls, p);
             if (timed) ckb(cudaEventRecord(ev[stage + 1], st), "event");
         }
-        launch_queue(3 * NCLS, p);
+        for (int v = 0; v < NFLOWQ; ++v) launch_queue(QF + v, p);
         if (timed) ckb(cudaEventRecord(ev[4], st), "event");
-        launch_queue(3 * NCLS + 1, p);
+        launch_queue(QG, p);
         if (timed) ckb(cudaEventRecord(ev[5], st), "event");
         ckb(cudaGetLastError(), "batch launch");
         cur ^= 1;
@@ -426,7 +435,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
             set(c2r_fn(c), c2r_smem(c));
             set(cols_fn(c), cols_smem(c));
         }
-        set((const void*)k_batch_flow, flow_smem_bytes_inl(64));
+        set((const void*)k_batch_flow<0>, flow_smem_bytes_inl(64));
         set((const void*)k_batch_gather, gather_smem_bytes_inl());
         transport_2d_set_attributes();
         fft2d_set_attributes(200 * 1024);
@@ -577,11 +586,12 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
             for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (k << 16) | g));
         for (int c = 0; c < d.C; ++c)
             for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
-        const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + FL_H - 1) / FL_H);
-        for (int t = 0; t < ftiles; ++t) items[3 * NCLS].push_back(make_int2(w, t));
+        const int fth = d.C <= 4 ? FR_H : FL_H;
+        const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + fth - 1) / fth);
+        for (int t = 0; t < ftiles; ++t) items[flow_queue(d.C)].push_back(make_int2(w, t));
         const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + GT_H - 1) / GT_H);
         for (int c = 0; c < d.C; ++c)
-            for (int t = 0; t < gtiles; ++t) items[3 * NCLS + 1].push_back(make_int2(w, (c << 16) | t));
+            for (int t = 0; t < gtiles; ++t) items[QG].push_back(make_int2(w, (c << 16) | t));
     }
     std::vector<int2> all;
     std::vector<int> qoff(NQUEUE + 1, 0);
@@ -600,13 +610,20 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     ckb(cudaGetDevice(&dev), "device");
     ckb(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
     for (int q = 0; q < NQUEUE; ++q) {
-        const int stage = q < 3 * NCLS ? q / NCLS : (q == 3 * NCLS ? 3 : 4);
+        const int stage = q < QF ? q / NCLS : (q < QG ? 3 : 4);
         const int cls = q % NCLS;
         switch (stage) {
             case 0: b->q_fn[q] = r2c_fn(cls); b->q_smem[q] = r2c_smem(cls); break;
             case 1: b->q_fn[q] = cols_fn(cls); b->q_smem[q] = cols_smem(cls); break;
             case 2: b->q_fn[q] = c2r_fn(cls); b->q_smem[q] = c2r_smem(cls); break;
-            case 3: b->q_fn[q] = (const void*)k_batch_flow; b->q_smem[q] = flow_smem_bytes_inl(cmax); break;
+            case 3: {
+                const void* fns[NFLOWQ] = {(const void*)k_batch_flow<0>, (const void*)k_batch_flow<1>,
+                                           (const void*)k_batch_flow<2>, (const void*)k_batch_flow<3>,
+                                           (const void*)k_batch_flow<4>};
+                b->q_fn[q] = fns[q - QF];
+                b->q_smem[q] = q == QF ? flow_smem_bytes_inl(cmax) : 0;
+                break;
+            }
             default: b->q_fn[q] = (const void*)k_batch_gather; b->q_smem[q] = gather_smem_bytes_inl(); break;
         }
         if (!b->n_q[q]) continue;

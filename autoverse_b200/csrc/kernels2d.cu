@@ -127,8 +127,29 @@ __global__ void __launch_bounds__(256, 3) gather_2d(const float* __restrict__ DX
                       fp, *dmax_slot, blockIdx.x * GT_W, blockIdx.y * GT_H);
 }
 
+template <int C, bool POW2>
+__global__ void __launch_bounds__(256) flow_rows_2d(const float* __restrict__ A, const float* __restrict__ U,
+                                                    float* __restrict__ DX, float* __restrict__ DY,
+                                                    float* __restrict__ MS, int W, int H, FlowParams fp,
+                                                    int* dmax_slot, int* status) {
+    flow_rows_item<C, POW2>(A, U, DX, DY, MS, W, H, fp, blockIdx.x * 32, blockIdx.y * FR_H, dmax_slot, status);
+}
+
+// One compiled kernel per channel count 1..4 (the register-resident row walk),
+// the staged kernel for more channels.
 void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float* MS, int C, int W, int H,
                     const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
+    if (C >= 1 && C <= 4) {
+        const dim3 g((W + 31) / 32, (H + FR_H - 1) / FR_H);
+#define FR_CASE(c)                                                                                                 \
+        if (C == c) {                                                                                              \
+            if (fp.area_pow2) flow_rows_2d<c, true><<<g, 256, 0, st>>>(A, U, DX, DY, MS, W, H, fp, dmax_slot, status);   \
+            else flow_rows_2d<c, false><<<g, 256, 0, st>>>(A, U, DX, DY, MS, W, H, fp, dmax_slot, status);              \
+            return;                                                                                                \
+        }
+        FR_CASE(1) FR_CASE(2) FR_CASE(3) FR_CASE(4)
+#undef FR_CASE
+    }
     dim3 grid((W + FL_W - 1) / FL_W, (H + FL_H - 1) / FL_H);
     if (fp.area_pow2)
         flow_2d<true><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);

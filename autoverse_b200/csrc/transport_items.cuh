@@ -30,6 +30,11 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+// 16-byte copy (global source and shared destination both 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -169,6 +174,109 @@ __device__ void flow_item(float* sm, const float* __restrict__ A, const float* _
     __syncthreads();
 }
 
+// ------------------------------------------------- flow_2d, row-walking ----
+// Register-resident variant for C <= 4 (same arithmetic as flow_item): a warp
+// covers 32 columns and each thread walks FR_RPT rows of its column, keeping a
+// 3-row window of the channel sum and of every U_c in registers.  Horizontal
+// neighbours come from warp shuffles; the two columns just outside the warp
+// (x0-1 for lane 0, x0+32 for lane 31) from one extra load per row and field.
+// Every lane loads the wrapped column of its position, so partial tiles and
+// grids narrower than a warp see the torus neighbours.
+constexpr int FR_RPT = 2;            // rows per thread
+constexpr int FR_H = 8 * FR_RPT;     // tile height: 8 warps of 32 columns
+
+template <int C, bool POW2>
+__device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, const float* __restrict__ U,
+                                               float* __restrict__ DX, float* __restrict__ DY,
+                                               float* __restrict__ MS, int W, int H, const FlowParams& fp, int x0,
+                                               int y0, int* dmax_slot, int* status) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const size_t N = size_t(W) * H;
+    const int X = x0 + lane;
+    const int xc = wrap_near(X, W);
+    const int xh = wrap_near(lane == 0 ? x0 - 1 : x0 + 32, W);
+    const int yb = y0 + FR_RPT * wp;
+    float sw[3][3], uw[C][3][3], ac[C], an[C];
+    float dmax = 0.f;
+    bool bad = false;
+#pragma unroll
+    for (int r = 0; r < FR_RPT + 2; ++r) {
+        const size_t row = size_t(wrap_near(yb - 1 + r, H)) * W;
+        float av[C], ah[C], uv[C], uh[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            av[c] = A[size_t(c) * N + row + xc];
+            ah[c] = A[size_t(c) * N + row + xh];
+            uv[c] = U[size_t(c) * N + row + xc];
+            uh[c] = U[size_t(c) * N + row + xh];
+        }
+        float sv = 0.f, sh = 0.f;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            sv = __fadd_rn(sv, av[c]);
+            sh = __fadd_rn(sh, ah[c]);
+        }
+        // shift the windows up one row
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            sw[0][j] = sw[1][j];
+            sw[1][j] = sw[2][j];
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                uw[c][0][j] = uw[c][1][j];
+                uw[c][1][j] = uw[c][2][j];
+            }
+        }
+        {
+            const float l = __shfl_up_sync(FULL, sv, 1), rr = __shfl_down_sync(FULL, sv, 1);
+            sw[2][0] = lane == 0 ? sh : l;
+            sw[2][1] = sv;
+            sw[2][2] = lane == 31 ? sh : rr;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float l = __shfl_up_sync(FULL, uv[c], 1), rr = __shfl_down_sync(FULL, uv[c], 1);
+            uw[c][2][0] = lane == 0 ? uh[c] : l;
+            uw[c][2][1] = uv[c];
+            uw[c][2][2] = lane == 31 ? uh[c] : rr;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            ac[c] = an[c];  // A_c of the window's centre row
+            an[c] = av[c];
+        }
+        if (r < 2) continue;
+        const int Y = yb + r - 2;
+        if (X >= W || Y >= H) continue;
+        float gax, gay;
+        sobel2(sw[0][0], sw[0][1], sw[0][2], sw[1][0], sw[1][2], sw[2][0], sw[2][1], sw[2][2], gax, gay);
+        const float alpha = alpha_fp(sw[1][1], fp);
+        const float oma = __fsub_rn(1.0f, alpha);
+        const float agx = __fmul_rn(alpha, gax), agy = __fmul_rn(alpha, gay);
+        const size_t cell = size_t(Y) * W + X;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            float gux, guy;
+            sobel2(uw[c][0][0], uw[c][0][1], uw[c][0][2], uw[c][1][0], uw[c][1][2], uw[c][2][0], uw[c][2][1],
+                   uw[c][2][2], gux, guy);
+            const float fx = __fsub_rn(__fmul_rn(oma, gux), agx);
+            const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
+            const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
+            const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
+            float mass = ac[c];
+            bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
+            if (fabsf(mass) < 1e-10f) mass = 0.f;
+            if (mass != 0.f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
+            DX[size_t(c) * N + cell] = dx;
+            DY[size_t(c) * N + cell] = dy;
+            MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
+        }
+    }
+    if (status && __syncthreads_or(bad ? 1 : 0) && threadIdx.x == 0) atomicOr(status, STATUS_NONFINITE);
+    block_max_atomic(dmax, bad, dmax_slot);
+}
+
 // ----------------------------------------------------------- gather_2d ----
 constexpr int GT_W = 64, GT_H = 16, TP = 4, RN_MAX = 3;
 constexpr int SR_W = GT_W + 2 * TP;             // 72 source columns (float4-aligned padding)
@@ -176,6 +284,41 @@ constexpr int SR_HMAX = GT_H + 2 * RN_MAX + 1;  // up to 23 source rows
 static_assert(SR_W % 4 == 0, "source rows must stay 16-byte aligned");
 
 inline size_t gather_smem_bytes_inl() { return sizeof(float) * 5 * SR_W * SR_HMAX; }
+
+// Stage the dx, dy and m planes of an SR_W x SRH source region (columns
+// colx[], rows rowy[]) into shared memory.  When W and the three base
+// pointers allow it, whole 16-byte chunks are copied: x0 - TP and W are
+// multiples of 4, so every chunk of 4 source columns is 4 contiguous, aligned
+// columns after the wrap.
+template <int SRH>
+__device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* smass, const float* __restrict__ DX,
+                                              const float* __restrict__ DY, const float* __restrict__ MS,
+                                              const int* colx, const int* rowy, int W) {
+    const int tid = threadIdx.x;
+    const bool vec = (W & 3) == 0 &&
+                     ((reinterpret_cast<uintptr_t>(DX) | reinterpret_cast<uintptr_t>(DY) |
+                       reinterpret_cast<uintptr_t>(MS)) & 15) == 0;
+    if (vec) {
+        constexpr int CH = SR_W / 4;
+        for (int i = tid; i < 3 * SRH * CH; i += 256) {
+            const int k = i / (SRH * CH), rem = i - k * (SRH * CH);
+            const int sy = rem / CH, c4 = rem - sy * CH;
+            const size_t idx = size_t(rowy[sy]) * W + colx[4 * c4];
+            const int cell = sy * SR_W + 4 * c4;
+            float* dst = k == 0 ? sdx + cell : (k == 1 ? sdy + cell : smass + cell);
+            cp_async16(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
+        }
+    } else {
+        constexpr int NS = SR_W * SRH;
+        for (int i = tid; i < 3 * NS; i += 256) {
+            const int k = i / NS, cell = i - k * NS;
+            const int sy = cell / SR_W, sx = cell - sy * SR_W;
+            const size_t idx = size_t(rowy[sy]) * W + colx[sx];
+            float* dst = k == 0 ? sdx + cell : (k == 1 ? sdy + cell : smass + cell);
+            cp_async4(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
+        }
+    }
+}
 
 __device__ __forceinline__ int wrap_pass(int g, int size) { return g >= size ? 0 : (g < 0 ? 2 : 1); }
 
@@ -293,21 +436,20 @@ __device__ void gather_body(float* sm, const float* __restrict__ DX, const float
     else if (tid < SR_W + SRH) rowy[tid - SR_W] = wrap_near(y0 - RN + (tid - SR_W), H);
     __syncthreads();
     // stage destinations and masses (dx -> xmin in place, dy -> ymin in place)
-    for (int i = tid; i < 3 * SR_W * SRH; i += 256) {
-        const int k = i / (SR_W * SRH), cell = i - k * (SR_W * SRH);
-        const int sy = cell / SR_W, sx = cell - sy * SR_W;
-        const size_t idx = size_t(rowy[sy]) * W + colx[sx];
-        float* dst = k == 0 ? sxmin + cell : (k == 1 ? symin + cell : smass + cell);
-        cp_async4(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
-    }
+    stage_sources<SRH>(sxmin, symin, smass, DX, DY, MS, colx, rowy, W);
     cp_async_wait_all();
     __syncthreads();
-    for (int i = tid; i < SR_W * SRH; i += 256) {
-        const float dx = sxmin[i], dy = symin[i];
-        sxmin[i] = __fsub_rn(dx, s);
-        sxmax[i] = __fadd_rn(dx, s);
-        symin[i] = __fsub_rn(dy, s);
-        symax[i] = __fadd_rn(dy, s);
+    for (int i = 4 * tid; i < SR_W * SRH; i += 1024) {
+        const float4 dx = *reinterpret_cast<const float4*>(sxmin + i);
+        const float4 dy = *reinterpret_cast<const float4*>(symin + i);
+        *reinterpret_cast<float4*>(sxmin + i) =
+            make_float4(__fsub_rn(dx.x, s), __fsub_rn(dx.y, s), __fsub_rn(dx.z, s), __fsub_rn(dx.w, s));
+        *reinterpret_cast<float4*>(sxmax + i) =
+            make_float4(__fadd_rn(dx.x, s), __fadd_rn(dx.y, s), __fadd_rn(dx.z, s), __fadd_rn(dx.w, s));
+        *reinterpret_cast<float4*>(symin + i) =
+            make_float4(__fsub_rn(dy.x, s), __fsub_rn(dy.y, s), __fsub_rn(dy.z, s), __fsub_rn(dy.w, s));
+        *reinterpret_cast<float4*>(symax + i) =
+            make_float4(__fadd_rn(dy.x, s), __fadd_rn(dy.y, s), __fadd_rn(dy.z, s), __fadd_rn(dy.w, s));
     }
     __syncthreads();
     const int Y = y0 + ty, X0 = x0 + 4 * tx;
