@@ -121,7 +121,7 @@ constexpr int G3_W = 32, G3_H = 8, G3_RNMAX = 2;
 constexpr int G3_SW = G3_W + 2 * G3_RNMAX + 1, G3_SH = G3_H + 2 * G3_RNMAX + 1, G3_SD = 2 * G3_RNMAX + 2;
 constexpr int G3_CELLS = G3_SW * G3_SH * G3_SD;
 
-size_t gather3d_smem_bytes() { return sizeof(float) * 4 * G3_CELLS; }
+
 
 // Overlap of one source cube with cell (ix, iy, iz): reintegration3d.rs:155-185.
 template <bool POW2>
@@ -247,30 +247,146 @@ __device__ float gather3d_generic(const float* __restrict__ DX, const float* __r
     return acc;
 }
 
+// ---- z-marching gather with overlap tables (RN <= 1) ----------------------
+// A CTA owns a 32x8 block of destination columns and G3_NZ consecutive
+// planes.  It keeps the 2RN+2 source planes that can reach the current
+// output plane in a ring in shared memory, each as per-source tables of the
+// x, y and z overlaps with the 2RN+2 candidate destination coordinates
+// (component k: destination = the source's own wrapped coordinate - (k - RN),
+// reintegration3d.rs:155-175) and the mass.  Each output plane loads one new
+// source plane.  A term is then vol = (ow * oh) * od, acc += m * vol: the
+// reference's operations, added in its deposit order (z, y, x over wrapped
+// source indices), with the overlap arithmetic done once per source instead
+// of once per (source, destination) pair.
+constexpr int G3_NZ = 8;
+
+template <int RN>
+struct March3 {
+    static constexpr int SW = G3_W + 2 * RN + 1, SH = G3_H + 2 * RN + 1, NS = SW * SH;
+    static constexpr int NW = 2 * RN + 2, SD = 2 * RN + 2;
+    static constexpr int PLANE = (3 * NW + 1) * NS;  // floats per ring slot
+    static constexpr size_t bytes = sizeof(float) * size_t(SD) * PLANE;
+};
+
+template <int RN, bool POW2>
+__device__ void gather3d_march(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
+                               const float* __restrict__ DZ, const float* __restrict__ MS, float* __restrict__ out,
+                               int W, int H, int D, int z0, int nz, const FlowParams& fp) {
+    using M = March3<RN>;
+    constexpr int SW = M::SW, SH = M::SH, NS = M::NS, NW = M::NW, SD = M::SD;
+    __shared__ int colx[March3<1>::SW], rowy[March3<1>::SH];
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * G3_W, y0 = blockIdx.y * G3_H;
+    if (tid < SW) colx[tid] = wrap_near(x0 - RN + tid, W);
+    else if (tid < SW + SH) rowy[tid - SW] = wrap_near(y0 - RN + (tid - SW), H);
+    __syncthreads();
+    const float s = fp.s;
+    auto load_plane = [&](int gz) {  // gz: unwrapped source plane, >= z0 - RN
+        float* P = sm + ((gz - (z0 - RN)) % SD) * M::PLANE;
+        float* OW = P;
+        float* OH = P + NW * NS;
+        float* OD = P + 2 * NW * NS;
+        float* Mm = P + 3 * NW * NS;
+        const int zw = wrap_near(gz, D);
+        const size_t zoff = size_t(zw) * H;
+        for (int i = tid; i < NS; i += 256) {
+            const int ly = i / SW, lx = i - ly * SW;
+            const int xw = colx[lx], yw = rowy[ly];
+            const size_t idx = (zoff + yw) * W + xw;
+            const float dx = DX[idx], dy = DY[idx], dz = DZ[idx];
+            Mm[i] = MS[idx];
+            const float xa = __fsub_rn(dx, s), xb = __fadd_rn(dx, s);
+            const float ya = __fsub_rn(dy, s), yb = __fadd_rn(dy, s);
+            const float za = __fsub_rn(dz, s), zb = __fadd_rn(dz, s);
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                const int ix = xw - (k - RN), iy = yw - (k - RN), iz = zw - (k - RN);
+                OW[k * NS + i] = fmaxf(__fsub_rn(fminf(float(ix + 1), xb), fmaxf(float(ix), xa)), 0.f);
+                OH[k * NS + i] = fmaxf(__fsub_rn(fminf(float(iy + 1), yb), fmaxf(float(iy), ya)), 0.f);
+                OD[k * NS + i] = fmaxf(__fsub_rn(fminf(float(iz + 1), zb), fmaxf(float(iz), za)), 0.f);
+            }
+        }
+    };
+    for (int gz = z0 - RN; gz <= z0 + RN; ++gz) load_plane(gz);
+    const int lx = tid & (G3_W - 1), ly = tid / G3_W;
+    const int X = x0 + lx, Y = y0 + ly;
+    for (int zz = 0; zz < nz; ++zz) {
+        const int Z = z0 + zz;
+        load_plane(Z + RN + 1);
+        __syncthreads();
+        if (X < W && Y < H) {
+            float acc = 0.f;
+            for (int jz = 0; jz < NW; ++jz) {
+                const int kz = rot_window(jz, Z, RN, D);
+                const float* P = sm + ((Z + kz - (z0 - RN)) % SD) * M::PLANE;
+                const float* OW = P;
+                const float* OHk = P + NW * NS;
+                const float* ODk = P + 2 * NW * NS + (kz + RN) * NS;
+                const float* Mm = P + 3 * NW * NS;
+                for (int jy = 0; jy < NW; ++jy) {
+                    const int ky = rot_window(jy, Y, RN, H);
+                    const int row = (ly + ky + RN) * SW + lx + RN;
+                    const float* OHr = OHk + (ky + RN) * NS;
+#pragma unroll
+                    for (int jx = 0; jx < NW; ++jx) {
+                        const int kx = rot_window(jx, X, RN, W);
+                        const int si = row + kx;
+                        const float m = Mm[si];
+                        if (!POW2 && m == 0.f) continue;
+                        const float vol = __fmul_rn(__fmul_rn(OW[(kx + RN) * NS + si], OHr[si]), ODk[si]);
+                        if (POW2) acc = __fadd_rn(acc, __fmul_rn(m, vol));
+                        else if (vol > 0.f) acc = __fadd_rn(acc, __fmul_rn(m, __fdiv_rn(vol, fp.total_area)));
+                    }
+                }
+            }
+            out[(size_t(Z) * H + Y) * W + X] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+inline size_t gather3d_dyn_smem() {
+    const size_t a = March3<1>::bytes, b = sizeof(float) * 4 * G3_CELLS;
+    return a > b ? a : b;
+}
+
+// Grid: (x tiles, y tiles, channels * z chunks of G3_NZ planes).
 template <bool POW2>
 __global__ void __launch_bounds__(256) gather_3d(const float* __restrict__ DX, const float* __restrict__ DY,
                                                  const float* __restrict__ DZ, const float* __restrict__ MS,
                                                  float* __restrict__ Anext, int C, int W, int H, int D, FlowParams fp,
                                                  const int* __restrict__ dmax_slot) {
     extern __shared__ __align__(16) float sm[];
-    const int c = blockIdx.z / D;
-    const int Z = blockIdx.z - c * D;
+    const int nchunk = (D + G3_NZ - 1) / G3_NZ;
+    const int c = blockIdx.z / nchunk;
+    const int z0 = (blockIdx.z - c * nchunk) * G3_NZ;
+    const int nz = min(G3_NZ, D - z0);
     const size_t N = size_t(W) * H * D, off = size_t(c) * N;
     const int RN = window_from_dmax(*dmax_slot, fp, max(max(W, H), D));
     const bool fast = RN <= G3_RNMAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && 2 * RN + 2 <= D && !fp.point_mode;
-    if (fast) {
-        switch (RN) {
-            case 0: gather3d_plane<0, POW2>(sm, DX + off, DY + off, DZ + off, MS + off, Anext + off, W, H, D, Z, fp); break;
-            case 1: gather3d_plane<1, POW2>(sm, DX + off, DY + off, DZ + off, MS + off, Anext + off, W, H, D, Z, fp); break;
-            default: gather3d_plane<2, POW2>(sm, DX + off, DY + off, DZ + off, MS + off, Anext + off, W, H, D, Z, fp); break;
-        }
+    const float *dx = DX + off, *dy = DY + off, *dz = DZ + off, *ms = MS + off;
+    float* o = Anext + off;
+    if (fast && RN == 0) {
+        gather3d_march<0, POW2>(sm, dx, dy, dz, ms, o, W, H, D, z0, nz, fp);
         return;
     }
-    const int X = blockIdx.x * G3_W + (threadIdx.x & (G3_W - 1)), Y = blockIdx.y * G3_H + (threadIdx.x / G3_W);
-    if (X < W && Y < H)
-        Anext[off + (size_t(Z) * H + Y) * W + X] =
-            gather3d_generic<POW2>(DX + off, DY + off, DZ + off, MS + off, W, H, D, X, Y, Z, RN + 1, fp);
+    if (fast && RN == 1) {
+        gather3d_march<1, POW2>(sm, dx, dy, dz, ms, o, W, H, D, z0, nz, fp);
+        return;
+    }
+    for (int Z = z0; Z < z0 + nz; ++Z) {
+        if (fast) {
+            gather3d_plane<2, POW2>(sm, dx, dy, dz, ms, o, W, H, D, Z, fp);
+            __syncthreads();
+        } else {
+            const int X = blockIdx.x * G3_W + (threadIdx.x & (G3_W - 1)), Y = blockIdx.y * G3_H + (threadIdx.x / G3_W);
+            if (X < W && Y < H)
+                o[(size_t(Z) * H + Y) * W + X] = gather3d_generic<POW2>(dx, dy, dz, ms, W, H, D, X, Y, Z, RN + 1, fp);
+        }
+    }
 }
+
+size_t gather3d_smem_bytes() { return gather3d_dyn_smem(); }
 
 void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
                     int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
@@ -283,7 +399,7 @@ void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float*
 
 void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
                       int H, int D, const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
-    dim3 grid((W + G3_W - 1) / G3_W, (H + G3_H - 1) / G3_H, C * D);
+    dim3 grid((W + G3_W - 1) / G3_W, (H + G3_H - 1) / G3_H, C * ((D + G3_NZ - 1) / G3_NZ));
     if (fp.area_pow2)
         gather_3d<true><<<grid, 256, gather3d_smem_bytes(), st>>>(DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
     else
