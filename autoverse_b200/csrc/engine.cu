@@ -132,6 +132,7 @@ struct flp_propagator {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // profiling
     std::vector<cudaEvent_t> prof_ev;
+    int prof_base = 0;  // first event of the step being recorded
     void* flush_buf = nullptr;
     size_t flush_bytes = 0;
 
@@ -566,13 +567,21 @@ static void invalidate_graphs(flp_propagator* h) {
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
-static void prof_hook(flp_propagator* h, int stage) { CK(cudaEventRecord(h->prof_ev[1 + stage], h->st)); }
+static void prof_hook(flp_propagator* h, int stage) {
+    CK(cudaEventRecord(h->prof_ev[h->prof_base + 1 + stage], h->st));
+}
 
 static void profile_run(flp_propagator* h, int steps, int flush, float* stage_ms, int max_stages, int* n_stages,
                         char* names, size_t names_len, float* step_ms) {
     std::vector<std::string> nm = h->stage_names();
     const int ns = int(nm.size());
-    while (int(h->prof_ev.size()) < ns + 1) {
+    // Up to RING steps in flight, each with its own ns+1 events, so that the
+    // host enqueues ahead and the device never waits for a launch inside a
+    // timed step; the L2 flush of a step is enqueued between the previous
+    // step's last event and this step's first one.
+    constexpr int RING = 32;
+    const int E = ns + 1;
+    while (int(h->prof_ev.size()) < RING * E) {
         cudaEvent_t e;
         CK(cudaEventCreate(&e));
         h->prof_ev.push_back(e);
@@ -586,23 +595,33 @@ static void profile_run(flp_propagator* h, int steps, int flush, float* stage_ms
     }
     std::vector<double> acc(ns, 0.0);
     double total = 0.0;
-    h->hook = prof_hook;
+    // Without stage_ms only the step is bracketed: no events between kernels.
+    const bool staged = stage_ms != nullptr;
+    auto harvest = [&](int slot) {
+        cudaEvent_t* ev = h->prof_ev.data() + size_t(slot) * E;
+        CK(cudaEventSynchronize(ev[ns]));
+        for (int i = 0; staged && i < ns; ++i) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+            acc[i] += ms;
+        }
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[0], ev[ns]));
+        total += ms;
+    };
+    h->hook = staged ? prof_hook : nullptr;
     try {
         for (int s = 0; s < steps; ++s) {
+            const int slot = s % RING;
+            if (s >= RING) harvest(slot);
             if (flush) CK(cudaMemsetAsync(h->flush_buf, s & 0xFF, h->flush_bytes, h->st));
-            CK(cudaEventRecord(h->prof_ev[0], h->st));
+            h->prof_base = slot * E;
+            CK(cudaEventRecord(h->prof_ev[h->prof_base], h->st));
             h->enqueue_step();
+            if (!staged) CK(cudaEventRecord(h->prof_ev[h->prof_base + ns], h->st));
             h->advance_clock(1);
-            CK(cudaEventSynchronize(h->prof_ev[ns]));
-            for (int i = 0; i < ns; ++i) {
-                float ms = 0.f;
-                CK(cudaEventElapsedTime(&ms, h->prof_ev[i], h->prof_ev[i + 1]));
-                acc[i] += ms;
-            }
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, h->prof_ev[0], h->prof_ev[ns]));
-            total += ms;
         }
+        for (int s = std::max(0, steps - RING); s < steps; ++s) harvest(s % RING);
     } catch (...) {
         h->hook = nullptr;
         throw;

@@ -249,18 +249,19 @@ class CudaPropagator:
     def stream(self) -> int:
         return nat.lib().flp_stream(self._h) or 0
 
-    def profile_run(self, steps: int, flush_l2: bool = True) -> dict:
-        """Run `steps` eager steps with CUDA events around every kernel; returns
-        summed device milliseconds per stage and per step (flp_profile_run)."""
+    def profile_run(self, steps: int, flush_l2: bool = True, stages: bool = True) -> dict:
+        """Run `steps` eager steps with CUDA events around every kernel (or,
+        with stages=False, around every step only); returns summed device
+        milliseconds per stage and per step (flp_profile_run)."""
         ms = (C.c_float * 16)()
         n = C.c_int()
         names = C.create_string_buffer(512)
         step_ms = C.c_float()
-        nat.check(nat.lib().flp_profile_run(self._h, int(steps), int(bool(flush_l2)), ms, 16, C.byref(n), names,
-                                            512, C.byref(step_ms)))
+        nat.check(nat.lib().flp_profile_run(self._h, int(steps), int(bool(flush_l2)), ms if stages else None, 16,
+                                            C.byref(n), names, 512, C.byref(step_ms)))
         stage_names = names.value.decode().split(",")
-        return {"stages": {stage_names[i]: ms[i] for i in range(n.value)}, "step_ms": step_ms.value,
-                "steps": int(steps), "launches_per_step": n.value}
+        return {"stages": {stage_names[i]: ms[i] for i in range(n.value)} if stages else {},
+                "step_ms": step_ms.value, "steps": int(steps), "launches_per_step": n.value}
 
     def debug_affinity(self) -> np.ndarray:
         info = self.info()

@@ -131,6 +131,8 @@ FLP_API int flp_host_free(void* p);
  * kernel.  Writes the summed device time of each stage (ms) to stage_ms[i]
  * (up to max_stages entries), the stage names (comma-separated) to names,
  * the number of stages to n_stages and the summed step time to step_ms.
+ * With stage_ms NULL only each step is bracketed (no events between its
+ * kernels) and only step_ms (and n_stages, names) are written.
  * Synchronous. */
 FLP_API int flp_profile_run(flp_propagator* h, int steps, int flush_l2, float* stage_ms, int max_stages,
                             int* n_stages, char* names, size_t names_len, float* step_ms);
