@@ -86,10 +86,13 @@ class BatchedPropagator:
     def stream(self) -> int:
         return nat.lib().flp_batch_stream(self._h) or 0
 
-    def profile_run(self, steps: int, flush_l2: bool = True) -> dict:
+    def profile_run(self, steps: int, flush_l2: bool = True, stages: bool = True) -> dict:
+        """Run `steps` eager steps with CUDA events between the stages (or,
+        with stages=False, around each step only); summed device ms."""
         ms = (C.c_float * 5)()
         step_ms = C.c_float()
-        nat.check(nat.lib().flp_batch_profile_run(self._h, int(steps), int(bool(flush_l2)), ms, C.byref(step_ms)))
+        nat.check(nat.lib().flp_batch_profile_run(self._h, int(steps), int(bool(flush_l2)), ms if stages else None,
+                                                  C.byref(step_ms)))
         names = ["batch_r2c", "batch_cols", "batch_c2r", "batch_flow", "batch_gather"]
-        return {"stages": {n: ms[i] for i, n in enumerate(names)}, "step_ms": step_ms.value, "steps": int(steps),
-                "launches_per_step": 5}
+        return {"stages": {n: ms[i] for i, n in enumerate(names)} if stages else {}, "step_ms": step_ms.value,
+                "steps": int(steps), "launches_per_step": 5}

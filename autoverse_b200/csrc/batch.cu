@@ -351,6 +351,7 @@ struct flp_batch {
     std::vector<uint64_t> steps;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     cudaEvent_t ev[NSTAGE + 1] = {nullptr};
+    std::vector<cudaEvent_t> pev;  // per-step event ring of the profiling entry
     void* flush_buf = nullptr;
     size_t flush_bytes = 0;
 
@@ -384,18 +385,20 @@ struct flp_batch {
     }
 
     // reset, then per stage the size-class kernels of that stage
-    void enqueue_step(bool timed = false) {
+    // evs (NSTAGE + 1 events, optional): evs[0] before the step, evs[NSTAGE]
+    // after it and, when staged, evs[1..NSTAGE-1] between the stages.
+    void enqueue_step(cudaEvent_t* evs = nullptr, bool staged = false) {
         Pools p = pools();
+        if (evs) ckb(cudaEventRecord(evs[0], st), "event");
         k_batch_reset<<<1, 256, 0, st>>>(p);
-        if (timed) ckb(cudaEventRecord(ev[0], st), "event");
         for (int stage = 0; stage < 3; ++stage) {
             for (int cls = 0; cls < NCLS; ++cls) launch_queue(stage * NCLS + cls, p);
-            if (timed) ckb(cudaEventRecord(ev[stage + 1], st), "event");
+            if (evs && staged) ckb(cudaEventRecord(evs[stage + 1], st), "event");
         }
         for (int v = 0; v < NFLOWQ; ++v) launch_queue(QF + v, p);
-        if (timed) ckb(cudaEventRecord(ev[4], st), "event");
+        if (evs && staged) ckb(cudaEventRecord(evs[4], st), "event");
         launch_queue(QG, p);
-        if (timed) ckb(cudaEventRecord(ev[5], st), "event");
+        if (evs) ckb(cudaEventRecord(evs[5], st), "event");
         ckb(cudaGetLastError(), "batch launch");
         cur ^= 1;
     }
@@ -412,6 +415,8 @@ struct flp_batch {
             if (g) cudaGraphExecDestroy(g);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : pev) cudaEventDestroy(e);
+        pev.clear();
         void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, MS, S, T,
                         KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf};
         for (void* q : ptrs)
@@ -814,21 +819,37 @@ int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms
             b->flush_bytes = std::max<size_t>(size_t(2) * size_t(l2), size_t(64) << 20);
             ckb(cudaMalloc(&b->flush_buf, b->flush_bytes), "flush buffer");
         }
+        // Up to RING steps in flight, each with its own events, so the host
+        // enqueues ahead of the device; without stage_ms only whole steps are
+        // bracketed.
+        constexpr int RING = 16, E = NSTAGE + 1;
+        while (int(b->pev.size()) < RING * E) {
+            cudaEvent_t e;
+            ckb(cudaEventCreate(&e), "event");
+            b->pev.push_back(e);
+        }
+        const bool staged = stage_ms != nullptr;
         double acc[NSTAGE] = {0}, tot = 0;
-        for (int s = 0; s < steps; ++s) {
-            if (flush_l2) ckb(cudaMemsetAsync(b->flush_buf, s & 0xFF, b->flush_bytes, b->st), "flush");
-            b->enqueue_step(true);
-            b->advance(1);
-            ckb(cudaEventSynchronize(b->ev[NSTAGE]), "sync");
-            for (int i = 0; i < NSTAGE; ++i) {
+        auto harvest = [&](int slot) {
+            cudaEvent_t* ev = b->pev.data() + size_t(slot) * E;
+            ckb(cudaEventSynchronize(ev[NSTAGE]), "sync");
+            for (int i = 0; staged && i < NSTAGE; ++i) {
                 float ms = 0.f;
-                ckb(cudaEventElapsedTime(&ms, b->ev[i], b->ev[i + 1]), "elapsed");
+                ckb(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "elapsed");
                 acc[i] += ms;
             }
             float ms = 0.f;
-            ckb(cudaEventElapsedTime(&ms, b->ev[0], b->ev[NSTAGE]), "elapsed");
+            ckb(cudaEventElapsedTime(&ms, ev[0], ev[NSTAGE]), "elapsed");
             tot += ms;
+        };
+        for (int s = 0; s < steps; ++s) {
+            const int slot = s % RING;
+            if (s >= RING) harvest(slot);
+            if (flush_l2) ckb(cudaMemsetAsync(b->flush_buf, s & 0xFF, b->flush_bytes, b->st), "flush");
+            b->enqueue_step(b->pev.data() + size_t(slot) * E, staged);
+            b->advance(1);
         }
+        for (int s = std::max(0, steps - RING); s < steps; ++s) harvest(s % RING);
         if (stage_ms)
             for (int i = 0; i < NSTAGE; ++i) stage_ms[i] = float(acc[i]);
         if (step_ms) *step_ms = float(tot);

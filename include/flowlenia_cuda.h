@@ -171,7 +171,8 @@ FLP_API int flp_batch_synchronize(flp_batch* b);
 FLP_API int flp_batch_total_mass(flp_batch* b, double* per_world, int n);
 FLP_API int flp_batch_info(flp_batch* b, int* n_worlds, size_t* cell_channels, size_t* cells);
 FLP_API void* flp_batch_stream(flp_batch* b);
-/* As flp_profile_run: 5 stages (r2c, cols, c2r, flow, gather). */
+/* As flp_profile_run: 5 stages (r2c, cols, c2r, flow, gather); stage_ms may be NULL
+ * (whole steps timed only). */
 FLP_API int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms, float* step_ms);
 
 /* ---- Differentiable step (adjoint) ------------------------------------
