@@ -75,6 +75,10 @@ SIGNATURES = {
     "flp_debug_affinity": (I, [P, P, Z]),
     "flp_affinity_noalloc": (I, [S, P, P, P]),
     "flp_batch_create": (I, [C.POINTER(C.c_char_p), I, PP]),
+    "flp_batch_stats": (I, [P, P, Z]),
+    "flp_batch_reserve_snapshots": (I, [P, I]),
+    "flp_batch_snapshot": (I, [P, I]),
+    "flp_batch_similarity": (I, [P, I, I, P, I]),
     "flp_adj_create": (I, [C.POINTER(C.c_char_p), I, PP]),
     "flp_adj_destroy": (I, [P]),
     "flp_adj_write_state": (I, [P, I, P, Z]),

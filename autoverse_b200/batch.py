@@ -96,3 +96,29 @@ class BatchedPropagator:
         names = ["batch_r2c", "batch_cols", "batch_c2r", "batch_flow", "batch_gather"]
         return {"stages": {n: ms[i] for i, n in enumerate(names)} if stages else {}, "step_ms": step_ms.value,
                 "steps": int(steps), "launches_per_step": 5}
+
+    # ---- trajectory statistics (fitness evaluation) -------------------------
+    NSTAT = 12
+    STAT_NAMES = ("total", "positive", "cx", "cy", "radius", "max", "active", "negative", "mean", "variance",
+                  "gradient_mean", "cells")
+
+    def stats(self) -> np.ndarray:
+        """(n_worlds, 12) statistics of each world's channel sum, reduced in FP64
+        on the device (flp_batch_stats; columns in STAT_NAMES order)."""
+        out = np.empty((len(self), self.NSTAT), dtype=np.float64)
+        nat.check(nat.lib().flp_batch_stats(self._h, out.ctypes.data, out.size))
+        return out
+
+    def reserve_snapshots(self, n_slots: int) -> None:
+        nat.check(nat.lib().flp_batch_reserve_snapshots(self._h, int(n_slots)))
+
+    def snapshot(self, slot: int) -> None:
+        """Keep every world's current channel sum in device slot `slot`."""
+        nat.check(nat.lib().flp_batch_snapshot(self._h, int(slot)))
+
+    def similarity(self, slot_a: int, slot_b: int) -> np.ndarray:
+        """Normalised dot product of two snapshot slots, per world."""
+        out = np.empty(len(self), dtype=np.float64)
+        nat.check(nat.lib().flp_batch_similarity(self._h, int(slot_a), int(slot_b), out.ctypes.data, out.size))
+        return out
+

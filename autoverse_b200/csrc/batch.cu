@@ -324,6 +324,129 @@ size_t cols_smem(int cls) {
 
 using namespace flp;
 
+// ---- per-world statistics of the channel sum (fitness evaluation) ----------
+// S = sum_c A_c per cell, channels added in order as SimulationState::
+// channel_sum does (propagator.rs:109-120); every reduction is FP64.
+__device__ __forceinline__ float chan_sum(const float* a, size_t N, int C, size_t i) {
+    float s = 0.f;
+    for (int c = 0; c < C; ++c) s = __fadd_rn(s, a[size_t(c) * N + i]);
+    return s;
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum_nd(double (&v)[NV], double (*red)[NV]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = 0.0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w][k];
+        v[k] = t;
+    }
+}
+
+// One CTA per world.  Writes FLP_BATCH_NSTAT doubles: total of S, total of
+// S > 0, centre of mass (x, y) of S > 0 (the grid centre when that total is at
+// most 1e-6), radius (second moment about it), max(0, max S), #(S > 1e-6),
+// #(S < 0), mean, variance, mean neighbour difference (left and up, no wrap,
+// over 2N), N (fitness.rs:195-240, 420-520).
+__global__ void __launch_bounds__(256) k_batch_stats(const BWorld* worlds, const float* A, double* out) {
+    __shared__ double red[8][8];
+    __shared__ float redm[8];
+    const BWorld w = worlds[blockIdx.x];
+    const size_t N = size_t(w.W) * w.H;
+    const float* a = A + w.offA;
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // total, pos, xm, ym, active, neg, grad, -
+    float mx = 0.f;
+    for (size_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const int x = int(i % w.W), y = int(i / w.W);
+        const float S = chan_sum(a, N, w.C, i);
+        v[0] += S;
+        if (S > 0.f) {
+            v[1] += S;
+            v[2] += double(x) * S;
+            v[3] += double(y) * S;
+        }
+        mx = fmaxf(mx, S);
+        v[4] += S > 1e-6f ? 1.0 : 0.0;
+        v[5] += S < 0.f ? 1.0 : 0.0;
+        if (x > 0) v[6] += fabs(double(S) - double(chan_sum(a, N, w.C, i - 1)));
+        if (y > 0) v[6] += fabs(double(S) - double(chan_sum(a, N, w.C, i - w.W)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) redm[threadIdx.x >> 5] = mx;
+    block_sum_nd<8>(v, red);
+    for (int k = 0; k < int(blockDim.x >> 5); ++k) mx = fmaxf(mx, redm[k]);
+    const bool has = v[1] > 1e-6;
+    const double cx = has ? v[2] / v[1] : 0.5 * w.W, cy = has ? v[3] / v[1] : 0.5 * w.H;
+    const double mean = v[0] / double(N);
+    double u[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // moment, sum of squared deviations
+    for (size_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const double x = double(i % w.W), y = double(i / w.W);
+        const double S = chan_sum(a, N, w.C, i);
+        if (S > 0.0) u[0] += S * ((x - cx) * (x - cx) + (y - cy) * (y - cy));
+        u[1] += (S - mean) * (S - mean);
+    }
+    block_sum_nd<8>(u, red);
+    if (threadIdx.x == 0) {
+        double* o = out + size_t(blockIdx.x) * FLP_BATCH_NSTAT;
+        o[0] = v[0];
+        o[1] = v[1];
+        o[2] = cx;
+        o[3] = cy;
+        o[4] = has ? sqrt(u[0] / v[1]) : 0.0;
+        o[5] = double(mx);
+        o[6] = v[4];
+        o[7] = v[5];
+        o[8] = mean;
+        o[9] = u[1] / double(N);
+        o[10] = v[6] / (2.0 * double(N));
+        o[11] = double(N);
+    }
+}
+
+// Channel sums of every world into snapshot slot `slot` (cells of world w at
+// cell_off[w]).
+__global__ void __launch_bounds__(256) k_batch_snapshot(const BWorld* worlds, const float* A,
+                                                        const long long* cell_off, float* snaps, size_t cells,
+                                                        int slot) {
+    const BWorld w = worlds[blockIdx.x];
+    const size_t N = size_t(w.W) * w.H;
+    float* dst = snaps + size_t(slot) * cells + size_t(cell_off[blockIdx.x]);
+    for (size_t i = threadIdx.x; i < N; i += blockDim.x) dst[i] = chan_sum(A + w.offA, N, w.C, i);
+}
+
+// Normalised dot product of two snapshots of every world (fitness.rs:337-350),
+// 0 when either norm is at most 1e-6.
+__global__ void __launch_bounds__(256) k_batch_similarity(const BWorld* worlds, const long long* cell_off,
+                                                          const float* snaps, size_t cells, int sa, int sb,
+                                                          double* out) {
+    __shared__ double red[8][4];
+    const BWorld w = worlds[blockIdx.x];
+    const size_t N = size_t(w.W) * w.H;
+    const float* pa = snaps + size_t(sa) * cells + size_t(cell_off[blockIdx.x]);
+    const float* pb = snaps + size_t(sb) * cells + size_t(cell_off[blockIdx.x]);
+    double v[4] = {0, 0, 0, 0};
+    for (size_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const double x = pa[i], y = pb[i];
+        v[0] += x * y;
+        v[1] += x * x;
+        v[2] += y * y;
+    }
+    block_sum_nd<4>(v, red);
+    if (threadIdx.x == 0) {
+        const double na = sqrt(v[1]), nb = sqrt(v[2]);
+        out[blockIdx.x] = (na > 1e-6 && nb > 1e-6) ? v[0] / (na * nb) : 0.0;
+    }
+}
+
 struct flp_batch {
     std::vector<SimulationConfig> cfgs;
     std::vector<BWorld> hw;
@@ -343,6 +466,11 @@ struct flp_batch {
     KDesc* d_kd = nullptr;
     int *d_srcs = nullptr, *d_slots = nullptr;
     double* d_mass = nullptr;
+    double* d_stats = nullptr;        // n x FLP_BATCH_NSTAT
+    long long* d_celloff = nullptr;   // first cell of each world in a snapshot slot
+    float* d_snaps = nullptr;         // n_snap slots of sum_w W*H floats
+    int n_snap = 0;
+    size_t cells = 0;                 // sum over worlds of W*H
     int cur = 0;
     const void* q_fn[NQUEUE] = {nullptr};
     int q_grid[NQUEUE] = {0};
@@ -418,7 +546,7 @@ struct flp_batch {
         for (cudaEvent_t e : pev) cudaEventDestroy(e);
         pev.clear();
         void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, MS, S, T,
-                        KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf};
+                        KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf, d_stats, d_celloff, d_snaps};
         for (void* q : ptrs)
             if (q) cudaFree(q);
         if (st) cudaStreamDestroy(st);
@@ -542,6 +670,18 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     b->d_dmax = dalloc_b<int>(n);
     b->d_status = dalloc_b<int>(1);
     b->d_mass = dalloc_b<double>(n);
+    b->d_stats = dalloc_b<double>(size_t(n) * FLP_BATCH_NSTAT);
+    {
+        std::vector<long long> co(n);
+        long long acc = 0;
+        for (int w = 0; w < n; ++w) {
+            co[w] = acc;
+            acc += (long long)b->hw[w].W * b->hw[w].H;
+        }
+        b->cells = size_t(acc);
+        b->d_celloff = dalloc_b<long long>(n);
+        ckb(cudaMemcpy(b->d_celloff, co.data(), n * sizeof(long long), cudaMemcpyHostToDevice), "copy");
+    }
     ckb(cudaMemsetAsync(b->d_counters, 0, NQUEUE * sizeof(int), b->st), "memset");
     ckb(cudaMemsetAsync(b->d_status, 0, sizeof(int), b->st), "memset");
     ckb(cudaMemcpy(b->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice), "copy");
@@ -789,6 +929,56 @@ int flp_batch_total_mass(flp_batch* b, double* per_world, int n) {
         k_batch_mass<<<b->n, 256, 0, b->st>>>(b->d_worlds, b->A[b->cur], b->d_mass);
         ckb(cudaGetLastError(), "mass");
         ckb(cudaMemcpyAsync(per_world, b->d_mass, n * sizeof(double), cudaMemcpyDeviceToHost, b->st), "copy");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+    })
+}
+
+int flp_batch_stats(flp_batch* b, double* out, size_t n) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (!out || n != size_t(b->n) * FLP_BATCH_NSTAT)
+            throw std::invalid_argument("output needs FLP_BATCH_NSTAT doubles per world");
+        k_batch_stats<<<b->n, 256, 0, b->st>>>(b->d_worlds, b->A[b->cur], b->d_stats);
+        ckb(cudaGetLastError(), "stats");
+        ckb(cudaMemcpyAsync(out, b->d_stats, n * sizeof(double), cudaMemcpyDeviceToHost, b->st), "copy");
+        ckb(cudaStreamSynchronize(b->st), "sync");
+    })
+}
+
+int flp_batch_reserve_snapshots(flp_batch* b, int n_slots) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (n_slots < 0) throw std::invalid_argument("negative slot count");
+        if (n_slots <= b->n_snap) return FLP_OK;
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        if (b->d_snaps) cudaFree(b->d_snaps);
+        b->d_snaps = nullptr;
+        b->n_snap = 0;
+        b->d_snaps = dalloc_b<float>(size_t(n_slots) * b->cells);
+        b->n_snap = n_slots;
+    })
+}
+
+int flp_batch_snapshot(flp_batch* b, int slot) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (slot < 0 || slot >= b->n_snap) throw std::invalid_argument("snapshot slot out of range");
+        k_batch_snapshot<<<b->n, 256, 0, b->st>>>(b->d_worlds, b->A[b->cur], b->d_celloff, b->d_snaps, b->cells,
+                                                  slot);
+        ckb(cudaGetLastError(), "snapshot");
+    })
+}
+
+int flp_batch_similarity(flp_batch* b, int slot_a, int slot_b, double* out, int n) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (slot_a < 0 || slot_b < 0 || slot_a >= b->n_snap || slot_b >= b->n_snap)
+            throw std::invalid_argument("snapshot slot out of range");
+        if (!out || n != b->n) throw std::invalid_argument("output needs one double per world");
+        k_batch_similarity<<<b->n, 256, 0, b->st>>>(b->d_worlds, b->d_celloff, b->d_snaps, b->cells, slot_a, slot_b,
+                                                    b->d_stats);
+        ckb(cudaGetLastError(), "similarity");
+        ckb(cudaMemcpyAsync(out, b->d_stats, n * sizeof(double), cudaMemcpyDeviceToHost, b->st), "copy");
         ckb(cudaStreamSynchronize(b->st), "sync");
     })
 }

@@ -171,6 +171,22 @@ FLP_API int flp_batch_synchronize(flp_batch* b);
 FLP_API int flp_batch_total_mass(flp_batch* b, double* per_world, int n);
 FLP_API int flp_batch_info(flp_batch* b, int* n_worlds, size_t* cell_channels, size_t* cells);
 FLP_API void* flp_batch_stream(flp_batch* b);
+/* Trajectory statistics for fitness evaluation (the quantities the reference's
+ * FitnessEvaluator samples, src/compute/evolution/fitness.rs:96-240 and
+ * 420-520), for every world at once, of the channel sum S of its current
+ * state, reduced in FP64 on the device.  Per world FLP_BATCH_NSTAT doubles:
+ *   0 sum S   1 sum of S > 0   2,3 centre of mass (x, y) of S > 0 (grid centre
+ *   when that sum <= 1e-6)   4 radius (second moment about it)
+ *   5 max(0, max S)   6 #(S > 1e-6)   7 #(S < 0)   8 mean   9 variance
+ *   10 mean |S - left| + |S - up| over 2N (no wrap)   11 N. */
+#define FLP_BATCH_NSTAT 12
+FLP_API int flp_batch_stats(flp_batch* b, double* out, size_t n);
+/* Device snapshots of every world's channel sum: reserve n_slots slots (kept
+ * across calls), copy the current state's channel sums into a slot, and the
+ * normalised dot product of two slots per world (0 when a norm <= 1e-6). */
+FLP_API int flp_batch_reserve_snapshots(flp_batch* b, int n_slots);
+FLP_API int flp_batch_snapshot(flp_batch* b, int slot);
+FLP_API int flp_batch_similarity(flp_batch* b, int slot_a, int slot_b, double* out, int n);
 /* As flp_profile_run: 5 stages (r2c, cols, c2r, flow, gather); stage_ms may be NULL
  * (whole steps timed only). */
 FLP_API int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms, float* step_ms);
