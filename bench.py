@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--adjoint-worlds", type=int, default=64, help="worlds in the adjoint measurement (0 = skip)")
     ap.add_argument("--adjoint-steps", type=int, default=64)
     ap.add_argument("--adjoint-every", type=int, default=8)
+    ap.add_argument("--fitness-candidates", type=int, default=512, help="population of the fitness measurement (0 = skip)")
     return ap.parse_args()
 
 
@@ -327,6 +328,39 @@ def measure_adjoint(args, dist):
             "forward_cell_steps_per_s": cells / (f / 1e3), "backward_cell_steps_per_s": cells / (g / 1e3)}
 
 
+def measure_fitness(args, dist):
+    """Population fitness: `--fitness-candidates` candidates (worlds of sides
+    {64,96,128}, 1-2 channels, the batched-world parameter distributions) each
+    evaluated for 200 steps with a sample every 10 and the reference's default
+    metrics (Persistence 1.0, Compactness 0.5), all in one batch through the
+    public API; wall clock around the whole evaluation.  CPU leg: the
+    restatement of the reference's evaluator over the oracle, one candidate
+    after another on one core, on the first 4 candidates."""
+    import autoverse_b200.fitness as FT
+    from autoverse_b200 import workloads as wl
+    pop = wl.batched_worlds(args.fitness_candidates, sides=(64, 96, 128), seed=wl.DEFAULT_SEED + 23 + RANK)
+    cfgs, seeds = [c for c, _ in pop], [s for _, s in pop]
+    FT.evaluate_population(cfgs[:8], seeds[:8], evaluation={"steps": 10})  # warm-up
+    t0 = time.perf_counter()
+    res = FT.evaluate_population(cfgs, seeds)
+    t = reduce_max(dist, time.perf_counter() - t0)
+    cells = sum(c["width"] * c["height"] for c in cfgs)
+    out = {"workload": f"{args.fitness_candidates} candidates per GPU, sides {{64,96,128}}, 200 steps, sample every 10, "
+                       "metrics Persistence 1.0 + Compactness 0.5",
+           "candidates_per_s": WORLD * len(cfgs) / t, "cell_steps_per_s": WORLD * cells * 200 / t, "seconds": t,
+           "mean_fitness": float(np.mean([r["fitness"] for r in res]))}
+    if RANK == 0 and not args.skip_cpu:
+        from oracle import fitness_ref as FR
+        t0 = time.perf_counter()
+        for c, sd in zip(cfgs[:4], seeds[:4]):
+            FR.evaluate(c, sd, FT.DEFAULT_FITNESS, FT.DEFAULT_EVALUATION)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"candidates_per_s": 4 / dt, "cores": 1, "kind": "port",
+                               "sample": "4 candidates, one after another (the reference runs candidates in "
+                                         "parallel over a rayon pool, one per core)"}
+    return out
+
+
 def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
@@ -412,6 +446,7 @@ def main():
 
     batched = measure_batched(args, dist) if args.batch_worlds > 0 else None
     adjoint = measure_adjoint(args, dist) if args.adjoint_worlds > 0 else None
+    fitness = measure_fitness(args, dist) if args.fitness_candidates > 0 else None
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
@@ -446,6 +481,7 @@ def main():
         "batched_over_plain": batched["small_worlds_batched_over_plain"]["ratio"] if batched else None,
         "adjoint": adjoint,
         "backward_over_forward": adjoint["backward_over_forward"] if adjoint else None,
+        "fitness": fitness,
     }
     print(json.dumps(line), flush=True)
 
