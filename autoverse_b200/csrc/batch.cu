@@ -34,6 +34,7 @@ extern thread_local std::string g_last_error;
 
 namespace {
 
+constexpr int BATCH_ROW_ELEMS = 2048;  // complex values per CTA in the batched row passes
 constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
 constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
 constexpr int NSTAGE = 5;
@@ -51,7 +52,7 @@ int col_class(int H) {
 }
 int row_nr(int M) {
     switch (M) {
-#define X(n) case n: return RowCfg<n>::NR;
+#define X(n) case n: return RowCfg<n, BATCH_ROW_ELEMS>::NR;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
         const int c = p.srcs[w.offSrc + slot];
         const size_t N = size_t(2 * M) * w.H;
         float2* Sc = p.S + w.offS + size_t(slot) * (M + 1) * w.H;
-        r2c_rows_item<M>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * RowCfg<M>::NR, p.tw + w.twM, p.tw + w.twW);
+        r2c_rows_item<M, BATCH_ROW_ELEMS>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * RowCfg<M, BATCH_ROW_ELEMS>::NR, p.tw + w.twM, p.tw + w.twW);
     }
 }
 
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
         const BWorld w = p.worlds[item.x];
         const int c = item.y >> 16, g = item.y & 0xFFFF;
         float* Uc = p.U + w.offA + size_t(c) * (2 * M) * w.H;
-        c2r_growth_item<M>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H, g * RowCfg<M>::NR, p.tw + w.twM,
+        c2r_growth_item<M, BATCH_ROW_ELEMS>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H, g * RowCfg<M, BATCH_ROW_ELEMS>::NR, p.tw + w.twM,
                            p.tw + w.twW);
     }
 }
@@ -296,7 +297,7 @@ const void* cols_fn(int cls) {
 }
 size_t r2c_smem(int cls) {
     switch (ROW_SIZES[cls]) {
-#define X(n) case n: return RowCfg<n>::smem_r2c;
+#define X(n) case n: return RowCfg<n, BATCH_ROW_ELEMS>::smem_r2c;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -304,7 +305,7 @@ size_t r2c_smem(int cls) {
 }
 size_t c2r_smem(int cls) {
     switch (ROW_SIZES[cls]) {
-#define X(n) case n: return RowCfg<n>::smem_c2r;
+#define X(n) case n: return RowCfg<n, BATCH_ROW_ELEMS>::smem_c2r;
         FLP_ROW_SIZES(X)
 #undef X
     }

@@ -170,11 +170,14 @@ __device__ __forceinline__ float2* ct_fft(float2* a, float2* b, const float2* __
     }
 }
 
-// Rows per CTA for a row pass of half-length M, columns per CTA for a column
-// pass of length H: about 2048 complex values per CTA.
-template <int M>
+// Rows per CTA for a row pass of half-length M (E complex values per CTA: 1024
+// for the single-world kernels, which run under one wave and want many CTAs;
+// 2048 for the batched ones, which are throughput-bound and keep all threads
+// of a CTA busy in the radix-8 stages), columns per CTA for a column pass of
+// length H: about 2048 complex values per CTA.
+template <int M, int E = 1024>
 struct RowCfg {
-    static constexpr int NR = M >= 256 ? 4 : (1024 / M);
+    static constexpr int NR = (E / M) < 1 ? 1 : (E / M);  // E complex values per CTA
     static constexpr int LS = CtPlan<M>::LS;
     static constexpr size_t buf = size_t(NR) * LS;  // float2 per buffer (LS > M+1)
     static constexpr size_t smem_r2c = sizeof(float2) * (M + M + 1 + 2 * buf);
@@ -191,14 +194,14 @@ struct ColCfg {
 // ---- items: one CTA's share of a pass, shared by the plain and batched launches
 
 // NR rows of one real plane -> transposed half spectra S[kx][y0..y0+NR).
-template <int M>
+template <int M, int E = 1024>
 __device__ void r2c_rows_item(float2* sm, const float* __restrict__ x, float2* __restrict__ Sc, int H, int y0,
                               const float2* __restrict__ twM_g, const float2* __restrict__ twW_g) {
-    constexpr int NR = RowCfg<M>::NR, LS = RowCfg<M>::LS, Wc = M + 1, W = 2 * M;
+    constexpr int NR = RowCfg<M, E>::NR, LS = RowCfg<M, E>::LS, Wc = M + 1, W = 2 * M;
     float2* twM = sm;
     float2* twW = twM + M;
     float2* a = twW + Wc;
-    float2* b = a + RowCfg<M>::buf;
+    float2* b = a + RowCfg<M, E>::buf;
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += 256) twM[i] = twM_g[i];
     for (int i = tid; i < Wc; i += 256) twW[i] = twW_g[i];
@@ -348,16 +351,16 @@ __device__ void zconv_item(float2* sm, const float2* __restrict__ src, const flo
 
 // NR rows of one target channel: inverse real FFT of each kernel spectrum
 // targeting it (kernel order), growth, weighted sum -> U rows.
-template <int M>
+template <int M, int E = 1024>
 __device__ void c2r_growth_item(float2* sm, const float2* __restrict__ T, const KDesc* __restrict__ kd, int K, int c,
                                 float* __restrict__ Uc, int H, int y0, const float2* __restrict__ twM_g,
                                 const float2* __restrict__ twW_g) {
-    constexpr int NR = RowCfg<M>::NR, LS = RowCfg<M>::LS, Wc = M + 1, W = 2 * M;
+    constexpr int NR = RowCfg<M, E>::NR, LS = RowCfg<M, E>::LS, Wc = M + 1, W = 2 * M;
     float2* twM = sm;
     float2* twW = twM + M;
     float2* a = twW + Wc;
-    float2* b = a + RowCfg<M>::buf;
-    float* u = reinterpret_cast<float*>(b + RowCfg<M>::buf);
+    float2* b = a + RowCfg<M, E>::buf;
+    float* u = reinterpret_cast<float*>(b + RowCfg<M, E>::buf);
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += 256) twM[i] = twM_g[i];
     for (int i = tid; i < Wc; i += 256) twW[i] = twW_g[i];
@@ -410,15 +413,15 @@ __device__ void c2r_growth_item(float2* sm, const float2* __restrict__ T, const 
 // NR rows of one spectrum slot: inverse real FFT, times `scale`, written to
 // (or, with accumulate, added to) the rows of `out`.  Same arithmetic as the
 // growth epilogue's inverse, without the growth.
-template <int M>
+template <int M, int E = 1024>
 __device__ void c2r_raw_item(float2* sm, const float2* __restrict__ t, float* __restrict__ out, int H, int y0,
                              float scale, bool accumulate, const float2* __restrict__ twM_g,
                              const float2* __restrict__ twW_g) {
-    constexpr int NR = RowCfg<M>::NR, LS = RowCfg<M>::LS, Wc = M + 1, W = 2 * M;
+    constexpr int NR = RowCfg<M, E>::NR, LS = RowCfg<M, E>::LS, Wc = M + 1, W = 2 * M;
     float2* twM = sm;
     float2* twW = twM + M;
     float2* a = twW + Wc;
-    float2* b = a + RowCfg<M>::buf;
+    float2* b = a + RowCfg<M, E>::buf;
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += 256) twM[i] = twM_g[i];
     for (int i = tid; i < Wc; i += 256) twW[i] = twW_g[i];

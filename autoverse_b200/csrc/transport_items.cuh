@@ -279,7 +279,11 @@ __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, cons
 
 // ----------------------------------------------------------- gather_2d ----
 constexpr int GT_W = 64, GT_H = 16, TP = 4, RN_MAX = 3;
-constexpr int SR_W = GT_W + 2 * TP;             // 72 source columns (float4-aligned padding)
+// Staged source columns: x0 - TP .. x0 + GT_W + TP - 1 plus 4 unused ones, so
+// that a row is 76 floats: with the column-major thread mapping of the gather
+// (a warp is 2 x 16 threads, 16 rows apart) the rows of a quarter-warp then
+// start in distinct bank groups.
+constexpr int SR_W = GT_W + 2 * TP + 4;
 constexpr int SR_HMAX = GT_H + 2 * RN_MAX + 1;  // up to 23 source rows
 static_assert(SR_W % 4 == 0, "source rows must stay 16-byte aligned");
 
@@ -290,7 +294,7 @@ inline size_t gather_smem_bytes_inl() { return sizeof(float) * 5 * SR_W * SR_HMA
 // pointers allow it, whole 16-byte chunks are copied: x0 - TP and W are
 // multiples of 4, so every chunk of 4 source columns is 4 contiguous, aligned
 // columns after the wrap.
-template <int SRH>
+template <int SRH, int SW>
 __device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* smass, const float* __restrict__ DX,
                                               const float* __restrict__ DY, const float* __restrict__ MS,
                                               const int* colx, const int* rowy, int W) {
@@ -299,20 +303,20 @@ __device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* sma
                      ((reinterpret_cast<uintptr_t>(DX) | reinterpret_cast<uintptr_t>(DY) |
                        reinterpret_cast<uintptr_t>(MS)) & 15) == 0;
     if (vec) {
-        constexpr int CH = SR_W / 4;
+        constexpr int CH = SW / 4;
         for (int i = tid; i < 3 * SRH * CH; i += 256) {
             const int k = i / (SRH * CH), rem = i - k * (SRH * CH);
             const int sy = rem / CH, c4 = rem - sy * CH;
             const size_t idx = size_t(rowy[sy]) * W + colx[4 * c4];
-            const int cell = sy * SR_W + 4 * c4;
+            const int cell = sy * SW + 4 * c4;
             float* dst = k == 0 ? sdx + cell : (k == 1 ? sdy + cell : smass + cell);
             cp_async16(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
         }
     } else {
-        constexpr int NS = SR_W * SRH;
+        constexpr int NS = SW * SRH;
         for (int i = tid; i < 3 * NS; i += 256) {
             const int k = i / NS, cell = i - k * NS;
-            const int sy = cell / SR_W, sx = cell - sy * SR_W;
+            const int sy = cell / SW, sx = cell - sy * SW;
             const size_t idx = size_t(rowy[sy]) * W + colx[sx];
             float* dst = k == 0 ? sdx + cell : (k == 1 ? sdy + cell : smass + cell);
             cp_async4(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
@@ -321,6 +325,14 @@ __device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* sma
 }
 
 __device__ __forceinline__ int wrap_pass(int g, int size) { return g >= size ? 0 : (g < 0 ? 2 : 1); }
+
+// Whether a gather tile uses the column-major thread mapping: tiles whose
+// sources reach across an x edge of the torus.  Each thread takes the wrap
+// passes of its own window, and with this mapping the threads that need more
+// than one pass sit in the two edge warps instead of in every warp.
+__device__ __forceinline__ bool gather_column_major(int x0, int W, int RN) {
+    return x0 - RN < 0 || x0 + GT_W + RN >= W;
+}
 
 // One source row of the gather for the thread's 4 destinations X0..X0+3.
 // Source column j of the strip window is x0-TP+4tx+j; its offset from
@@ -383,11 +395,16 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
 template <int RN, bool POW2>
 __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sxmax, const float* symin,
                                              const float* symax, const float* smass, float* __restrict__ out, int W,
-                                             int H, const FlowParams& fp, int x0, int y0, float (&acc)[4]) {
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+                                             int H, const FlowParams& fp, int x0, int y0, int sw, float (&acc)[4]) {
+    // Tiles at an x edge of the torus use the column-major mapping (a warp owns
+    // 2 columns of 4 destinations x 16 rows), so only the two warps at the
+    // edge take the wrap-pass path; other tiles map a warp to 2 rows.
+    const bool cm = gather_column_major(x0, W, RN);
+    const int tx = cm ? threadIdx.x >> 4 : threadIdx.x & 15, ty = cm ? threadIdx.x & 15 : threadIdx.x >> 4;
     const int Y = y0 + ty, X0 = x0 + 4 * tx;
-    const int rp_lo = (y0 + GT_H + RN >= H) ? 0 : 1, rp_hi = (y0 - RN < 0) ? 2 : 1;
-    const int cp_lo = (x0 + GT_W + RN >= W) ? 0 : 1, cp_hi = (x0 - RN < 0) ? 2 : 1;
+    // wrap passes of this thread's own window (sources X0-RN .. X0+4+RN, Y-RN .. Y+RN+1)
+    const int rp_lo = (Y + RN + 1 >= H) ? 0 : 1, rp_hi = (Y - RN < 0) ? 2 : 1;
+    const int cp_lo = (X0 + 4 + RN >= W) ? 0 : 1, cp_hi = (X0 - RN < 0) ? 2 : 1;
     const bool xin = cp_lo == 1 && cp_hi == 1;
     const int gx_base = x0 - TP + 4 * tx;
     for (int rp = rp_lo; rp <= rp_hi; ++rp) {
@@ -397,7 +414,7 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
             if (wrap_pass(gy, H) != rp) continue;
             const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
             const float cy0 = float(iy), cy1 = float(iy + 1);
-            const int off = (ty + RN + ky) * SR_W + 4 * tx;
+            const int off = (ty + RN + ky) * sw + 4 * tx;
             if (xin) {
                 gather_row<RN, POW2, false>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off, cy0,
                                             cy1, X0, gx_base, W, 1, fp.total_area, acc);
@@ -423,23 +440,26 @@ __device__ void gather_body(float* sm, const float* __restrict__ DX, const float
                             const float* __restrict__ MS, float* __restrict__ out, int W, int H, const FlowParams& fp,
                             int x0, int y0, float (&acc)[4]) {
     constexpr int SRH = GT_H + 2 * RN + 1;
-    float* sxmin = sm;                  // SRH x SR_W each
-    float* sxmax = sxmin + SR_W * SRH;
-    float* symin = sxmax + SR_W * SRH;
-    float* symax = symin + SR_W * SRH;
-    float* smass = symax + SR_W * SRH;
-    __shared__ int colx[SR_W], rowy[SRH];
     const int tid = threadIdx.x;
-    const int tx = tid & 15, ty = tid >> 4;
+    const bool cm = gather_column_major(x0, W, RN);
+    const int tx = cm ? tid >> 4 : tid & 15, ty = cm ? tid & 15 : tid >> 4;
+    const int sw = cm ? SR_W : SR_W - 4;  // row stride: padded only for the column-major mapping
+    float* sxmin = sm;                    // SRH x sw each
+    float* sxmax = sxmin + sw * SRH;
+    float* symin = sxmax + sw * SRH;
+    float* symax = symin + sw * SRH;
+    float* smass = symax + sw * SRH;
+    __shared__ int colx[SR_W], rowy[SRH];
     const float s = fp.s;
     if (tid < SR_W) colx[tid] = wrap_near(x0 - TP + tid, W);
     else if (tid < SR_W + SRH) rowy[tid - SR_W] = wrap_near(y0 - RN + (tid - SR_W), H);
     __syncthreads();
     // stage destinations and masses (dx -> xmin in place, dy -> ymin in place)
-    stage_sources<SRH>(sxmin, symin, smass, DX, DY, MS, colx, rowy, W);
+    if (cm) stage_sources<SRH, SR_W>(sxmin, symin, smass, DX, DY, MS, colx, rowy, W);
+    else stage_sources<SRH, SR_W - 4>(sxmin, symin, smass, DX, DY, MS, colx, rowy, W);
     cp_async_wait_all();
     __syncthreads();
-    for (int i = 4 * tid; i < SR_W * SRH; i += 1024) {
+    for (int i = 4 * tid; i < sw * SRH; i += 1024) {
         const float4 dx = *reinterpret_cast<const float4*>(sxmin + i);
         const float4 dy = *reinterpret_cast<const float4*>(symin + i);
         *reinterpret_cast<float4*>(sxmin + i) =
@@ -453,7 +473,8 @@ __device__ void gather_body(float* sm, const float* __restrict__ DX, const float
     }
     __syncthreads();
     const int Y = y0 + ty, X0 = x0 + 4 * tx;
-    if (Y < H && X0 < W) gather_strip<RN, POW2>(sxmin, sxmax, symin, symax, smass, out, W, H, fp, x0, y0, acc);
+    if (Y < H && X0 < W)
+        gather_strip<RN, POW2>(sxmin, sxmax, symin, symax, smass, out, W, H, fp, x0, y0, sw, acc);
     __syncthreads();
 }
 
