@@ -16,6 +16,15 @@ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 
+// 8-byte asynchronous copy global -> shared (both 8-byte aligned), and the
+// commit / wait of the copies issued so far.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_groups() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // ------------------------------------------------- compile-time FFTs -----
 // For the line lengths of the benchmarked worlds every size, radix, stride and
 // thread mapping is a compile-time constant.  Lines sit contiguously in shared
@@ -181,7 +190,8 @@ struct RowCfg {
     static constexpr int LS = CtPlan<M>::LS;
     static constexpr size_t buf = size_t(NR) * LS;  // float2 per buffer (LS > M+1)
     static constexpr size_t smem_r2c = sizeof(float2) * (M + M + 1 + 2 * buf);
-    static constexpr size_t smem_c2r = smem_r2c + sizeof(float) * NR * 2 * M;
+    // plus the U rows and a prefetch buffer for the next kernel's rows
+    static constexpr size_t smem_c2r = smem_r2c + sizeof(float) * NR * 2 * M + sizeof(float2) * buf;
 };
 template <int H>
 struct ColCfg {
@@ -361,33 +371,46 @@ __device__ void c2r_growth_item(float2* sm, const float2* __restrict__ T, const 
     float2* a = twW + Wc;
     float2* b = a + RowCfg<M, E>::buf;
     float* u = reinterpret_cast<float*>(b + RowCfg<M, E>::buf);
+    float2* pre = reinterpret_cast<float2*>(u + NR * W);  // rows of the next kernel, loaded during this one
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += 256) twM[i] = twM_g[i];
     for (int i = tid; i < Wc; i += 256) twW[i] = twW_g[i];
     for (int i = tid; i < NR * W; i += 256) u[i] = 0.f;
-    for (int k = 0; k < K; ++k) {
-        const KDesc d = kd[k];
-        if (d.tgt != c) continue;
+    auto next = [&](int k) {
+        for (++k; k < K; ++k)
+            if (kd[k].tgt == c) break;
+        return k;
+    };
+    auto prefetch = [&](int k) {
         const float2* t = T + size_t(k) * Wc * H;
-        __syncthreads();
 #pragma unroll 4
         for (int i = tid; i < NR * Wc; i += 256) {
             const int r = i % NR, kk = i / NR;
             const int y = y0 + r;
-            a[r * LS + kk] = y < H ? t[size_t(kk) * H + y] : make_float2(0.f, 0.f);
+            if (y < H) cp_async8(pre + r * LS + kk, t + size_t(kk) * H + y);
+            else pre[r * LS + kk] = make_float2(0.f, 0.f);
         }
+        cp_async_commit();
+    };
+    int kn = next(-1);
+    if (kn < K) prefetch(kn);
+    while (kn < K) {
+        const KDesc d = kd[kn];
+        cp_async_wait_all_groups();
         __syncthreads();
         // Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) e^{+2 pi i k / W}
 #pragma unroll 4
         for (int i = tid; i < NR * M; i += 256) {
             const int r = i / M, kk = i - r * M;
-            const float2 xk = a[r * LS + kk];
-            const float2 xm = cconj(a[r * LS + M - kk]);
+            const float2 xk = pre[r * LS + kk];
+            const float2 xm = cconj(pre[r * LS + M - kk]);
             const float2 e = cadd(xk, xm);
             const float2 o = cmul(csub(xk, xm), cconj(twW[kk]));
             b[r * LS + pad8(kk)] = make_float2(e.x - o.y, e.y + o.x);
         }
         __syncthreads();
+        kn = next(kn);
+        if (kn < K) prefetch(kn);  // overlaps the transform below
         const float2* z = ct_fft<M, NR, true>(b, a, twM);
 #pragma unroll 4
         for (int i = tid; i < NR * W; i += 256) {

@@ -65,12 +65,20 @@ __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, cons
     else if (tid < F3_RW + F3_RH) rowy[tid - F3_RW] = wrap_near(y0 - 1 + (tid - F3_RW), H);
     else if (tid < F3_RW + F3_RH + 3) plz[tid - F3_RW - F3_RH] = wrap_near(z - 1 + (tid - F3_RW - F3_RH), D);
     __syncthreads();
-    for (int i = tid; i < 2 * C * F3_RC; i += 256) {
-        const int k = i / F3_RC, cell = i - k * F3_RC;
-        const int pz = cell / F3_PL, r = cell - pz * F3_PL;
-        const int ly = r / F3_RW, lx = r - ly * F3_RW;
-        const size_t idx = (size_t(plz[pz]) * H + rowy[ly]) * W + colx[lx];
-        cp_async4(sm + i, (k < C ? A + size_t(k) * N : U + size_t(k - C) * N) + idx);
+    // one staged row (field k, plane pz, row ly) per warp and pass, lanes over
+    // its 34 columns: no index division per element
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+        const int x_a = colx[lane], x_b = lane < F3_RW - 32 ? colx[32 + lane] : 0;
+        for (int row = warp; row < 2 * C * 3 * F3_RH; row += 8) {
+            const int k = row / (3 * F3_RH), q = row - k * (3 * F3_RH);
+            const int pz = q / F3_RH, ly = q - pz * F3_RH;
+            const float* src = (k < C ? A + size_t(k) * N : U + size_t(k - C) * N) +
+                               (size_t(plz[pz]) * H + rowy[ly]) * W;
+            float* dst = sm + k * F3_RC + pz * F3_PL + ly * F3_RW;
+            cp_async4(dst + lane, src + x_a);
+            if (lane < F3_RW - 32) cp_async4(dst + 32 + lane, src + x_b);
+        }
     }
     cp_async_wait_all();
     __syncthreads();
