@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
         const int slot = p.slots[w.offKd + k];
         const int kx0 = g * ColCfg<H>::NC;
         const int nl = min(ColCfg<H>::NC, Wc - kx0);
-        cols_conv_item<H>(fsm, p.S + w.offS + (size_t(slot) * Wc + kx0) * H, p.KH + w.offT + (size_t(k) * Wc + kx0) * H,
+        cols_conv_item<H, true>(fsm, p.S + w.offS + (size_t(slot) * Wc + kx0) * H, p.KH + w.offT + (size_t(k) * Wc + kx0) * H,
                           p.T + w.offT + (size_t(k) * Wc + kx0) * H, nl, 0, 1.f, p.tw + w.twH);
     }
 }
@@ -313,7 +313,7 @@ size_t c2r_smem(int cls) {
 }
 size_t cols_smem(int cls) {
     switch (COL_SIZES[cls]) {
-#define X(n) case n: return ColCfg<n>::smem;
+#define X(n) case n: return ColCfg<n>::smem_prefetch;
         FLP_COL_SIZES(X)
 #undef X
     }

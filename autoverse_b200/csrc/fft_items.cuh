@@ -199,6 +199,8 @@ struct ColCfg {
     static constexpr int LS = CtPlan<H>::LS;
     static constexpr size_t buf = size_t(NC) * LS;
     static constexpr size_t smem = sizeof(float2) * (H + 2 * buf);
+    // with the kernel spectrum prefetched during the forward FFT (batched engine)
+    static constexpr size_t smem_prefetch = smem + sizeof(float2) * size_t(NC) * H;
 };
 
 // ---- items: one CTA's share of a pass, shared by the plain and batched launches
@@ -248,7 +250,10 @@ __device__ void r2c_rows_item(float2* sm, const float* __restrict__ x, float2* _
 // nl (<= NC) contiguous columns of length H: forward FFT, then either scale
 // (mode 1) or multiply by the kernel spectrum and inverse FFT (mode 0); mode 2
 // is the inverse FFT alone.
-template <int H>
+// PREFETCH copies the kernel spectrum in with cp.async while the forward FFT
+// runs: a gain when many CTAs share the SMs (batched engine), a loss for a
+// single world under one wave, where the copies delay the column loads.
+template <int H, bool PREFETCH = false>
 __device__ void cols_conv_item(float2* sm, const float2* __restrict__ src, const float2* __restrict__ kh,
                                float2* __restrict__ dst, int nl, int mode, float scale,
                                const float2* __restrict__ twH_g) {
@@ -256,8 +261,13 @@ __device__ void cols_conv_item(float2* sm, const float2* __restrict__ src, const
     float2* twH = sm;
     float2* a = twH + H;
     float2* b = a + ColCfg<H>::buf;
+    float2* khs = b + ColCfg<H>::buf;  // PREFETCH, mode 0: the kernel spectrum
     const int tid = threadIdx.x;
     for (int i = tid; i < H; i += 256) twH[i] = twH_g[i];
+    if (PREFETCH && mode == 0) {
+        for (int i = tid; i < nl * H; i += 256) cp_async8(khs + i, kh + i);
+        cp_async_commit();
+    }
 #pragma unroll 4
     for (int i = tid; i < NC * H; i += 256) {
         const int l = i / H, y = i - l * H;
@@ -285,11 +295,12 @@ __device__ void cols_conv_item(float2* sm, const float2* __restrict__ src, const
         __syncthreads();
         return;
     }
+    if (PREFETCH) cp_async_wait_all_groups();  // each thread multiplies the values it copied
 #pragma unroll 4
     for (int i = tid; i < NC * H; i += 256) {
         const int l = i / H, y = i - l * H;
         float2& f = F[l * LS + pad8(y)];
-        f = l < nl ? cmul(f, kh[i]) : make_float2(0.f, 0.f);
+        f = l < nl ? cmul(f, PREFETCH ? khs[i] : kh[i]) : make_float2(0.f, 0.f);
     }
     __syncthreads();
     float2* R = ct_fft<H, NC, true>(F, G, twH);
