@@ -21,6 +21,7 @@ the reference's f32 host sums to rounding.
 from __future__ import annotations
 
 import math
+import time
 from typing import Any, Sequence
 
 import numpy as np
@@ -128,10 +129,13 @@ def _concentration(final: np.ndarray) -> float:
 
 
 def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: dict | None = None,
-                        evaluation: dict | None = None) -> list[dict]:
+                        evaluation: dict | None = None, timings: dict | None = None) -> list[dict]:
     """FitnessEvaluator::evaluate for every (config, seed) pair at once.
     Returns per candidate {"fitness", "scores": [(type, score, weight)],
-    "behavior": {...}} in the reference's shapes."""
+    "behavior": {...}} in the reference's shapes.  `timings`, when given,
+    receives the wall-clock seconds of the set-up (batch creation and seeds),
+    the simulation with its sampling, and the metric evaluation."""
+    t_start = time.perf_counter()
     fitness = fitness or DEFAULT_FITNESS
     evaluation = {**DEFAULT_EVALUATION, **(evaluation or {})}
     metrics = fitness.get("metrics", [])
@@ -148,6 +152,7 @@ def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: d
         if snaps:
             b.reserve_snapshots(1 + len(sample_steps))
             b.snapshot(0)  # the initial state's channel sum
+        t_setup = time.perf_counter()
         init = b.stats()
         traj = [_Trajectory(c["width"], c["height"], init[i]) for i, c in enumerate(b.configs)]
         if warm:
@@ -165,6 +170,7 @@ def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: d
         if done < steps:
             b.run(steps - done)
         final = b.stats()
+        t_run = time.perf_counter()
         sim = {}
 
         def similarity(sa: int, sb: int) -> np.ndarray:
@@ -220,4 +226,7 @@ def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: d
             tw = sum(w for _, _, w in scores)
             f = sum(v * w for v, (_, _, w) in zip(vals, scores)) / max(tw, 1e-6)
             results.append({"fitness": float(f), "scores": scores, "behavior": t.behavior()})
+        if timings is not None:
+            t_end = time.perf_counter()
+            timings.update(setup_s=t_setup - t_start, simulate_s=t_run - t_setup, metrics_s=t_end - t_run)
         return results

@@ -342,13 +342,14 @@ def measure_fitness(args, dist):
     cfgs, seeds = [c for c, _ in pop], [s for _, s in pop]
     FT.evaluate_population(cfgs[:8], seeds[:8], evaluation={"steps": 10})  # warm-up
     t0 = time.perf_counter()
-    res = FT.evaluate_population(cfgs, seeds)
+    tm = {}
+    res = FT.evaluate_population(cfgs, seeds, timings=tm)
     t = reduce_max(dist, time.perf_counter() - t0)
     cells = sum(c["width"] * c["height"] for c in cfgs)
     out = {"workload": f"{args.fitness_candidates} candidates per GPU, sides {{64,96,128}}, 200 steps, sample every 10, "
                        "metrics Persistence 1.0 + Compactness 0.5",
            "candidates_per_s": WORLD * len(cfgs) / t, "cell_steps_per_s": WORLD * cells * 200 / t, "seconds": t,
-           "mean_fitness": float(np.mean([r["fitness"] for r in res]))}
+           "mean_fitness": float(np.mean([r["fitness"] for r in res])), "seconds_split": tm}
     if RANK == 0 and not args.skip_cpu:
         from oracle import fitness_ref as FR
         t0 = time.perf_counter()
