@@ -48,8 +48,8 @@ __global__ void __launch_bounds__(256, 3) k_gather_worlds(const float* __restric
     const int p = blockIdx.z, w = p / C;
     const size_t off = size_t(p) * W * H;
     const FlowParams fp = fps[w];
-    gather_item<POW2>(sm, DX + off, DY + off, MS + off, An + off, W, H, fp, dmax[w], blockIdx.x * GT_W,
-                      blockIdx.y * GT_H);
+    gather_item<POW2, 1>(sm, DX + off, DY + off, MS + off, An + off, W, H, fp, dmax[w], blockIdx.x * GT_W,
+                      blockIdx.y * gt_h(1));
 }
 
 void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, float* MS, int B, int C, int W, int H,
@@ -70,7 +70,7 @@ void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, fl
 
 void launch_gather_worlds(const float* DX, const float* DY, const float* MS, float* An, int B, int C, int W, int H,
                           const FlowParams* fps, bool pow2, const int* dmax, cudaStream_t st) {
-    dim3 grid((W + GT_W - 1) / GT_W, (H + GT_H - 1) / GT_H, B * C);
+    dim3 grid((W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), B * C);
     if (pow2)
         k_gather_worlds<true><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, An, C, W, H, fps, dmax);
     else

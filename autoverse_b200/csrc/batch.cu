@@ -35,6 +35,7 @@ extern thread_local std::string g_last_error;
 namespace {
 
 constexpr int BATCH_ROW_ELEMS = 2048;  // complex values per CTA in the batched row passes
+constexpr int BATCH_GBY = 2;           // destination rows per thread in the batched gather (64x32 tiles)
 constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
 constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
 constexpr int NSTAGE = 5;
@@ -124,12 +125,14 @@ __device__ __forceinline__ int next_item(int* counter, int n) {
 
 // Zero every queue counter and every world's displacement slot.
 __global__ void k_batch_reset(Pools p) {
+    dep_enter();
     for (int i = threadIdx.x; i < NQUEUE; i += blockDim.x) p.counters[i] = 0;
     for (int i = threadIdx.x; i < p.n_worlds; i += blockDim.x) p.dmax[i] = 0;
 }
 
 template <int M>
 __global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
     for (;;) {
@@ -147,6 +150,7 @@ __global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
 
 template <int H>
 __global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
     for (;;) {
@@ -166,6 +170,7 @@ __global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
 
 template <int M>
 __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
     for (;;) {
@@ -182,6 +187,7 @@ __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
 
 template <int CV>
 __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
+    dep_enter();
     extern __shared__ __align__(16) float sm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
     for (;;) {
@@ -205,6 +211,7 @@ __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
 }
 
 __global__ void __launch_bounds__(256, 3) k_batch_gather(Pools p) {
+    dep_enter();
     extern __shared__ __align__(16) float sm[];
     constexpr int q = QG;
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -215,13 +222,13 @@ __global__ void __launch_bounds__(256, 3) k_batch_gather(Pools p) {
         const BWorld w = p.worlds[item.x];
         const int c = item.y >> 16, t = item.y & 0xFFFF;
         const int tiles_x = (w.W + GT_W - 1) / GT_W;
-        const int x0 = (t % tiles_x) * GT_W, y0 = (t / tiles_x) * GT_H;
+        const int x0 = (t % tiles_x) * GT_W, y0 = (t / tiles_x) * gt_h(BATCH_GBY);
         const size_t off = size_t(w.offA) + size_t(c) * w.W * w.H;
         const int bits = p.dmax[item.x];
         if (w.fp.area_pow2)
-            gather_item<true>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
+            gather_item<true, BATCH_GBY>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
         else
-            gather_item<false>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
+            gather_item<false, BATCH_GBY>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
     }
 }
 
@@ -501,16 +508,25 @@ struct flp_batch {
         return p;
     }
 
+    // Queue kernels are launched with programmatic stream serialization (they
+    // begin with dep_enter), so each one's blocks are placed while its
+    // predecessor drains.
     void launch_queue(int q, Pools& p) {
         if (!n_q[q]) return;
-        if (q < QG) {
-            int qq = q;
-            void* args[] = {&p, &qq};
-            ckb(cudaLaunchKernel(q_fn[q], dim3(q_grid[q]), dim3(256), args, q_smem[q], st), "batch launch");
-        } else {
-            void* args[] = {&p};
-            ckb(cudaLaunchKernel(q_fn[q], dim3(q_grid[q]), dim3(256), args, q_smem[q], st), "batch launch");
-        }
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(q_grid[q]);
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = q_smem[q];
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int qq = q;
+        void* args2[] = {&p, &qq};
+        void* args1[] = {&p};
+        ckb(cudaLaunchKernelExC(&cfg, q_fn[q], q < QG ? args2 : args1), "batch launch");
     }
 
     // reset, then per stage the size-class kernels of that stage
@@ -519,7 +535,7 @@ struct flp_batch {
     void enqueue_step(cudaEvent_t* evs = nullptr, bool staged = false) {
         Pools p = pools();
         if (evs) ckb(cudaEventRecord(evs[0], st), "event");
-        k_batch_reset<<<1, 256, 0, st>>>(p);
+        launch_dep(k_batch_reset, 1, 256, 0, st, p);
         for (int stage = 0; stage < 3; ++stage) {
             for (int cls = 0; cls < NCLS; ++cls) launch_queue(stage * NCLS + cls, p);
             if (evs && staged) ckb(cudaEventRecord(evs[stage + 1], st), "event");
@@ -570,7 +586,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
             set(cols_fn(c), cols_smem(c));
         }
         set((const void*)k_batch_flow<0>, flow_smem_bytes_inl(64));
-        set((const void*)k_batch_gather, gather_smem_bytes_inl());
+        set((const void*)k_batch_gather, gather_smem_bytes_inl(BATCH_GBY));
         transport_2d_set_attributes();
         fft2d_set_attributes(200 * 1024);
     });
@@ -735,7 +751,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         const int fth = d.C <= 4 ? FR_H : FL_H;
         const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + fth - 1) / fth);
         for (int t = 0; t < ftiles; ++t) items[flow_queue(d.C)].push_back(make_int2(w, t));
-        const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + GT_H - 1) / GT_H);
+        const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + gt_h(BATCH_GBY) - 1) / gt_h(BATCH_GBY));
         for (int c = 0; c < d.C; ++c)
             for (int t = 0; t < gtiles; ++t) items[QG].push_back(make_int2(w, (c << 16) | t));
     }
@@ -770,7 +786,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
                 b->q_smem[q] = q == QF ? flow_smem_bytes_inl(cmax) : 0;
                 break;
             }
-            default: b->q_fn[q] = (const void*)k_batch_gather; b->q_smem[q] = gather_smem_bytes_inl(); break;
+            default: b->q_fn[q] = (const void*)k_batch_gather; b->q_smem[q] = gather_smem_bytes_inl(BATCH_GBY); break;
         }
         if (!b->n_q[q]) continue;
         int per_sm = 0;

@@ -37,6 +37,40 @@ struct FlowParams {
     int point_mode;     // total_area < 1e-10: nearest-cell deposit
 };
 
+// Programmatic dependent launch.  The step's kernels are launched with
+// programmatic stream serialization (launch_dep below), so a kernel's blocks
+// may be placed on the SMs while its predecessor in the stream is finishing.
+// Every such kernel first signals that its own successor may be placed
+// (dep_launch: takes effect once all of this grid's blocks have signalled,
+// i.e. are resident, so the successor never takes a slot this grid needs),
+// then waits for the predecessor to complete with its writes visible
+// (dep_wait) before it touches any global memory.  Launched without the
+// attribute, both are no-ops.
+__device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void dep_enter() {
+    dep_launch();
+    dep_wait();
+}
+
+// Launch with programmatic stream serialization; the kernel must begin with
+// dep_enter().  Errors surface through cudaGetLastError like a <<<>>> launch.
+template <typename... KArgs, typename... Args>
+inline void launch_dep(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Float <-> order-preserving int, for atomicMax/atomicMin on floats.
 __host__ __device__ inline int float_to_ordered(float f) {
 #ifdef __CUDA_ARCH__

@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(256) fft_rows_r2c(const float* __restrict__ A,
                                                     const int* __restrict__ srcs, int W, int H, int NR, FftPlan pm,
                                                     const float2* __restrict__ twM_g, const float2* __restrict__ twW_g,
                                                     int* reset_slot, int nreset) {
+    dep_enter();
     extern __shared__ float2 fsm[];
     const int M = W / 2, Wc = M + 1;
     float2* twM = fsm;
@@ -181,6 +182,7 @@ __global__ void __launch_bounds__(256) fft_cols_conv(const float2* __restrict__ 
                                                      float2* __restrict__ T, const int* __restrict__ slot_of_kernel,
                                                      int Wc, int H, int NC, FftPlan ph,
                                                      const float2* __restrict__ twH_g, int mode, float scale) {
+    dep_enter();
     extern __shared__ float2 fsm[];
     float2* twH = fsm;
     float2* a = twH + H;
@@ -215,6 +217,7 @@ __global__ void __launch_bounds__(256) fft_rows_c2r_growth(const float2* __restr
                                                            const KDesc* __restrict__ kd, int K, int W, int H, int NR,
                                                            FftPlan pm, const float2* __restrict__ twM_g,
                                                            const float2* __restrict__ twW_g) {
+    dep_enter();
     extern __shared__ float2 fsm[];
     const int M = W / 2, Wc = M + 1;
     float2* twM = fsm;
@@ -275,6 +278,7 @@ template <int M>
 __global__ void __launch_bounds__(256) k_r2c_t(const float* __restrict__ A, float2* __restrict__ S,
                                                const int* __restrict__ srcs, int H, const float2* __restrict__ twM,
                                                const float2* __restrict__ twW, int* reset_slot, int nreset) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
         for (int i = 0; i < nreset; ++i) reset_slot[i] = 0;
@@ -288,6 +292,7 @@ template <int H>
 __global__ void __launch_bounds__(256) k_cols_t(const float2* __restrict__ S, const float2* __restrict__ KH,
                                                 float2* __restrict__ T, const int* __restrict__ slot_of_kernel, int Wc,
                                                 int mode, float scale, const float2* __restrict__ twH) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     constexpr int NC = ColCfg<H>::NC;
     const int kx0 = blockIdx.x * NC, k = blockIdx.y;
@@ -301,6 +306,7 @@ template <int M>
 __global__ void __launch_bounds__(256) k_c2r_t(const float2* __restrict__ T, float* __restrict__ U,
                                                const KDesc* __restrict__ kd, int K, int H,
                                                const float2* __restrict__ twM, const float2* __restrict__ twW) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int c = blockIdx.y;
     constexpr int W = 2 * M;
@@ -311,6 +317,7 @@ template <int M>
 __global__ void __launch_bounds__(256) k_c2r_raw_t(const float2* __restrict__ T, float* __restrict__ out,
                                                    const int* __restrict__ planes, int H, float scale, int accumulate,
                                                    const float2* __restrict__ twM, const float2* __restrict__ twW) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int slot = blockIdx.y;
     const int plane = planes ? planes[slot] : slot;
@@ -363,14 +370,14 @@ void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W,
 #define X(n)                                                                                        \
     if (M == n) {                                                                                   \
         dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, nsrc);                                   \
-        k_r2c_t<n><<<grid, 256, RowCfg<n>::smem_r2c, st>>>(A, S, srcs, H, g.twM, g.twW, reset_slot, \
+        launch_dep(k_r2c_t<n>, grid, 256, RowCfg<n>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW, reset_slot, \
                                                             nreset);                                \
         return;                                                                                     \
     }
     FLP_ROW_SIZES(X)
 #undef X
     dim3 grid((H + g.NR - 1) / g.NR, nsrc);
-    fft_rows_r2c<<<grid, 256, fft_rows_smem(W, g.NR, false), st>>>(A, S, srcs, W, H, g.NR, g.pm, g.twM, g.twW,
+    launch_dep(fft_rows_r2c, grid, 256, fft_rows_smem(W, g.NR, false), st, A, S, srcs, W, H, g.NR, g.pm, g.twM, g.twW,
                                                                     reset_slot, nreset);
 }
 
@@ -379,13 +386,13 @@ void launch_fft_lines(const float2* S, const float2* KH, float2* T, const int* s
 #define X(n)                                                                                                   \
     if (H == n) {                                                                                              \
         dim3 grid((nlines + ColCfg<n>::NC - 1) / ColCfg<n>::NC, K);                                            \
-        k_cols_t<n><<<grid, 256, ColCfg<n>::smem, st>>>(S, KH, T, slot_of_kernel, nlines, mode, scale, g.twH); \
+        launch_dep(k_cols_t<n>, grid, 256, ColCfg<n>::smem, st, S, KH, T, slot_of_kernel, nlines, mode, scale, g.twH); \
         return;                                                                                                \
     }
     FLP_COL_SIZES(X)
 #undef X
     dim3 grid((nlines + g.NC - 1) / g.NC, K);
-    fft_cols_conv<<<grid, 256, fft_cols_smem(H, g.NC), st>>>(S, KH, T, slot_of_kernel, nlines, H, g.NC, g.ph, g.twH,
+    launch_dep(fft_cols_conv, grid, 256, fft_cols_smem(H, g.NC), st, S, KH, T, slot_of_kernel, nlines, H, g.NC, g.ph, g.twH,
                                                               mode, scale);
 }
 
@@ -400,13 +407,13 @@ void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, in
 #define X(n)                                                                                     \
     if (M == n) {                                                                                \
         dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, C);                                   \
-        k_c2r_t<n><<<grid, 256, RowCfg<n>::smem_c2r, st>>>(T, U, kd, K, H, g.twM, g.twW);       \
+        launch_dep(k_c2r_t<n>, grid, 256, RowCfg<n>::smem_c2r, st, T, U, kd, K, H, g.twM, g.twW);       \
         return;                                                                                  \
     }
     FLP_ROW_SIZES(X)
 #undef X
     dim3 grid((H + g.NR - 1) / g.NR, C);
-    fft_rows_c2r_growth<<<grid, 256, fft_rows_smem(W, g.NR, true), st>>>(T, U, kd, K, W, H, g.NR, g.pm, g.twM,
+    launch_dep(fft_rows_c2r_growth, grid, 256, fft_rows_smem(W, g.NR, true), st, T, U, kd, K, W, H, g.NR, g.pm, g.twM,
                                                                           g.twW);
 }
 
@@ -416,7 +423,7 @@ void launch_fft_c2r_raw(const float2* T, float* out, const int* planes, int nslo
 #define X(n)                                                                                                  \
     if (M == n) {                                                                                             \
         dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, nslots);                                           \
-        k_c2r_raw_t<n><<<grid, 256, RowCfg<n>::smem_r2c, st>>>(T, out, planes, H, scale, accumulate ? 1 : 0, \
+        launch_dep(k_c2r_raw_t<n>, grid, 256, RowCfg<n>::smem_r2c, st, T, out, planes, H, scale, accumulate ? 1 : 0, \
                                                                 g.twM, g.twW);                                \
         return;                                                                                               \
     }

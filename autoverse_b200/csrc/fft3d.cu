@@ -20,6 +20,7 @@ __global__ void __launch_bounds__(256) k_zconv_t(const float2* __restrict__ S, c
                                                  float2* __restrict__ T, const int* __restrict__ slot_of_kernel,
                                                  int Wc, int H, int mode, float scale,
                                                  const float2* __restrict__ twD) {
+    dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     constexpr int NZ = ZCfg<D>::NZ;
     const int groups = (H + NZ - 1) / NZ;
@@ -54,7 +55,7 @@ void launch_fft_z(const float2* S, const float2* KH, float2* T, const int* slot_
 #define X(n)                                                                                                  \
     if (D == n) {                                                                                             \
         const int groups = (H + ZCfg<n>::NZ - 1) / ZCfg<n>::NZ;                                               \
-        k_zconv_t<n><<<dim3(Wc * groups, nlines_k), 256, ZCfg<n>::smem, st>>>(S, KH, T, slot_of_kernel, Wc, H, mode, \
+        launch_dep(k_zconv_t<n>, dim3(Wc * groups, nlines_k), 256, ZCfg<n>::smem, st, S, KH, T, slot_of_kernel, Wc, H, mode, \
                                                                              scale, twD);                     \
         return;                                                                                               \
     }

@@ -34,6 +34,7 @@ __global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __rest
                                                              const KDesc* __restrict__ kd, int K,
                                                              const float* __restrict__ taps, int W, int H, int rmax,
                                                              int* reset_slot, int nreset) {
+    dep_enter();
     extern __shared__ float sm[];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * 32 + tx;
@@ -101,17 +102,18 @@ void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, con
                            int rmax, int* reset_slot, cudaStream_t st) {
     dim3 grid((W + CD_TW - 1) / CD_TW, (H + CD_TH - 1) / CD_TH, C);
     size_t smem = conv_direct_smem_bytes(rmax);
-    conv_direct_growth_2d<<<grid, dim3(32, 8), smem, st>>>(A, U, kd, K, taps, W, H, rmax, reset_slot, 1);
+    launch_dep(conv_direct_growth_2d, grid, dim3(32, 8), smem, st, A, U, kd, K, taps, W, H, rmax, reset_slot, 1);
 }
 
 size_t flow_smem_bytes(int C) { return flow_smem_bytes_inl(C); }
-size_t gather_smem_bytes() { return gather_smem_bytes_inl(); }
+size_t gather_smem_bytes() { return gather_smem_bytes_inl(1); }
 
 template <bool POW2>
 __global__ void __launch_bounds__(256) flow_2d(const float* __restrict__ A, const float* __restrict__ U,
                                                float* __restrict__ DX, float* __restrict__ DY,
                                                float* __restrict__ MS, int C, int W, int H, FlowParams fp,
                                                int* dmax_slot, int* status) {
+    dep_enter();
     extern __shared__ __align__(16) float sm[];
     flow_item<POW2>(sm, A, U, DX, DY, MS, C, W, H, fp, blockIdx.x * FL_W, blockIdx.y * FL_H, dmax_slot, status);
 }
@@ -120,11 +122,12 @@ template <bool POW2>
 __global__ void __launch_bounds__(256, 3) gather_2d(const float* __restrict__ DX, const float* __restrict__ DY,
                                                     const float* __restrict__ MS, float* __restrict__ Anext, int W,
                                                     int H, FlowParams fp, const int* __restrict__ dmax_slot) {
+    dep_enter();
     extern __shared__ __align__(16) float sm[];
     const int c = blockIdx.z;
     const size_t N = size_t(W) * H;
-    gather_item<POW2>(sm, DX + size_t(c) * N, DY + size_t(c) * N, MS + size_t(c) * N, Anext + size_t(c) * N, W, H,
-                      fp, *dmax_slot, blockIdx.x * GT_W, blockIdx.y * GT_H);
+    gather_item<POW2, 1>(sm, DX + size_t(c) * N, DY + size_t(c) * N, MS + size_t(c) * N, Anext + size_t(c) * N, W, H,
+                      fp, *dmax_slot, blockIdx.x * GT_W, blockIdx.y * gt_h(1));
 }
 
 template <int C, bool POW2>
@@ -132,6 +135,7 @@ __global__ void __launch_bounds__(256) flow_rows_2d(const float* __restrict__ A,
                                                     float* __restrict__ DX, float* __restrict__ DY,
                                                     float* __restrict__ MS, int W, int H, FlowParams fp,
                                                     int* dmax_slot, int* status) {
+    dep_enter();
     flow_rows_item<C, POW2>(A, U, DX, DY, MS, W, H, fp, blockIdx.x * 32, blockIdx.y * FR_H, dmax_slot, status);
 }
 
@@ -143,8 +147,8 @@ void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float*
         const dim3 g((W + 31) / 32, (H + FR_H - 1) / FR_H);
 #define FR_CASE(c)                                                                                                 \
         if (C == c) {                                                                                              \
-            if (fp.area_pow2) flow_rows_2d<c, true><<<g, 256, 0, st>>>(A, U, DX, DY, MS, W, H, fp, dmax_slot, status);   \
-            else flow_rows_2d<c, false><<<g, 256, 0, st>>>(A, U, DX, DY, MS, W, H, fp, dmax_slot, status);              \
+            if (fp.area_pow2) launch_dep(flow_rows_2d<c, true>, g, 256, 0, st, A, U, DX, DY, MS, W, H, fp, dmax_slot, status);   \
+            else launch_dep(flow_rows_2d<c, false>, g, 256, 0, st, A, U, DX, DY, MS, W, H, fp, dmax_slot, status);              \
             return;                                                                                                \
         }
         FR_CASE(1) FR_CASE(2) FR_CASE(3) FR_CASE(4)
@@ -152,18 +156,18 @@ void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float*
     }
     dim3 grid((W + FL_W - 1) / FL_W, (H + FL_H - 1) / FL_H);
     if (fp.area_pow2)
-        flow_2d<true><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
+        launch_dep(flow_2d<true>, grid, 256, flow_smem_bytes(C), st, A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
     else
-        flow_2d<false><<<grid, 256, flow_smem_bytes(C), st>>>(A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
+        launch_dep(flow_2d<false>, grid, 256, flow_smem_bytes(C), st, A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
 }
 
 void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
                       const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
-    dim3 grid((W + GT_W - 1) / GT_W, (H + GT_H - 1) / GT_H, C);
+    dim3 grid((W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), C);
     if (fp.area_pow2)
-        gather_2d<true><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, Anext, W, H, fp, dmax_slot);
+        launch_dep(gather_2d<true>, grid, 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, fp, dmax_slot);
     else
-        gather_2d<false><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, Anext, W, H, fp, dmax_slot);
+        launch_dep(gather_2d<false>, grid, 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, fp, dmax_slot);
 }
 
 void transport_2d_set_attributes() {

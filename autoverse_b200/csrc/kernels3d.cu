@@ -53,6 +53,7 @@ __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, cons
                                                float* __restrict__ DX, float* __restrict__ DY,
                                                float* __restrict__ DZ, float* __restrict__ MS, int C, int W, int H,
                                                int D, FlowParams fp, int* dmax_slot, int* status) {
+    dep_enter();
     extern __shared__ __align__(16) float sm[];
     float* as = sm;                    // C staged A blocks (3 planes each)
     float* us = sm + C * F3_RC;        // C staged U blocks
@@ -364,6 +365,7 @@ __global__ void __launch_bounds__(256) gather_3d(const float* __restrict__ DX, c
                                                  const float* __restrict__ DZ, const float* __restrict__ MS,
                                                  float* __restrict__ Anext, int C, int W, int H, int D, FlowParams fp,
                                                  const int* __restrict__ dmax_slot) {
+    dep_enter();
     extern __shared__ __align__(16) float sm[];
     const int nchunk = (D + G3_NZ - 1) / G3_NZ;
     const int c = blockIdx.z / nchunk;
@@ -400,18 +402,18 @@ void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float*
                     int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
     dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, D);
     if (fp.area_pow2)
-        flow_3d<true><<<grid, 256, flow3d_smem_bytes(C), st>>>(A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+        launch_dep(flow_3d<true>, grid, 256, flow3d_smem_bytes(C), st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
     else
-        flow_3d<false><<<grid, 256, flow3d_smem_bytes(C), st>>>(A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+        launch_dep(flow_3d<false>, grid, 256, flow3d_smem_bytes(C), st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
 }
 
 void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
                       int H, int D, const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
     dim3 grid((W + G3_W - 1) / G3_W, (H + G3_H - 1) / G3_H, C * ((D + G3_NZ - 1) / G3_NZ));
     if (fp.area_pow2)
-        gather_3d<true><<<grid, 256, gather3d_smem_bytes(), st>>>(DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
+        launch_dep(gather_3d<true>, grid, 256, gather3d_smem_bytes(), st, DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
     else
-        gather_3d<false><<<grid, 256, gather3d_smem_bytes(), st>>>(DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
+        launch_dep(gather_3d<false>, grid, 256, gather3d_smem_bytes(), st, DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
 }
 
 void transport_3d_set_attributes() {

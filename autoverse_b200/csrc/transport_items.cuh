@@ -6,6 +6,9 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <type_traits>
+
+
 namespace flp {
 
 // ---------------------------------------------------------------------------
@@ -17,7 +20,8 @@ namespace flp {
 // planes per channel; it also publishes the largest |dest - x| of any cell
 // with mass.
 //
-// gather_2d (one block per 64x16 tile and channel): with D the largest
+// gather_2d (one block per 64x16 or 64x32 tile and channel, 4x1 or 4x2
+// destinations per thread): with D the largest
 // displacement, a source at x overlaps cell ix only if x - ix lies in
 // (-(D+s), D+s+1) (reintegration.rs:105-146), so sources x = ix + k with
 // k in [-RN, RN+1], RN = ceil(D+s) - 1, cover every deposit.  Each
@@ -278,16 +282,23 @@ __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, cons
 }
 
 // ----------------------------------------------------------- gather_2d ----
-constexpr int GT_W = 64, GT_H = 16, TP = 4, RN_MAX = 3;
+// A tile is 64 x (16 * GBY) destinations; each of its 256 threads sums a
+// block of 4 x GBY destinations, so a source's x overlaps serve GBY rows and
+// its y overlaps serve 4 columns.  The single-world kernel uses GBY = 1 (its
+// one wave of tiles then overlaps staging and compute across co-resident
+// blocks); the batched engine, whose persistent blocks pull tiles from a
+// queue, uses GBY = 2.
+constexpr int GT_W = 64, TP = 4, RN_MAX = 3;
+__host__ __device__ constexpr int gt_h(int gby) { return 16 * gby; }
 // Staged source columns: x0 - TP .. x0 + GT_W + TP - 1 plus 4 unused ones, so
-// that a row is 76 floats: with the column-major thread mapping of the gather
-// (a warp is 2 x 16 threads, 16 rows apart) the rows of a quarter-warp then
-// start in distinct bank groups.
+// that a row is 76 floats: with the column-major thread mappings of the
+// gather (gather_thread) the rows of a quarter-warp then start in distinct
+// bank groups.
 constexpr int SR_W = GT_W + 2 * TP + 4;
-constexpr int SR_HMAX = GT_H + 2 * RN_MAX + 1;  // up to 23 source rows
+__host__ __device__ constexpr int sr_hmax(int gby) { return gt_h(gby) + 2 * RN_MAX + 1; }  // up to 39 source rows
 static_assert(SR_W % 4 == 0, "source rows must stay 16-byte aligned");
 
-inline size_t gather_smem_bytes_inl() { return sizeof(float) * 5 * SR_W * SR_HMAX; }
+inline size_t gather_smem_bytes_inl(int gby) { return sizeof(float) * 5 * SR_W * sr_hmax(gby); }
 
 // Stage the dx, dy and m planes of an SR_W x SRH source region (columns
 // colx[], rows rowy[]) into shared memory.  When W and the three base
@@ -334,16 +345,22 @@ __device__ __forceinline__ bool gather_column_major(int x0, int W, int RN) {
     return x0 - RN < 0 || x0 + GT_W + RN >= W;
 }
 
-// One source row of the gather for the thread's 4 destinations X0..X0+3.
-// Source column j of the strip window is x0-TP+4tx+j; its offset from
-// destination i is kx = j - TP - i, kept in [-RN, RN+1] at compile time.
-// Sources are streamed one float4 chunk (4 columns) at a time.  CHECK adds
-// the wrap-pass predicate for tiles whose source columns wrap the torus.
-template <int RN, bool POW2, bool CHECK>
+// One source row of the gather for the thread's 4 x GBY destinations
+// (X0..X0+3, Y0..Y0+GBY-1).  Bit d of DM says whether the row is within
+// [-RN, RN+1] rows of destination row d (with GBY = 2 only the first and the
+// last source row of the thread's window miss one).  Source column j of the
+// strip window is x0-TP+4tx+j; its offset from destination column i is
+// kx = j - TP - i, kept in [-RN, RN+1] at compile time.  fy[d] = float(Y0+d)
+// in the source row's frame (shifted by H when the row wraps), fxs[i] =
+// float(X0+i).  Sources are streamed one float4 chunk (4 columns) at a time.
+// CHECK adds the wrap-pass predicate for threads whose source columns wrap the
+// torus.
+template <int RN, bool POW2, bool CHECK, int DM, int GBY>
 __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, const float* __restrict__ rxmax,
                                            const float* __restrict__ rymin, const float* __restrict__ rymax,
-                                           const float* __restrict__ rm, float cy0, float cy1, int X0, int gx_base,
-                                           int W, int cp, float total_area, float (&acc)[4]) {
+                                           const float* __restrict__ rm, const float (&fy)[GBY + 1],
+                                           const float (&fxs)[5], int X0, int gx_base, int W, int cp,
+                                           float total_area, float (&acc)[GBY][4]) {
     constexpr int JLO = TP - RN, JHI = TP + 3 + RN + 1;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -360,89 +377,147 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
         for (int jj = 0; jj < 4; ++jj) {
             const int j = 4 * q + jj;
             if (j < JLO || j > JHI) continue;
-            int xsh = 0;
+            float fx0 = 0.f;
             if (CHECK) {
                 const int gx = gx_base + j;
                 if (wrap_pass(gx, W) != cp) continue;
-                xsh = gx < 0 ? W : (gx >= W ? -W : 0);
+                fx0 = float(X0 + (gx < 0 ? W : (gx >= W ? -W : 0)));
             }
             const float m = mm[jj];
-            const float oy0 = fmaxf(cy0, ya[jj]), oy1 = fminf(cy1, yb[jj]);
-            const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
-            // POW2: a zero mass or a zero height adds a signed zero, which
-            // leaves acc (never -0: it starts at +0) unchanged, so the loop
-            // runs branch-free; the division path keeps the reference's skip.
-            if (!POW2 && (m == 0.f || !(oh > 0.f))) continue;
+            float oh[GBY];
+#pragma unroll
+            for (int d = 0; d < GBY; ++d) {
+                if (!((DM >> d) & 1)) continue;
+                const float oy0 = fmaxf(fy[d], ya[jj]), oy1 = fminf(fy[d + 1], yb[jj]);
+                oh[d] = fmaxf(__fsub_rn(oy1, oy0), 0.f);
+            }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 if (j - TP - i < -RN || j - TP - i > RN + 1) continue;
-                const int ix = X0 + i + xsh;
-                const float ox0 = fmaxf(float(ix), xa[jj]), ox1 = fminf(float(ix + 1), xb[jj]);
+                // exact: integers below 2^24
+                const float cx0 = CHECK ? fx0 + float(i) : fxs[i], cx1 = CHECK ? fx0 + float(i + 1) : fxs[i + 1];
+                const float ox0 = fmaxf(cx0, xa[jj]), ox1 = fminf(cx1, xb[jj]);
                 const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
-                const float area = __fmul_rn(ow, oh);
-                if (POW2) {
-                    // m holds mass * (1 / total_area), exact for a power-of-two
-                    // area; a zero area adds a signed zero, which leaves acc as is.
-                    acc[i] = __fadd_rn(acc[i], __fmul_rn(m, area));
-                } else if (area > 0.f) {
-                    acc[i] = __fadd_rn(acc[i], __fmul_rn(m, __fdiv_rn(area, total_area)));
+#pragma unroll
+                for (int d = 0; d < GBY; ++d) {
+                    if (!((DM >> d) & 1)) continue;
+                    const float area = __fmul_rn(ow, oh[d]);
+                    if (POW2) {
+                        // m holds mass * (1 / total_area), exact for a power-of-two
+                        // area; a zero area adds a signed zero, which leaves acc
+                        // (never -0: it starts at +0) unchanged, so this runs
+                        // branch-free.
+                        acc[d][i] = __fadd_rn(acc[d][i], __fmul_rn(m, area));
+                    } else if (m != 0.f && area > 0.f) {
+                        // the division path keeps the reference's skips
+                        acc[d][i] = __fadd_rn(acc[d][i], __fmul_rn(m, __fdiv_rn(area, total_area)));
+                    }
                 }
             }
         }
     }
 }
 
-template <int RN, bool POW2>
+// The 4 x GBY destinations of one thread.  Each destination sums its sources
+// in the reference's deposit order: row-major over wrapped source indices,
+// i.e. rows in wrap-pass order (rows past the bottom edge wrap to the top and
+// come first, rows above the top edge come last), then columns the same way.
+template <int RN, bool POW2, int GBY>
 __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sxmax, const float* symin,
                                              const float* symax, const float* smass, float* __restrict__ out, int W,
-                                             int H, const FlowParams& fp, int x0, int y0, int sw, float (&acc)[4]) {
-    // Tiles at an x edge of the torus use the column-major mapping (a warp owns
-    // 2 columns of 4 destinations x 16 rows), so only the two warps at the
-    // edge take the wrap-pass path; other tiles map a warp to 2 rows.
-    const bool cm = gather_column_major(x0, W, RN);
-    const int tx = cm ? threadIdx.x >> 4 : threadIdx.x & 15, ty = cm ? threadIdx.x & 15 : threadIdx.x >> 4;
-    const int Y = y0 + ty, X0 = x0 + 4 * tx;
-    // wrap passes of this thread's own window (sources X0-RN .. X0+4+RN, Y-RN .. Y+RN+1)
-    const int rp_lo = (Y + RN + 1 >= H) ? 0 : 1, rp_hi = (Y - RN < 0) ? 2 : 1;
+                                             int H, const FlowParams& fp, int x0, int y0, int sw, int tx, int ty) {
+    const int Y0 = y0 + GBY * ty, X0 = x0 + 4 * tx;
+    float acc[GBY][4];
+#pragma unroll
+    for (int d = 0; d < GBY; ++d)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[d][i] = 0.f;
+    // wrap passes of this thread's window (sources X0-RN .. X0+4+RN, Y0-RN .. Y0+GBY+RN)
+    const int rp_lo = (Y0 + GBY + RN >= H) ? 0 : 1, rp_hi = (Y0 - RN < 0) ? 2 : 1;
     const int cp_lo = (X0 + 4 + RN >= W) ? 0 : 1, cp_hi = (X0 - RN < 0) ? 2 : 1;
     const bool xin = cp_lo == 1 && cp_hi == 1;
     const int gx_base = x0 - TP + 4 * tx;
+    float fxs[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) fxs[i] = float(X0 + i);
+    constexpr int NSY = GBY + 2 * RN + 1;  // source rows of the thread's window
+    // source row r (global row Y0 - RN + r) in pass rp, for the destination rows DM
+    auto row = [&](auto dm, int r, int rp) {
+        constexpr int DM = decltype(dm)::value;
+        const int gy = Y0 - RN + r;
+        if (wrap_pass(gy, H) != rp) return;
+        const int yb = Y0 + (gy < 0 ? H : (gy >= H ? -H : 0));
+        float fy[GBY + 1];
+#pragma unroll
+        for (int d = 0; d <= GBY; ++d) fy[d] = float(yb + d);
+        const int off = (GBY * ty + r) * sw + 4 * tx;
+        if (xin) {
+            gather_row<RN, POW2, false, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
+                                                 fy, fxs, X0, gx_base, W, 1, fp.total_area, acc);
+        } else {
+            for (int cp = cp_lo; cp <= cp_hi; ++cp)
+                gather_row<RN, POW2, true, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
+                                                    fy, fxs, X0, gx_base, W, cp, fp.total_area, acc);
+        }
+    };
     for (int rp = rp_lo; rp <= rp_hi; ++rp) {
+        if constexpr (GBY == 1) {
 #pragma unroll 1
-        for (int ky = -RN; ky <= RN + 1; ++ky) {
-            const int gy = Y + ky;
-            if (wrap_pass(gy, H) != rp) continue;
-            const int iy = Y + (gy < 0 ? H : (gy >= H ? -H : 0));
-            const float cy0 = float(iy), cy1 = float(iy + 1);
-            const int off = (ty + RN + ky) * sw + 4 * tx;
-            if (xin) {
-                gather_row<RN, POW2, false>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off, cy0,
-                                            cy1, X0, gx_base, W, 1, fp.total_area, acc);
-            } else {
-                for (int cp = cp_lo; cp <= cp_hi; ++cp)
-                    gather_row<RN, POW2, true>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
-                                               cy0, cy1, X0, gx_base, W, cp, fp.total_area, acc);
-            }
+            for (int r = 0; r < NSY; ++r) row(std::integral_constant<int, 1>(), r, rp);
+        } else {
+            static_assert(GBY == 2, "row masks are written out for one or two destination rows per thread");
+            // the first source row reaches destination row 0 only, the last row 1 only
+            row(std::integral_constant<int, 1>(), 0, rp);
+#pragma unroll 1
+            for (int r = 1; r < NSY - 1; ++r) row(std::integral_constant<int, 3>(), r, rp);
+            row(std::integral_constant<int, 2>(), NSY - 1, rp);
         }
     }
-    float* o = out + size_t(Y) * W;
-    if (X0 + 3 < W && (W & 3) == 0) {
-        *reinterpret_cast<float4*>(o + X0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
-    } else {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (X0 + i < W) o[X0 + i] = acc[i];
+    for (int d = 0; d < GBY; ++d) {
+        if (Y0 + d >= H) break;
+        float* o = out + size_t(Y0 + d) * W;
+        if (X0 + 3 < W && (W & 3) == 0) {
+            *reinterpret_cast<float4*>(o + X0) = make_float4(acc[d][0], acc[d][1], acc[d][2], acc[d][3]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (X0 + i < W) o[X0 + i] = acc[d][i];
+        }
     }
 }
 
-template <int RN, bool POW2>
+// Thread (tx, ty) of a gather tile.  Tiles inside the torus map a warp to
+// 16 x 2 threads.  Tiles whose sources reach across an x edge use a
+// column-major mapping (a warp is 2 x 16 threads), which puts the threads that
+// need more than one column pass into the two edge warps; its lane order
+// keeps the rows read by a quarter-warp in distinct bank groups of the
+// 76-float rows (GBY = 1: 8 consecutive thread rows of one column; GBY = 2:
+// 4 thread rows of two columns).
+template <int GBY>
+__device__ __forceinline__ void gather_thread(bool cm, int& tx, int& ty) {
+    const int tid = threadIdx.x;
+    if (!cm) {
+        tx = tid & 15;
+        ty = tid >> 4;
+    } else if (GBY == 1) {
+        tx = tid >> 4;
+        ty = tid & 15;
+    } else {
+        tx = 2 * (tid >> 5) + (tid & 1);
+        ty = (tid & 31) >> 1;
+    }
+}
+
+template <int RN, bool POW2, int GBY>
 __device__ void gather_body(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
                             const float* __restrict__ MS, float* __restrict__ out, int W, int H, const FlowParams& fp,
-                            int x0, int y0, float (&acc)[4]) {
-    constexpr int SRH = GT_H + 2 * RN + 1;
+                            int x0, int y0) {
+    constexpr int SRH = gt_h(GBY) + 2 * RN + 1;
     const int tid = threadIdx.x;
     const bool cm = gather_column_major(x0, W, RN);
-    const int tx = cm ? tid >> 4 : tid & 15, ty = cm ? tid & 15 : tid >> 4;
+    int tx, ty;
+    gather_thread<GBY>(cm, tx, ty);
     const int sw = cm ? SR_W : SR_W - 4;  // row stride: padded only for the column-major mapping
     float* sxmin = sm;                    // SRH x sw each
     float* sxmax = sxmin + sw * SRH;
@@ -472,9 +547,8 @@ __device__ void gather_body(float* sm, const float* __restrict__ DX, const float
             make_float4(__fadd_rn(dy.x, s), __fadd_rn(dy.y, s), __fadd_rn(dy.z, s), __fadd_rn(dy.w, s));
     }
     __syncthreads();
-    const int Y = y0 + ty, X0 = x0 + 4 * tx;
-    if (Y < H && X0 < W)
-        gather_strip<RN, POW2>(sxmin, sxmax, symin, symax, smass, out, W, H, fp, x0, y0, sw, acc);
+    if (y0 + GBY * ty < H && x0 + 4 * tx < W)
+        gather_strip<RN, POW2, GBY>(sxmin, sxmax, symin, symax, smass, out, W, H, fp, x0, y0, sw, tx, ty);
     __syncthreads();
 }
 
@@ -519,32 +593,34 @@ __device__ float gather_generic_2d(const float* __restrict__ DX, const float* __
     return acc;
 }
 
-// One 64x16 tile of one channel of gather_2d; `sm` holds gather_smem_bytes().
-// dxc/dyc/msc/out are that channel's planes.
-template <bool POW2>
+// One 64 x (16 * GBY) tile of one channel of gather_2d; `sm` holds
+// gather_smem_bytes_inl(GBY).  dxc/dyc/msc/out are that channel's planes.
+template <bool POW2, int GBY>
 __device__ void gather_item(float* sm, const float* __restrict__ dxc, const float* __restrict__ dyc,
                             const float* __restrict__ msc, float* __restrict__ out, int W, int H,
                             const FlowParams& fp, int dmax_bits, int x0, int y0) {
     const int RN = window_from_dmax(dmax_bits, fp, max(W, H));
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
     const bool fast = RN <= RN_MAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && !fp.point_mode;
     if (fast) {
         switch (RN) {
-            case 0: gather_body<0, POW2>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0, acc); break;
-            case 1: gather_body<1, POW2>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0, acc); break;
-            case 2: gather_body<2, POW2>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0, acc); break;
-            default: gather_body<3, POW2>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0, acc); break;
+            case 0: gather_body<0, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
+            case 1: gather_body<1, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
+            case 2: gather_body<2, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
+            default: gather_body<3, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
         }
         return;
     }
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int Y = y0 + ty;
 #pragma unroll 1
-    for (int i = 0; i < 4; ++i) {
-        const int X = x0 + 4 * tx + i;
-        if (X < W && Y < H) out[size_t(Y) * W + X] = gather_generic_2d<POW2>(dxc, dyc, msc, W, H, X, Y, RN + 1, fp);
+    for (int d = 0; d < GBY; ++d) {
+        const int Y = y0 + GBY * ty + d;
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int X = x0 + 4 * tx + i;
+            if (X < W && Y < H)
+                out[size_t(Y) * W + X] = gather_generic_2d<POW2>(dxc, dyc, msc, W, H, X, Y, RN + 1, fp);
+        }
     }
 }
-
 
 }  // namespace flp
