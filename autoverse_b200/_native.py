@@ -61,6 +61,7 @@ SIGNATURES = {
     "flp_read_state": (I, [P, P, Z, C.POINTER(F), C.POINTER(U64)]),
     "flp_step": (I, [P]),
     "flp_run": (I, [P, U64]),
+    "flp_step_host": (I, [P, P, Z, C.POINTER(F), C.POINTER(U64), U64]),
     "flp_synchronize": (I, [P]),
     "flp_total_mass": (I, [P, C.POINTER(C.c_double)]),
     "flp_total_mass_f32": (I, [P, C.POINTER(F)]),

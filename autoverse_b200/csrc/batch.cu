@@ -488,6 +488,12 @@ struct flp_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     cudaEvent_t ev[NSTAGE + 1] = {nullptr};
     std::vector<cudaEvent_t> pev;  // per-step event ring of the profiling entry
+    // The size-class kernels of one stage are independent: all but the first
+    // run on side streams forked from and joined back into st, so that in the
+    // captured graph they are parallel branches that fill each other's tails.
+    static constexpr int NSIDE = NCLS - 1;
+    cudaStream_t side[NSIDE] = {nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[NSIDE] = {nullptr};
     void* flush_buf = nullptr;
     size_t flush_bytes = 0;
 
@@ -511,7 +517,7 @@ struct flp_batch {
     // Queue kernels are launched with programmatic stream serialization (they
     // begin with dep_enter), so each one's blocks are placed while its
     // predecessor drains.
-    void launch_queue(int q, Pools& p) {
+    void launch_queue(int q, Pools& p, cudaStream_t qs) {
         if (!n_q[q]) return;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -520,7 +526,7 @@ struct flp_batch {
         cfg.gridDim = dim3(q_grid[q]);
         cfg.blockDim = dim3(256);
         cfg.dynamicSmemBytes = q_smem[q];
-        cfg.stream = st;
+        cfg.stream = qs;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int qq = q;
@@ -532,17 +538,33 @@ struct flp_batch {
     // reset, then per stage the size-class kernels of that stage
     // evs (NSTAGE + 1 events, optional): evs[0] before the step, evs[NSTAGE]
     // after it and, when staged, evs[1..NSTAGE-1] between the stages.
+    // The non-empty queues q0 .. q0+nq-1 of one stage: the first on st, the
+    // others forked onto side streams and joined back.
+    void launch_stage(int q0, int nq, Pools& p) {
+        int act[NCLS], na = 0;
+        for (int q = q0; q < q0 + nq; ++q)
+            if (n_q[q]) act[na++] = q;
+        if (na > 1) ckb(cudaEventRecord(ev_fork, st), "event");
+        for (int k = 1; k < na; ++k) {
+            ckb(cudaStreamWaitEvent(side[k - 1], ev_fork, 0), "fork");
+            launch_queue(act[k], p, side[k - 1]);
+            ckb(cudaEventRecord(ev_join[k - 1], side[k - 1]), "event");
+        }
+        if (na > 0) launch_queue(act[0], p, st);
+        for (int k = 1; k < na; ++k) ckb(cudaStreamWaitEvent(st, ev_join[k - 1], 0), "join");
+    }
+
     void enqueue_step(cudaEvent_t* evs = nullptr, bool staged = false) {
         Pools p = pools();
         if (evs) ckb(cudaEventRecord(evs[0], st), "event");
         launch_dep(k_batch_reset, 1, 256, 0, st, p);
         for (int stage = 0; stage < 3; ++stage) {
-            for (int cls = 0; cls < NCLS; ++cls) launch_queue(stage * NCLS + cls, p);
+            launch_stage(stage * NCLS, NCLS, p);
             if (evs && staged) ckb(cudaEventRecord(evs[stage + 1], st), "event");
         }
-        for (int v = 0; v < NFLOWQ; ++v) launch_queue(QF + v, p);
+        launch_stage(QF, NFLOWQ, p);
         if (evs && staged) ckb(cudaEventRecord(evs[4], st), "event");
-        launch_queue(QG, p);
+        launch_queue(QG, p, st);
         if (evs) ckb(cudaEventRecord(evs[5], st), "event");
         ckb(cudaGetLastError(), "batch launch");
         cur ^= 1;
@@ -562,6 +584,11 @@ struct flp_batch {
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : pev) cudaEventDestroy(e);
         pev.clear();
+        for (cudaEvent_t e : ev_join)
+            if (e) cudaEventDestroy(e);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        for (cudaStream_t q : side)
+            if (q) cudaStreamDestroy(q);
         void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, MS, S, T,
                         KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf, d_stats, d_celloff, d_snaps};
         for (void* q : ptrs)
@@ -593,6 +620,9 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     b->n = n;
     ckb(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
     for (auto& e : b->ev) ckb(cudaEventCreate(&e), "event");
+    for (auto& q : b->side) ckb(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking), "stream");
+    ckb(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "event");
+    for (auto& e : b->ev_join) ckb(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
     // ---- per-world layout
     std::vector<KDesc> kd;
     std::vector<int> srcs, slots;

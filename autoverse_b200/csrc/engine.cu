@@ -129,6 +129,7 @@ struct flp_propagator {
     float time = 0.f;
     uint64_t step = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step from A[cur] to A[cur ^ 1]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // profiling
     std::vector<cudaEvent_t> prof_ev;
@@ -548,6 +549,29 @@ static void build_graph(flp_propagator* h) {
     h->graph[c0] = ge;
 }
 
+// A one-step graph per buffer parity, for the steps left over after the
+// GRAPH_STEPS graphs (one launch instead of one per kernel).
+static void build_graph1(flp_propagator* h) {
+    const int c0 = h->cur;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    try {
+        h->enqueue_step();
+    } catch (...) {
+        cudaStreamEndCapture(h->st, &g);
+        if (g) cudaGraphDestroy(g);
+        h->cur = c0;
+        throw;
+    }
+    CK(cudaStreamEndCapture(h->st, &g));
+    h->cur = c0;
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    h->graph1[c0] = ge;
+}
+
 static void run_steps(flp_propagator* h, uint64_t n) {
     ensure_conv_mode(h);
     while (n >= uint64_t(GRAPH_STEPS)) {
@@ -557,13 +581,17 @@ static void run_steps(flp_propagator* h, uint64_t n) {
         n -= GRAPH_STEPS;
     }
     for (uint64_t i = 0; i < n; ++i) {
-        h->enqueue_step();
+        if (!h->graph1[h->cur]) build_graph1(h);
+        CK(cudaGraphLaunch(h->graph1[h->cur], h->st));
+        h->cur ^= 1;
         h->advance_clock(1);
     }
 }
 
 static void invalidate_graphs(flp_propagator* h) {
     for (auto& g : h->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto& g : h->graph1)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
@@ -741,10 +769,23 @@ int flp_read_state(flp_propagator* h, float* out, size_t n, float* time, uint64_
 
 int flp_step(flp_propagator* h) {
     FLP_CHECK_HANDLE(h);
+    FLP_TRY(run_steps(h, 1))
+}
+
+int flp_step_host(flp_propagator* h, float* state, size_t n, float* time, uint64_t* step, uint64_t steps) {
+    FLP_CHECK_HANDLE(h);
     FLP_TRY({
-        ensure_conv_mode(h);
-        h->enqueue_step();
-        h->advance_clock(1);
+        const size_t CN = size_t(h->C) * h->N;
+        if (!state || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "state size mismatch: expected " + std::to_string(CN));
+        ensure_conv_mode(h);  // a pending measurement runs before the state is replaced
+        CK(cudaMemcpyAsync(h->A[h->cur], state, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+        if (time) h->time = *time;
+        if (step) h->step = *step;
+        run_steps(h, steps);
+        CK(cudaMemcpyAsync(state, h->A[h->cur], CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        if (time) *time = h->time;
+        if (step) *step = h->step;
     })
 }
 

@@ -212,6 +212,21 @@ class CudaPropagator:
     def synchronize(self) -> None:
         nat.check(nat.lib().flp_synchronize(self._h))
 
+    def step_host(self, channels: np.ndarray, steps: int = 1, time: float | None = None,
+                  step: int | None = None) -> tuple[float, int]:
+        """Advance a state held in host memory in place (flp_step_host): copy in,
+        `steps` steps, copy back, one synchronisation.  `channels` must be a
+        C-contiguous float32 array of channels*cells values (a PinnedBuffer's
+        array makes both copies DMA transfers).  Returns the advanced (time, step)."""
+        if channels.dtype != np.float32 or not channels.flags["C_CONTIGUOUS"] or not channels.flags["WRITEABLE"]:
+            raise ValueError("channels must be a writeable C-contiguous float32 array")
+        t = C.c_float(self.info().time if time is None else time)
+        s = C.c_uint64(self.info().step if step is None else step)
+        nat.check(nat.lib().flp_step_host(self._h, channels.ctypes.data, channels.size, C.byref(t), C.byref(s),
+                                          C.c_uint64(int(steps))))
+        self._bound_state = None
+        return t.value, s.value
+
     def read_state(self) -> np.ndarray:
         info = self.info()
         out = np.empty((info.channels, info.width * info.height * info.depth), dtype=np.float32)

@@ -425,18 +425,15 @@ def main():
         with open(prof_json) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
 
-    # end to end through the public API with pinned host buffers: every step
-    # uploads its input from one pinned buffer and reads its result into the
-    # other, which is the next step's input
-    pins = [fl.propagator.PinnedBuffer(state.shape), fl.propagator.PinnedBuffer(state.shape)]
-    pins[0].array[...] = state
-    lib = nat.lib()
+    # end to end through the public API on a state in pinned host memory, the
+    # reference's step(&mut state): every step copies the state in, advances
+    # it one step and copies the result back into the same buffer (one C call,
+    # one synchronisation)
+    pin = fl.propagator.PinnedBuffer(state.shape)
+    pin.array[...] = state
 
     def e2e_step(s):
-        src, dst = pins[s & 1].array, pins[(s + 1) & 1].array
-        p.write_state(src)
-        p.run_device(1)
-        nat.check(lib.flp_read_state(p._h, dst.ctypes.data, dst.size, None, None))
+        p.step_host(pin.array)
 
     for s in range(4):
         e2e_step(s)

@@ -91,6 +91,14 @@ FLP_API int flp_step(flp_propagator* h);
  * from a captured CUDA graph.  Asynchronous. */
 FLP_API int flp_run(flp_propagator* h, uint64_t n);
 
+/* CpuPropagator::step / run on a state held in host memory, the form the
+ * reference's callers use (step(&mut state), src/compute/propagator.rs:239):
+ * copies state[channels*depth*height*width] in (with *time and *step when
+ * given), advances `steps` steps, and copies the state and the advanced clock
+ * back into the same buffers; one stream synchronisation.  With `state` in
+ * pinned memory (flp_host_alloc) both copies are DMA transfers. */
+FLP_API int flp_step_host(flp_propagator* h, float* state, size_t n, float* time, uint64_t* step, uint64_t steps);
+
 /* Wait for the handle's stream; reports device-side status words
  * (FLP_ERR_NONFINITE when the bound check saw a non-finite mass). */
 FLP_API int flp_synchronize(flp_propagator* h);

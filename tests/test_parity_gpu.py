@@ -153,6 +153,30 @@ def test_run_graph_matches_eager_steps():
         assert p1.info().step == 37
 
 
+def test_step_host_matches_device_steps():
+    """flp_step_host (copy in, steps, copy out, one synchronisation) equals
+    write_state + run + read_state bit for bit and advances the clock; works on
+    pinned and on pageable host memory."""
+    cfg, st = species_case(seed=14)
+    with fl.CudaPropagator(cfg) as p1, fl.CudaPropagator(cfg) as p2:
+        p1.write_state(st)
+        p1.run_device(3)
+        ref3 = p1.read_state()
+        p1.run_device(1)
+        ref4 = p1.read_state()
+        pin = fl.propagator.PinnedBuffer(st.shape)
+        pin.array[...] = st
+        t, n = p2.step_host(pin.array, steps=3, time=0.0, step=0)
+        assert np.array_equal(pin.array, ref3)
+        assert n == 3 and t == pytest.approx(float(np.float32(0.2) * 3), rel=1e-6)
+        host = np.array(pin.array)
+        t, n = p2.step_host(host)
+        assert np.array_equal(host, ref4)
+        assert n == 4
+        with pytest.raises(ValueError):
+            p2.step_host(host.astype(np.float64))
+
+
 def nat_step(p):
     from autoverse_b200 import _native as nat
     nat.check(nat.lib().flp_step(p._h))
