@@ -780,6 +780,279 @@ EXPORT void ORC_SYM(prop_run_many)(orc_prop** props, real** states, int n_worlds
 }
 
 /* ---------------------------------------------------------------------- */
+/* EmbeddedPropagator: per-cell parameters advected with mass              */
+/* (src/compute/embedded_propagator.rs:222-372, direct_convolution.rs:     */
+/* 129-177, param_advection.rs:83-165 and 263-320, schema/embedding.rs:    */
+/* 64-166).  CellParams are 5 consecutive reals per cell, in the order of  */
+/* the struct (embedding.rs:20-31): mu, sigma, weight, beta_a, n.          */
+/* ---------------------------------------------------------------------- */
+
+#define NPAR 5
+
+/* CellParams::default (embedding.rs:33-43) */
+static const real cell_default[NPAR] = {R_LIT(0.15), R_LIT(0.015), R_LIT(1.0), R_LIT(1.0), R_LIT(2.0)};
+
+/* convolve_growth_accumulate_embedded (direct_convolution.rs:133-177):
+ * correlation sum in ky-major order skipping zero taps, then the growth with
+ * the cell's own mu/sigma/weight (of the target channel). */
+EXPORT void ORC_SYM(conv_growth_acc_embedded)(const real* input, const real* kern, int ksize, const real* params,
+                                              real* target, int W, int H) {
+    int k_half = ksize / 2;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t idx = (size_t)y * W + x;
+            real conv_sum = R_LIT(0.0);
+            for (int ky = 0; ky < ksize; ++ky)
+                for (int kx = 0; kx < ksize; ++kx) {
+                    real k_val = kern[ky * ksize + kx];
+                    if (k_val == R_LIT(0.0)) continue;
+                    int sx = ORC_SYM(wrap_coord)(x + kx - k_half, W);
+                    int sy = ORC_SYM(wrap_coord)(y + ky - k_half, H);
+                    conv_sum += input[(size_t)sy * W + sx] * k_val;
+                }
+            const real* cp = params + NPAR * idx;
+            real diff = conv_sum - cp[0];
+            real sigma_sq_2 = R_LIT(2.0) * cp[1] * cp[1];
+            real g = R_LIT(2.0) * R_EXP(-diff * diff / sigma_sq_2) - R_LIT(1.0);
+            target[idx] += cp[2] * g;
+        }
+}
+
+/* compute_distribution_overlap (param_advection.rs:263-300) */
+EXPORT real ORC_SYM(distribution_overlap)(real dest_x, real dest_y, real s, real cell_x, real cell_y) {
+    real dist_x_min = dest_x - s, dist_x_max = dest_x + s;
+    real dist_y_min = dest_y - s, dist_y_max = dest_y + s;
+    real cell_x_max = cell_x + R_LIT(1.0), cell_y_max = cell_y + R_LIT(1.0);
+    real ox0 = r_max(dist_x_min, cell_x), ox1 = r_min(dist_x_max, cell_x_max);
+    real oy0 = r_max(dist_y_min, cell_y), oy1 = r_min(dist_y_max, cell_y_max);
+    real ow = r_max(ox1 - ox0, R_LIT(0.0));
+    real oh = r_max(oy1 - oy0, R_LIT(0.0));
+    real area = ow * oh;
+    real total_area = (R_LIT(2.0) * s) * (R_LIT(2.0) * s);
+    if (total_area > R_LIT(1e-10)) return area / total_area;
+    return (cell_x <= dest_x && dest_x < cell_x_max && cell_y <= dest_y && dest_y < cell_y_max) ? R_LIT(1.0)
+                                                                                                : R_LIT(0.0);
+}
+
+/* CellParams::mix_softmax (embedding.rs:64-125): masses[i] with params rows
+ * prm[i] (NPAR each). */
+EXPORT void ORC_SYM(mix_softmax)(const real* masses, const real* const* prm, int n, real temperature,
+                                 real* out) {
+    if (n == 0) { memcpy(out, cell_default, sizeof(cell_default)); return; }
+    if (n == 1) { memcpy(out, prm[0], sizeof(real) * NPAR); return; }
+    real max_mass = -(real)INFINITY;
+    for (int i = 0; i < n; ++i) max_mass = r_max(max_mass, masses[i]);
+    real* w = (real*)malloc(sizeof(real) * (size_t)n);
+    real weight_sum = R_LIT(0.0);
+    for (int i = 0; i < n; ++i) {
+        w[i] = R_EXP((masses[i] - max_mass) / temperature);
+        weight_sum += w[i];
+    }
+    if (weight_sum > R_LIT(0.0)) {
+        for (int i = 0; i < n; ++i) w[i] /= weight_sum;
+    } else {
+        real uniform = R_LIT(1.0) / (real)n;
+        for (int i = 0; i < n; ++i) w[i] = uniform;
+    }
+    for (int f = 0; f < NPAR; ++f) out[f] = R_LIT(0.0);
+    for (int i = 0; i < n; ++i)
+        for (int f = 0; f < NPAR; ++f) out[f] += prm[i][f] * w[i];
+    free(w);
+}
+
+/* CellParams::mix_linear (embedding.rs:127-166) */
+EXPORT void ORC_SYM(mix_linear)(const real* masses, const real* const* prm, int n, real* out) {
+    if (n == 0) { memcpy(out, cell_default, sizeof(cell_default)); return; }
+    if (n == 1) { memcpy(out, prm[0], sizeof(real) * NPAR); return; }
+    real total = R_LIT(0.0);
+    for (int i = 0; i < n; ++i) total += masses[i];
+    if (total <= R_LIT(0.0)) { memcpy(out, cell_default, sizeof(cell_default)); return; }
+    for (int f = 0; f < NPAR; ++f) out[f] = R_LIT(0.0);
+    for (int i = 0; i < n; ++i) {
+        real w = masses[i] / total;
+        for (int f = 0; f < NPAR; ++f) out[f] += prm[i][f] * w;
+    }
+}
+
+/* compute_max_flow_magnitude (param_advection.rs:303-309): fold(0, f32::max). */
+EXPORT real ORC_SYM(max_flow_magnitude)(const real* fx, const real* fy, size_t n) {
+    real m = R_LIT(0.0);
+    for (size_t i = 0; i < n; ++i) m = r_max(m, R_SQRT(fx[i] * fx[i] + fy[i] * fy[i]));
+    return m;
+}
+
+/* advect_mass_and_params_into (param_advection.rs:83-165), a gather over
+ * (2R+1)^2 wrapped offsets in dy-major order with R from the largest flow
+ * magnitude.  The overlap is taken between the source's square placed at its
+ * wrapped index plus dt*F and the unwrapped destination cell, as the
+ * reference does.  next_params is left untouched where no mass arrives. */
+EXPORT void ORC_SYM(advect_params2d)(const real* mass, const real* params, const real* fx, const real* fy,
+                                     int linear, real temperature, real dt, real s, int W, int H, real* next_mass,
+                                     real* next_params) {
+    real max_flow = ORC_SYM(max_flow_magnitude)(fx, fy, (size_t)W * H);
+    int R = r_to_i32(R_CEIL(max_flow * dt + s)) + 1;
+    int cap = (2 * R + 1) * (2 * R + 1);
+    real* cm = (real*)malloc(sizeof(real) * (size_t)cap);
+    const real** cpp = (const real**)malloc(sizeof(real*) * (size_t)cap);
+    for (int dest_y = 0; dest_y < H; ++dest_y)
+        for (int dest_x = 0; dest_x < W; ++dest_x) {
+            size_t dest_idx = (size_t)dest_y * W + dest_x;
+            int n = 0;
+            real total_mass = R_LIT(0.0);
+            for (int dy = -R; dy <= R; ++dy)
+                for (int dx = -R; dx <= R; ++dx) {
+                    int src_x = ORC_SYM(wrap_coord)(dest_x + dx, W);
+                    int src_y = ORC_SYM(wrap_coord)(dest_y + dy, H);
+                    size_t src_idx = (size_t)src_y * W + src_x;
+                    real src_mass = mass[src_idx];
+                    if (R_FABS(src_mass) < R_LIT(1e-10)) continue;
+                    real dest_fx = (real)src_x + dt * fx[src_idx];
+                    real dest_fy = (real)src_y + dt * fy[src_idx];
+                    real overlap = ORC_SYM(distribution_overlap)(dest_fx, dest_fy, s, (real)dest_x, (real)dest_y);
+                    if (overlap > R_LIT(0.0)) {
+                        real mc = src_mass * overlap;
+                        total_mass += mc;
+                        cm[n] = mc;
+                        cpp[n] = params + NPAR * src_idx;
+                        ++n;
+                    }
+                }
+            next_mass[dest_idx] = total_mass;
+            if (n > 0 && total_mass > R_LIT(1e-10)) {
+                real* out = next_params + NPAR * dest_idx;
+                if (n == 1) memcpy(out, cpp[0], sizeof(real) * NPAR);
+                else if (linear) ORC_SYM(mix_linear)(cm, cpp, n, out);
+                else ORC_SYM(mix_softmax)(cm, cpp, n, temperature, out);
+            }
+        }
+    free(cm);
+    free(cpp);
+}
+
+typedef struct {
+    int W, H, C, K;
+    real dt, s, temperature;
+    int enabled, linear;
+    int* src;
+    int* tgt;
+    int* ksize;
+    real** kern;
+    real** aff;
+    real** next;
+    real* next_params;  /* C x N x NPAR: the propagator's own parameter buffer */
+    real* csum;
+    real* ga;           /* 2 x N */
+    real* gu;           /* 2 x N */
+    real* flow;         /* 2 x N */
+} orc_emb;
+
+/* EmbeddedPropagator::new (embedded_propagator.rs:177-221).  kparams: K x 6
+ * (radius, weight, mu, sigma, source_channel, target_channel) as for
+ * prop_new; only the stencils and channels are used (growth takes the cells'
+ * parameters).  The propagator's next parameter buffer starts at
+ * CellParams::default(). */
+EXPORT orc_emb* ORC_SYM(emb_new)(int W, int H, int C, real dt, int kernel_radius, int K, const real* kparams,
+                                 const int* ring_count, const real* rings, real s, int enabled, int linear,
+                                 real temperature) {
+    orc_emb* p = (orc_emb*)calloc(1, sizeof(orc_emb));
+    p->W = W; p->H = H; p->C = C; p->K = K;
+    p->dt = dt; p->s = s; p->enabled = enabled; p->linear = linear; p->temperature = temperature;
+    size_t N = (size_t)W * H;
+    int kk = K > 0 ? K : 1;
+    p->src = (int*)malloc(sizeof(int) * kk);
+    p->tgt = (int*)malloc(sizeof(int) * kk);
+    p->ksize = (int*)malloc(sizeof(int) * kk);
+    p->kern = (real**)calloc(kk, sizeof(real*));
+    int roff = 0;
+    for (int k = 0; k < K; ++k) {
+        const real* kp = kparams + 6 * k;
+        p->src[k] = (int)kp[4];
+        p->tgt[k] = (int)kp[5];
+        int size = ORC_SYM(kernel_build)(2, kp[0], kernel_radius, ring_count[k], rings + 3 * roff, NULL);
+        p->ksize[k] = size;
+        p->kern[k] = (real*)malloc(sizeof(real) * (size_t)size * size);
+        ORC_SYM(kernel_build)(2, kp[0], kernel_radius, ring_count[k], rings + 3 * roff, p->kern[k]);
+        roff += ring_count[k];
+    }
+    p->aff = (real**)calloc(C, sizeof(real*));
+    p->next = (real**)calloc(C, sizeof(real*));
+    for (int c = 0; c < C; ++c) {
+        p->aff[c] = (real*)malloc(sizeof(real) * N);
+        p->next[c] = (real*)malloc(sizeof(real) * N);
+    }
+    p->next_params = (real*)malloc(sizeof(real) * N * C * NPAR);
+    for (size_t i = 0; i < N * C; ++i) memcpy(p->next_params + NPAR * i, cell_default, sizeof(cell_default));
+    p->csum = (real*)malloc(sizeof(real) * N);
+    p->ga = (real*)malloc(sizeof(real) * 2 * N);
+    p->gu = (real*)malloc(sizeof(real) * 2 * N);
+    p->flow = (real*)malloc(sizeof(real) * 2 * N);
+    return p;
+}
+
+EXPORT void ORC_SYM(emb_free)(orc_emb* p) {
+    if (!p) return;
+    for (int k = 0; k < p->K; ++k) free(p->kern[k]);
+    for (int c = 0; c < p->C; ++c) { free(p->aff[c]); free(p->next[c]); }
+    free(p->kern); free(p->src); free(p->tgt); free(p->ksize);
+    free(p->aff); free(p->next); free(p->next_params);
+    free(p->csum); free(p->ga); free(p->gu); free(p->flow);
+    free(p);
+}
+
+/* The propagator's own parameter buffer (C x N x NPAR), for checks of the
+ * buffer-swap semantics. */
+EXPORT void ORC_SYM(emb_next_params)(orc_emb* p, real* out) {
+    memcpy(out, p->next_params, sizeof(real) * (size_t)p->W * p->H * p->C * NPAR);
+}
+
+/* EmbeddedPropagator::step (embedded_propagator.rs:222-339) on
+ * state[C][N] and params[C][N][NPAR], in place: channels and parameter grids
+ * are swapped with the propagator's buffers as the reference swaps them. */
+EXPORT void ORC_SYM(emb_step)(orc_emb* p, real* state, real* params, int steps) {
+    size_t N = (size_t)p->W * p->H;
+    size_t PN = N * NPAR;
+    for (int t = 0; t < steps; ++t) {
+        for (int c = 0; c < p->C; ++c) memset(p->aff[c], 0, sizeof(real) * N);
+        for (int k = 0; k < p->K; ++k)
+            ORC_SYM(conv_growth_acc_embedded)(state + (size_t)p->src[k] * N, p->kern[k], p->ksize[k],
+                                              params + (size_t)p->tgt[k] * PN, p->aff[p->tgt[k]], p->W, p->H);
+        memset(p->csum, 0, sizeof(real) * N);
+        for (int c = 0; c < p->C; ++c)
+            for (size_t i = 0; i < N; ++i) p->csum[i] += state[(size_t)c * N + i];
+        ORC_SYM(sobel2d)(p->csum, p->ga, p->ga + N, p->W, p->H);
+        for (int c = 0; c < p->C; ++c) {
+            const real* cp = params + (size_t)c * PN;
+            ORC_SYM(sobel2d)(p->aff[c], p->gu, p->gu + N, p->W, p->H);
+            /* compute_flow_field_embedded_into (embedded_propagator.rs:353-372) */
+            for (size_t i = 0; i < N; ++i) {
+                real alpha = ORC_SYM(alpha)(p->csum[i], cp[NPAR * i + 3], cp[NPAR * i + 4]);
+                real oma = R_LIT(1.0) - alpha;
+                p->flow[i] = oma * p->gu[i] - alpha * p->ga[i];
+                p->flow[N + i] = oma * p->gu[N + i] - alpha * p->ga[N + i];
+            }
+            real* np_c = p->next_params + (size_t)c * PN;
+            if (p->enabled) {
+                ORC_SYM(advect_params2d)(state + (size_t)c * N, cp, p->flow, p->flow + N, p->linear,
+                                         p->temperature, p->dt, p->s, p->W, p->H, p->next[c], np_c);
+            } else {
+                memset(p->next[c], 0, sizeof(real) * N);
+                ORC_SYM(advect2d)(state + (size_t)c * N, p->flow, p->flow + N, p->next[c], p->W, p->H, p->dt,
+                                  p->s);
+                memcpy(np_c, cp, sizeof(real) * PN);
+            }
+        }
+        /* swap channels (contents) and parameter grids with the propagator's buffers */
+        for (int c = 0; c < p->C; ++c) {
+            real* cur = state + (size_t)c * N;
+            for (size_t i = 0; i < N; ++i) { real v = cur[i]; cur[i] = p->next[c][i]; p->next[c][i] = v; }
+        }
+        for (size_t i = 0; i < PN * p->C; ++i) {
+            real v = params[i]; params[i] = p->next_params[i]; p->next_params[i] = v;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------- */
 /* Seeds: src/schema/seed.rs:160-524                                       */
 /* grid: C x D x H x W, accumulated in place.                              */
 /* ---------------------------------------------------------------------- */

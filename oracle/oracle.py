@@ -65,6 +65,16 @@ def _declare(lib: C.CDLL, p: str, R) -> None:
         "prop_last_flow": (None, [P, P]),
         "prop_run_many": (None, [P, P, I, I, I]),
         "seed_apply": (None, [P, I, I, I, I, I, P, I, C.c_uint64]),
+        "conv_growth_acc_embedded": (None, [P, P, I, P, P, I, I]),
+        "distribution_overlap": (R, [R, R, R, R, R]),
+        "mix_softmax": (None, [P, P, I, R, P]),
+        "mix_linear": (None, [P, P, I, P]),
+        "max_flow_magnitude": (R, [P, P, Z]),
+        "advect_params2d": (None, [P, P, P, P, I, R, R, R, I, I, P, P]),
+        "emb_new": (P, [I, I, I, R, I, I, P, P, P, R, I, I, R]),
+        "emb_free": (None, [P]),
+        "emb_next_params": (None, [P, P]),
+        "emb_step": (None, [P, P, P, I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, p + name)
@@ -403,3 +413,129 @@ def total_mass(g: np.ndarray) -> float:
     f64 = g.dtype == np.float64
     g = np.ascontiguousarray(g)
     return _fn(f64, "total_mass")(_ptr(g), g.size)
+
+
+# ---------------------------------------------------------------------------
+# EmbeddedPropagator (src/compute/embedded_propagator.rs:222-372,
+# direct_convolution.rs:129-177, param_advection.rs:83-165,
+# schema/embedding.rs:64-166).  Parameter grids are [channel][cell][5] with the
+# fields of CellParams in struct order: mu, sigma, weight, beta_a, n.
+# ---------------------------------------------------------------------------
+
+CELL_DEFAULT = (0.15, 0.015, 1.0, 1.0, 2.0)  # CellParams::default (embedding.rs:33-43)
+NPAR = 5
+
+
+def embedding_config(cfg: dict) -> dict:
+    """EmbeddingConfig with serde defaults (embedding.rs:331-352)."""
+    e = dict(cfg.get("embedding") or {})
+    return {"enabled": bool(e.get("enabled", False)), "mixing_temperature": f32(e.get("mixing_temperature", 1.0)),
+            "linear_mixing": bool(e.get("linear_mixing", False))}
+
+
+def default_params(cfg: dict) -> np.ndarray:
+    """EmbeddedState::from_seed's parameter grids (embedded_propagator.rs:41-66):
+    the first kernel's mu/sigma/weight and the flow's beta_a/n in every cell."""
+    ks = cfg["kernels"]
+    mu = f32(ks[0]["mu"]) if ks else 0.15
+    sigma = f32(ks[0]["sigma"]) if ks else 0.015
+    weight = f32(ks[0]["weight"]) if ks else 1.0
+    fl = cfg["flow"]
+    row = np.array([mu, sigma, weight, f32(fl["beta_a"]), f32(fl["n"])], dtype=np.float32)
+    N = cfg["width"] * cfg["height"]
+    return np.tile(row, (cfg["channels"], N, 1))
+
+
+def _rows(params) -> tuple:
+    arr = np.ascontiguousarray(np.asarray(params, dtype=np.float32).reshape(-1, NPAR))
+    ptrs = (C.c_void_p * len(arr))(*[arr.ctypes.data + i * NPAR * 4 for i in range(len(arr))])
+    return arr, ptrs
+
+
+def mix_softmax(masses, params, temperature: float = 1.0) -> np.ndarray:
+    m = np.ascontiguousarray(masses, dtype=np.float32)
+    arr, ptrs = _rows(params)
+    out = np.zeros(NPAR, dtype=np.float32)
+    _fn(False, "mix_softmax")(_ptr(m), C.cast(ptrs, C.c_void_p), len(m), f32(temperature), _ptr(out))
+    return out
+
+
+def mix_linear(masses, params) -> np.ndarray:
+    m = np.ascontiguousarray(masses, dtype=np.float32)
+    arr, ptrs = _rows(params)
+    out = np.zeros(NPAR, dtype=np.float32)
+    _fn(False, "mix_linear")(_ptr(m), C.cast(ptrs, C.c_void_p), len(m), _ptr(out))
+    return out
+
+
+def distribution_overlap(dest_x, dest_y, s, cell_x, cell_y) -> float:
+    return float(_fn(False, "distribution_overlap")(f32(dest_x), f32(dest_y), f32(s), f32(cell_x), f32(cell_y)))
+
+
+def conv_growth_embedded(inp: np.ndarray, kern: np.ndarray, params: np.ndarray, W: int, H: int,
+                         target: np.ndarray | None = None) -> np.ndarray:
+    """convolve_growth_accumulate_embedded into `target` (zeros when None)."""
+    x = np.ascontiguousarray(inp, dtype=np.float32).reshape(-1)
+    k = np.ascontiguousarray(kern, dtype=np.float32)
+    prm = np.ascontiguousarray(params, dtype=np.float32).reshape(-1, NPAR)
+    out = np.zeros(W * H, dtype=np.float32) if target is None else np.ascontiguousarray(target, np.float32).copy()
+    _fn(False, "conv_growth_acc_embedded")(_ptr(x), _ptr(k), k.shape[0], _ptr(prm), _ptr(out), W, H)
+    return out
+
+
+def advect_params2d(mass, params, fx, fy, W: int, H: int, dt: float, s: float, linear: bool = False,
+                    temperature: float = 1.0, next_params: np.ndarray | None = None):
+    """advect_mass_and_params_into; returns (next_mass, next_params) with
+    next_params starting from `next_params` (CellParams::default grids when None,
+    as advect_mass_and_params allocates)."""
+    m = np.ascontiguousarray(mass, dtype=np.float32).reshape(-1)
+    prm = np.ascontiguousarray(params, dtype=np.float32).reshape(-1, NPAR)
+    fxa = np.ascontiguousarray(fx, dtype=np.float32).reshape(-1)
+    fya = np.ascontiguousarray(fy, dtype=np.float32).reshape(-1)
+    nm = np.zeros(W * H, dtype=np.float32)
+    if next_params is None:
+        npr = np.tile(np.array(CELL_DEFAULT, dtype=np.float32), (W * H, 1))
+    else:
+        npr = np.ascontiguousarray(next_params, dtype=np.float32).reshape(-1, NPAR).copy()
+    _fn(False, "advect_params2d")(_ptr(m), _ptr(prm), _ptr(fxa), _ptr(fya), int(linear), f32(temperature),
+                                  f32(dt), f32(s), W, H, _ptr(nm), _ptr(npr))
+    return nm, npr
+
+
+class OracleEmbedded:
+    """EmbeddedPropagator restated in C (f32)."""
+
+    def __init__(self, cfg: dict | str):
+        cfg = normalize_config(cfg)
+        validate_config(cfg)
+        if cfg["depth"] != 1:
+            raise ValueError("parameter embedding is 2D only")
+        self.cfg = cfg
+        self.W, self.H, self.C = cfg["width"], cfg["height"], cfg["channels"]
+        self.N = self.W * self.H
+        kp, rc, ra = _pack_kernels(cfg, False)
+        self._keep = (kp, rc, ra)
+        e = embedding_config(cfg)
+        self._h = _fn(False, "emb_new")(self.W, self.H, self.C, f32(cfg["dt"]), cfg["kernel_radius"],
+                                       len(cfg["kernels"]), _ptr(kp), _ptr(rc), _ptr(ra),
+                                       f32(cfg["flow"]["distribution_size"]), int(e["enabled"]),
+                                       int(e["linear_mixing"]), e["mixing_temperature"])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _fn(False, "emb_free")(h)
+            self._h = None
+
+    def run(self, state: np.ndarray, params: np.ndarray, steps: int = 1):
+        """Returns the advanced (state, params); the oracle keeps its own
+        parameter buffer across calls, as the reference's propagator does."""
+        st = np.ascontiguousarray(state, dtype=np.float32).reshape(self.C, self.N).copy()
+        pr = np.ascontiguousarray(params, dtype=np.float32).reshape(self.C, self.N, NPAR).copy()
+        _fn(False, "emb_step")(self._h, _ptr(st), _ptr(pr), int(steps))
+        return st, pr
+
+    def next_params(self) -> np.ndarray:
+        out = np.zeros((self.C, self.N, NPAR), dtype=np.float32)
+        _fn(False, "emb_next_params")(self._h, _ptr(out))
+        return out
