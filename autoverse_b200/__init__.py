@@ -6,7 +6,8 @@ with a Python mirror of the reference crate's propagator surface.
 from ._native import CONV_AUTO, CONV_DIRECT, CONV_FFT, ConfigError, FlpError
 from .adjoint import AdjointBatch, FlowLeniaFunction
 from .batch import BatchedPropagator
+from .embedded import EmbeddedPropagator, EmbeddedState
 from .propagator import CudaPropagator, SimulationConfig, SimulationState
 
-__all__ = ["AdjointBatch", "FlowLeniaFunction", "BatchedPropagator", "CudaPropagator", "SimulationConfig", "SimulationState", "ConfigError", "FlpError", "CONV_AUTO",
+__all__ = ["AdjointBatch", "FlowLeniaFunction", "BatchedPropagator", "EmbeddedPropagator", "EmbeddedState", "CudaPropagator", "SimulationConfig", "SimulationState", "ConfigError", "FlpError", "CONV_AUTO",
            "CONV_DIRECT", "CONV_FFT"]

@@ -100,6 +100,17 @@ SIGNATURES = {
     "flp_batch_stream": (P, [P]),
     "flp_batch_profile_run": (I, [P, I, I, C.POINTER(F), C.POINTER(F)]),
     "flp_debug_transport": (I, [P, P, P, P, Z]),
+    "flp_emb_create": (I, [S, PP]),
+    "flp_emb_destroy": (I, [P]),
+    "flp_emb_state_from_seed": (I, [P, S]),
+    "flp_emb_write_state": (I, [P, P, Z, P, Z, F, U64]),
+    "flp_emb_read_state": (I, [P, P, Z, P, Z, C.POINTER(F), C.POINTER(U64)]),
+    "flp_emb_step": (I, [P]),
+    "flp_emb_run": (I, [P, U64]),
+    "flp_emb_synchronize": (I, [P]),
+    "flp_emb_total_mass": (I, [P, C.POINTER(C.c_double)]),
+    "flp_emb_profile_run": (I, [P, U64, C.POINTER(F), C.POINTER(F)]),
+    "flp_emb_stream": (P, [P]),
 }
 
 

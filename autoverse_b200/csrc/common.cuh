@@ -38,20 +38,16 @@ struct FlowParams {
 };
 
 // Programmatic dependent launch.  The step's kernels are launched with
-// programmatic stream serialization (launch_dep below), so a kernel's blocks
-// may be placed on the SMs while its predecessor in the stream is finishing.
-// Every such kernel first signals that its own successor may be placed
-// (dep_launch: takes effect once all of this grid's blocks have signalled,
-// i.e. are resident, so the successor never takes a slot this grid needs),
-// then waits for the predecessor to complete with its writes visible
-// (dep_wait) before it touches any global memory.  Launched without the
-// attribute, both are no-ops.
-__device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void dep_enter() {
-    dep_launch();
-    dep_wait();
-}
+// programmatic stream serialization (launch_dep below), so a kernel's launch
+// is processed while its predecessor in the stream drains; each such kernel
+// waits at entry for the predecessor to complete with its writes visible
+// (dep_enter) before it touches global memory.  No kernel signals its
+// dependents early: the implicit signal at exit was measured faster than
+// griddepcontrol.launch_dependents at entry (512x512 step 61.5 vs 65.6 us;
+// parameter-embedded 256x256 step 55 vs 90 us), whose waiting blocks hold SM
+// resources the running kernel needs.  Launched without the attribute, the
+// wait is a no-op.
+__device__ __forceinline__ void dep_enter() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 // Launch with programmatic stream serialization; the kernel must begin with
 // dep_enter().  Errors surface through cudaGetLastError like a <<<>>> launch.

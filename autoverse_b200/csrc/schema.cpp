@@ -201,8 +201,16 @@ SimulationConfig parse_config(const std::string& text) {
     }
     const Json& f = j.at("flow");
     c.flow = {f.at("beta_a").f32(), f.at("n").f32(), f.at("distribution_size").f32()};
-    if (j.has("embedding") && j.at("embedding").kind == Json::Object && j.at("embedding").has("enabled"))
-        c.embedding_enabled = j.at("embedding").at("enabled").b;
+    if (j.has("embedding") && j.at("embedding").kind != Json::Null) {
+        // a present EmbeddingConfig needs all three fields (no per-field serde defaults)
+        const Json& e = j.at("embedding");
+        if (e.kind != Json::Object || !e.has("enabled") || !e.has("mixing_temperature") || !e.has("linear_mixing") ||
+            e.at("enabled").kind != Json::Bool || e.at("linear_mixing").kind != Json::Bool)
+            throw ConfigError("embedding: expected {enabled, mixing_temperature, linear_mixing}");
+        c.embedding_enabled = e.at("enabled").b;
+        c.embedding_temperature = e.at("mixing_temperature").f32();
+        c.embedding_linear = e.at("linear_mixing").b;
+    }
     validate(c);
     return c;
 }

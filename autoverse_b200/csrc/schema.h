@@ -58,7 +58,11 @@ struct SimulationConfig {
     int kernel_radius = 0;
     std::vector<KernelConfig> kernels;
     FlowConfig flow{};
+    // EmbeddingConfig (schema/embedding.rs:331-352); serde fills it with its
+    // Default when the field is absent (config.rs:33-34)
     bool embedding_enabled = false;
+    float embedding_temperature = 1.0f;
+    bool embedding_linear = false;
 
     bool is_3d() const { return depth > 1; }
     size_t grid_size() const { return size_t(width) * height * depth; }

@@ -232,6 +232,46 @@ FLP_API int flp_adj_backward(flp_adjoint* h, const float* dl_dfinal, size_t n, f
 /* Device time of the last forward and backward passes (CUDA events). */
 FLP_API int flp_adj_timings(flp_adjoint* h, float* forward_ms, float* backward_ms);
 
+/* ---- Parameter-embedded worlds -----------------------------------------
+ * EmbeddedPropagator (src/compute/embedded_propagator.rs:144-345): a 2D world
+ * whose cells carry their own CellParams {mu, sigma, weight, beta_a, n}
+ * (src/schema/embedding.rs:20-31) that are advected and mixed with the mass.
+ * The config's "embedding" object is EmbeddingConfig {enabled,
+ * mixing_temperature, linear_mixing} (embedding.rs:331-352).  Parameter grids
+ * cross the ABI as channels*cells*5 floats, cell-major with the 5 fields in
+ * struct order (ParameterGrid's layout, embedding.rs:178-186).  Kernel radii
+ * up to 64 cells; 3D configs are rejected with FLP_ERR_UNSUPPORTED. */
+typedef struct flp_embedded flp_embedded;
+
+/* EmbeddedPropagator::new (embedded_propagator.rs:177-221); the state starts
+ * at zero mass with EmbeddedState::from_seed's parameters. */
+FLP_API int flp_emb_create(const char* config_json, flp_embedded** out);
+FLP_API int flp_emb_destroy(flp_embedded* h);
+/* EmbeddedState::from_seed (embedded_propagator.rs:41-69): the seed's
+ * channels, every cell at the first kernel's mu/sigma/weight and the flow's
+ * beta_a/n; time and step reset to 0. */
+FLP_API int flp_emb_state_from_seed(flp_embedded* h, const char* seed_json);
+/* Replace the state (channels*cells floats) and, when params is not NULL,
+ * its parameter grids (channels*cells*5 floats); both copied in. */
+FLP_API int flp_emb_write_state(flp_embedded* h, const float* channels, size_t n, const float* params,
+                                size_t n_params, float time, uint64_t step);
+/* Copy the state out; channels, params, time and step may each be NULL. */
+FLP_API int flp_emb_read_state(flp_embedded* h, float* channels, size_t n, float* params, size_t n_params,
+                               float* time, uint64_t* step);
+/* EmbeddedPropagator::step / run (embedded_propagator.rs:222-345), on the
+ * handle's stream; run replays a captured CUDA graph.  Asynchronous. */
+FLP_API int flp_emb_step(flp_embedded* h);
+FLP_API int flp_emb_run(flp_embedded* h, uint64_t n);
+/* Wait for the stream; FLP_ERR_NONFINITE when a non-finite mass was seen. */
+FLP_API int flp_emb_synchronize(flp_embedded* h);
+/* FP64 compensated total mass of all channels. */
+FLP_API int flp_emb_total_mass(flp_embedded* h, double* out);
+/* Device time of `steps` steps (CUDA events around flp_emb_run).  With
+ * stage_ms (3 floats) the steps run one by one with events between the
+ * kernels: convolution + growth, flow, gather (totals over the steps). */
+FLP_API int flp_emb_profile_run(flp_embedded* h, uint64_t steps, float* step_ms, float* stage_ms);
+FLP_API void* flp_emb_stream(flp_embedded* h);
+
 /* Allocation-free affinity.  No counterpart in the reference: an addition for
  * callers that may not allocate device memory, such as code enqueued from
  * another framework's plugin or custom operator on that framework's stream,
