@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--adjoint-steps", type=int, default=64)
     ap.add_argument("--adjoint-every", type=int, default=8)
     ap.add_argument("--fitness-candidates", type=int, default=512, help="population of the fitness measurement (0 = skip)")
+    ap.add_argument("--embedded-size", type=int, default=256, help="side of the parameter-embedded world (0 = skip)")
     return ap.parse_args()
 
 
@@ -362,6 +363,64 @@ def measure_fitness(args, dist):
     return out
 
 
+def embedded_workload(side: int):
+    """Two species in one 2-channel world: kernels for all 4 channel pairs
+    (R = 13, the reference's default kernel radius), the left and right halves
+    seeded with distinct CellParams, 20 U(0,1) 24x24 patches per channel,
+    softmax mixing at temperature 1."""
+    from autoverse_b200 import workloads as wl
+    rng = np.random.default_rng(wl.DEFAULT_SEED + 31)
+    ks = [wl.kernel(src=i, tgt=j, rings=wl.random_rings(rng), mu=float(rng.uniform(0.12, 0.18)),
+                    sigma=float(rng.uniform(0.012, 0.02))) for i in range(2) for j in range(2)]
+    cfg = wl.config(side, side, 2, ks, kernel_radius=13)
+    cfg["embedding"] = {"enabled": True, "mixing_temperature": 1.0, "linear_mixing": False}
+    st = np.zeros((2, side, side), np.float32)
+    for c in range(2):
+        for _ in range(20):
+            x, y = rng.integers(0, side - 24, 2)
+            st[c, y:y + 24, x:x + 24] = rng.random((24, 24), dtype=np.float32)
+    prm = np.empty((2, side, side, 5), np.float32)
+    prm[:, :, : side // 2] = [0.15, 0.015, 1.0, 1.0, 2.0]
+    prm[:, :, side // 2:] = [0.2, 0.025, 1.3, 0.8, 2.5]
+    return cfg, st.reshape(2, -1), prm.reshape(2, -1, 5)
+
+
+def measure_embedded(args, dist):
+    """Parameter-embedded world (EmbeddedPropagator): device time of 208
+    graph-replayed steps after 32 warm-up steps, plus per-kernel times of 20
+    eager steps.  CPU leg: the oracle's restatement of the reference's
+    single-threaded EmbeddedPropagator::step on 2 steps of the same world."""
+    import autoverse_b200 as fl
+    side = args.embedded_size
+    cfg, st, prm = embedded_workload(side)
+    steps = 208
+    with fl.EmbeddedPropagator(cfg) as p:
+        p.write(fl.EmbeddedState(st, prm, side, side))
+        p.run_device(32)
+        p.synchronize()
+        if dist:
+            dist.barrier()
+        ms = reduce_max(dist, p.profile_run(steps)["step_ms"])
+        stages = p.profile_run(20, stages=True)["stages"]
+        p.synchronize()
+    cells = side * side
+    out = {"workload": f"{side}x{side} torus, 2 channels, 4 kernels (all pairs), R=13, two species (left/right "
+                       "CellParams), 20 U(0,1) 24x24 patches per channel, softmax mixing T=1",
+           "steps": steps, "us_per_step": 1e3 * ms / steps, "cell_steps_per_s": WORLD * cells * steps / (ms * 1e-3),
+           "stage_us_per_step": {k: 1e3 * v / 20 for k, v in stages.items()}}
+    if RANK == 0 and not args.skip_cpu:
+        from oracle import oracle as O
+        o = O.OracleEmbedded(cfg)
+        o.run(st, prm, 1)
+        t0 = time.perf_counter()
+        o.run(st, prm, 2)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"cell_steps_per_s": cells * 2 / dt, "cores": 1, "kind": "port",
+                               "sample": "2 steps of the same world, C restatement of EmbeddedPropagator::step "
+                                         "(single-threaded, as the reference's)"}
+    return out
+
+
 def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
@@ -448,6 +507,7 @@ def main():
     batched = measure_batched(args, dist) if args.batch_worlds > 0 else None
     adjoint = measure_adjoint(args, dist) if args.adjoint_worlds > 0 else None
     fitness = measure_fitness(args, dist) if args.fitness_candidates > 0 else None
+    embedded = measure_embedded(args, dist) if args.embedded_size > 0 else None
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
@@ -483,6 +543,7 @@ def main():
         "adjoint": adjoint,
         "backward_over_forward": adjoint["backward_over_forward"] if adjoint else None,
         "fitness": fitness,
+        "embedded": embedded,
     }
     print(json.dumps(line), flush=True)
 
