@@ -258,8 +258,8 @@ def measure_batched(args, dist):
     b = fl.BatchedPropagator([c for c, _ in small])
     for i, (_, sd) in enumerate(small):
         b.load_seed(i, sd)
-    steps = 40
-    b.run(16)
+    steps = 48
+    b.run(steps)  # warm-up with the timed step count: every graph either arm replays is built before timing
     b.synchronize()
     t0 = time.perf_counter()
     b.run(steps)
@@ -270,7 +270,7 @@ def measure_batched(args, dist):
     for cfg, sd in small[:48]:
         p = fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT)
         p.load_seed(sd)
-        p.run_device(16)
+        p.run_device(steps)
         props.append(p)
     for p in props:
         p.synchronize()
@@ -286,8 +286,9 @@ def measure_batched(args, dist):
     out["small_worlds_batched_over_plain"] = {
         "batched": v_b, "plain": v_p, "ratio": v_b / v_p,
         "workload": "1024 worlds with sides {64,96,128} per axis (plain: 48 of them, one propagator each, "
-                    "graph-replayed, stepped in turn); both timed the same way: host wall time around "
-                    "device-synchronised run(40) calls on the public API"}
+                    "graph-replayed, each on its own stream, enqueued in turn); both timed the same way after a "
+                    "warm-up of the same length: host wall time around device-synchronised run(48) calls on the "
+                    "public API"}
     return out
 
 
