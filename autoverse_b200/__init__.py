@@ -5,9 +5,10 @@ with a Python mirror of the reference crate's propagator surface.
 """
 from ._native import CONV_AUTO, CONV_DIRECT, CONV_FFT, ConfigError, FlpError
 from .adjoint import AdjointBatch, FlowLeniaFunction
+from .animation import AnimationPlayer, AnimationRecorder
 from .batch import BatchedPropagator
 from .embedded import EmbeddedPropagator, EmbeddedState
 from .propagator import CudaPropagator, SimulationConfig, SimulationState
 
-__all__ = ["AdjointBatch", "FlowLeniaFunction", "BatchedPropagator", "EmbeddedPropagator", "EmbeddedState", "CudaPropagator", "SimulationConfig", "SimulationState", "ConfigError", "FlpError", "CONV_AUTO",
+__all__ = ["AdjointBatch", "AnimationPlayer", "AnimationRecorder", "FlowLeniaFunction", "BatchedPropagator", "EmbeddedPropagator", "EmbeddedState", "CudaPropagator", "SimulationConfig", "SimulationState", "ConfigError", "FlpError", "CONV_AUTO",
            "CONV_DIRECT", "CONV_FFT"]

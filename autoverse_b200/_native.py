@@ -111,6 +111,11 @@ SIGNATURES = {
     "flp_emb_total_mass": (I, [P, C.POINTER(C.c_double)]),
     "flp_emb_profile_run": (I, [P, U64, C.POINTER(F), C.POINTER(F)]),
     "flp_emb_stream": (P, [P]),
+    "flp_rec_create": (I, [P, S, I, C.c_uint32, U64, PP]),
+    "flp_rec_record": (I, [P, C.POINTER(I)]),
+    "flp_rec_run": (I, [P, U64]),
+    "flp_rec_frames_written": (I, [P, C.POINTER(U64)]),
+    "flp_rec_finalize": (I, [P, C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]),
 }
 
 

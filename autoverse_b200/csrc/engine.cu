@@ -426,6 +426,19 @@ static void resolve_conv_mode(flp_propagator* h, int requested) {
     g_tune_cache[key] = h->conv_mode;
 }
 
+PropView prop_view(flp_propagator* h) {
+    PropView v{};
+    v.state = h->A[h->cur];
+    v.stream = h->st;
+    v.width = h->W;
+    v.height = h->H;
+    v.depth = h->D;
+    v.channels = h->C;
+    v.dt = h->cfg.dt;
+    cudaGetDevice(&v.device);
+    return v;
+}
+
 FlowParams flow_params_of(const SimulationConfig& cfg) {
     FlowParams fp{};
     fp.dt = cfg.dt;

@@ -36,6 +36,24 @@ bool make_plan(int L, FftPlan& p);
 struct SimulationConfig;
 FlowParams flow_params_of(const SimulationConfig& cfg);
 
+}  // namespace flp
+
+struct flp_propagator;
+
+namespace flp {
+
+// What the animation recorder (recorder.cu) reads from a single-world handle:
+// the current state buffer (C x D x H x W f32, valid in stream order), the
+// handle's stream, the grid and dt.
+struct PropView {
+    const float* state;
+    cudaStream_t stream;
+    int width, height, depth, channels;
+    float dt;
+    int device;
+};
+PropView prop_view(flp_propagator* h);
+
 // direct convolution + growth
 size_t conv_direct_smem_bytes(int rmax);
 void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, const float* taps, int W, int H, int C,

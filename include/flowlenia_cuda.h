@@ -232,6 +232,35 @@ FLP_API int flp_adj_backward(flp_adjoint* h, const float* dl_dfinal, size_t n, f
 /* Device time of the last forward and backward passes (CUDA events). */
 FLP_API int flp_adj_timings(flp_adjoint* h, float* forward_ms, float* backward_ms);
 
+/* ---- Animation recording ------------------------------------------------
+ * AnimationRecorder (src/animation/recorder.rs:56-200) for a single-world
+ * handle: FLWA files (src/animation/format.rs: 52-byte header, raw f32
+ * little-endian frames of all channels, a 16-byte index entry per frame at
+ * the end) that the reference's AnimationPlayer reads.  Recording does not
+ * stall the handle's stream: a frame is a device copy of the state enqueued
+ * after the steps enqueued so far, moved to pinned host memory on a separate
+ * stream and written by a writer thread; flp_rec_record blocks only while all
+ * 4 frame slots are in flight.  compression: 0 = none; 1 (LZ4) is refused
+ * with FLP_ERR_UNSUPPORTED, as the reference refuses it without its optional
+ * lz4 feature.  The handle must outlive the recorder. */
+typedef struct flp_recorder flp_recorder;
+
+/* AnimationRecorder::new: creates the file and writes a placeholder header.
+ * frame_skip >= 1 records every frame_skip-th call; max_frames 0 = unlimited. */
+FLP_API int flp_rec_create(flp_propagator* h, const char* path, int compression, uint32_t frame_skip,
+                           uint64_t max_frames, flp_recorder** out);
+/* record_frame (recorder.rs:109-166) of the handle's current state, in stream
+ * order; *recorded (may be NULL) says whether this call took a frame. */
+FLP_API int flp_rec_record(flp_recorder* r, int* recorded);
+/* `steps` times: one step of the handle, then flp_rec_record. */
+FLP_API int flp_rec_run(flp_recorder* r, uint64_t steps);
+FLP_API int flp_rec_frames_written(flp_recorder* r, uint64_t* n);
+/* finalize (recorder.rs:171-200): waits for the frames in flight, appends the
+ * index table, rewrites the header with the frame count, closes the file and
+ * frees the recorder; the outputs (may be NULL) are AnimationStats' fields. */
+FLP_API int flp_rec_finalize(flp_recorder* r, uint64_t* frame_count, uint64_t* total_bytes,
+                             uint64_t* avg_frame_bytes);
+
 /* ---- Parameter-embedded worlds -----------------------------------------
  * EmbeddedPropagator (src/compute/embedded_propagator.rs:144-345): a 2D world
  * whose cells carry their own CellParams {mu, sigma, weight, beta_a, n}
