@@ -64,6 +64,7 @@ def parse_args():
     ap.add_argument("--adjoint-every", type=int, default=8)
     ap.add_argument("--fitness-candidates", type=int, default=512, help="population of the fitness measurement (0 = skip)")
     ap.add_argument("--embedded-size", type=int, default=256, help="side of the parameter-embedded world (0 = skip)")
+    ap.add_argument("--record-steps", type=int, default=400, help="steps of the recording measurement (0 = skip)")
     return ap.parse_args()
 
 
@@ -422,6 +423,37 @@ def measure_embedded(args, dist):
     return out
 
 
+def measure_recording(args, dist, cfg, state, mode):
+    """Animation recording of the headline world: `--record-steps` single
+    steps with a frame every 10 steps written to an FLWA file in the system's
+    temporary directory (wall clock including the finalize that waits for the
+    last frame), against the same single steps without recording."""
+    import autoverse_b200 as fl
+    n = args.record_steps
+    with fl.CudaPropagator(cfg, conv_mode=mode) as p:
+        p.write_state(state)
+        for _ in range(16):
+            p.run_device(1)
+        p.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            p.run_device(1)
+        p.synchronize()
+        plain = time.perf_counter() - t0
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "bench.flwa")
+            rec = fl.AnimationRecorder(path, p, frame_skip=10)
+            t0 = time.perf_counter()
+            rec.run(n)
+            stats = rec.finalize()
+            t = time.perf_counter() - t0
+    t, plain = reduce_max(dist, t), reduce_max(dist, plain)
+    return {"workload": f"{n} single steps of the headline world, a frame every 10 steps "
+                        f"({stats['frame_count']} frames of {stats['average_frame_size'] / 2**20:.1f} MiB)",
+            "steps_per_s_recording": n / t, "steps_per_s_without": n / plain, "overhead": t / plain - 1.0,
+            "frames": stats["frame_count"], "mib_per_s_written": stats["total_bytes"] / 2**20 / t}
+
+
 def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
@@ -509,6 +541,7 @@ def main():
     adjoint = measure_adjoint(args, dist) if args.adjoint_worlds > 0 else None
     fitness = measure_fitness(args, dist) if args.fitness_candidates > 0 else None
     embedded = measure_embedded(args, dist) if args.embedded_size > 0 else None
+    recording = measure_recording(args, dist, cfg, state, p.conv_mode) if args.record_steps > 0 else None
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
@@ -545,6 +578,7 @@ def main():
         "backward_over_forward": adjoint["backward_over_forward"] if adjoint else None,
         "fitness": fitness,
         "embedded": embedded,
+        "recording": recording,
     }
     print(json.dumps(line), flush=True)
 
