@@ -98,6 +98,7 @@ SIGNATURES = {
     "flp_batch_total_mass": (I, [P, P, I]),
     "flp_batch_info": (I, [P, C.POINTER(I), C.POINTER(Z), C.POINTER(Z)]),
     "flp_batch_stream": (P, [P]),
+    "flp_batch_kernel_spectra": (I, [P, C.POINTER(I), C.POINTER(Z)]),
     "flp_batch_profile_run": (I, [P, I, I, C.POINTER(F), C.POINTER(F)]),
     "flp_debug_transport": (I, [P, P, P, P, Z]),
     "flp_emb_create": (I, [S, PP]),

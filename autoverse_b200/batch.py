@@ -81,7 +81,11 @@ class BatchedPropagator:
         cc = C.c_size_t()
         cells = C.c_size_t()
         nat.check(nat.lib().flp_batch_info(self._h, C.byref(n), C.byref(cc), C.byref(cells)))
-        return {"worlds": n.value, "cell_channels": cc.value, "cells": cells.value}
+        sets = C.c_int()
+        kb = C.c_size_t()
+        nat.check(nat.lib().flp_batch_kernel_spectra(self._h, C.byref(sets), C.byref(kb)))
+        return {"worlds": n.value, "cell_channels": cc.value, "cells": cells.value, "kernel_spectra": sets.value,
+                "kernel_spectra_bytes": kb.value}
 
     def stream(self) -> int:
         return nat.lib().flp_batch_stream(self._h) or 0

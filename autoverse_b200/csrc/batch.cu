@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -72,7 +73,8 @@ struct BWorld {
     int W, H, C, K, nsrc, mcls, hcls, pad;
     long long offA;  // float offset of channel 0 in the state / U / DX / DY / MS pools
     long long offS;  // float2 offset in the source-spectrum pool
-    long long offT;  // float2 offset in the product and kernel-spectrum pools
+    long long offT;  // float2 offset in the product pool
+    long long offKH; // float2 offset in the kernel-spectrum pool, shared by worlds with the same grid and stencils
     int offKd;       // first kernel descriptor (and spectrum slot) of the world
     int offSrc;      // first source-channel entry
     int twM, twW, twH;
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
         const int slot = p.slots[w.offKd + k];
         const int kx0 = g * ColCfg<H>::NC;
         const int nl = min(ColCfg<H>::NC, Wc - kx0);
-        cols_conv_item<H, true>(fsm, p.S + w.offS + (size_t(slot) * Wc + kx0) * H, p.KH + w.offT + (size_t(k) * Wc + kx0) * H,
+        cols_conv_item<H, true>(fsm, p.S + w.offS + (size_t(slot) * Wc + kx0) * H, p.KH + w.offKH + (size_t(k) * Wc + kx0) * H,
                           p.T + w.offT + (size_t(k) * Wc + kx0) * H, nl, 0, 1.f, p.tw + w.twH);
     }
 }
@@ -460,6 +462,8 @@ struct flp_batch {
     std::vector<BWorld> hw;
     int n = 0;
     size_t cells_total = 0;  // sum of C*N
+    int unique_spectra = 0;  // distinct kernel-spectrum sets in the pool
+    size_t kh_bytes = 0;
     cudaStream_t st = nullptr;
     BWorld* d_worlds = nullptr;
     int2* d_items = nullptr;
@@ -639,7 +643,11 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         tw_index.push_back({L, off});
         return off;
     };
-    long long offA = 0, offS = 0, offT = 0;
+    long long offA = 0, offS = 0, offT = 0, offKH = 0;
+    // Kernel spectra depend only on the grid and the stencils: worlds that
+    // share both (a parameter sweep over growth, flow or dt) share one set.
+    std::map<std::string, long long> kh_of;
+    std::vector<char> kh_owner(n, 0);
     int cmax = 1;
     std::vector<std::vector<KernelStencil>> stencils(n);
     for (int w = 0; w < n; ++w) {
@@ -684,6 +692,22 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         offS += spec * std::max(d.nsrc, 1);
         d.offT = offT;
         offT += spec * std::max(d.K, 1);
+        {
+            std::string key = std::to_string(d.W) + "x" + std::to_string(d.H);
+            for (const KernelStencil& ks : stencils[w]) {
+                key += "|" + std::to_string(ks.size) + ":";
+                key.append(reinterpret_cast<const char*>(ks.data.data()), ks.data.size() * sizeof(float));
+            }
+            auto it = kh_of.find(key);
+            if (it != kh_of.end()) {
+                d.offKH = it->second;
+            } else {
+                d.offKH = offKH;
+                kh_of.emplace(key, offKH);
+                kh_owner[w] = 1;
+                offKH += spec * std::max(d.K, 1);
+            }
+        }
         d.twM = twiddles(d.W / 2);
         d.twW = twiddles(d.W);
         d.twH = twiddles(d.H);
@@ -707,7 +731,9 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     ckb(cudaMemsetAsync(b->U, 0, CN * sizeof(float), b->st), "memset");
     b->S = dalloc_b<float2>(size_t(offS));
     b->T = dalloc_b<float2>(size_t(offT));
-    b->KH = dalloc_b<float2>(size_t(offT));
+    b->KH = dalloc_b<float2>(size_t(offKH));
+    b->unique_spectra = int(kh_of.size());
+    b->kh_bytes = size_t(offKH) * sizeof(float2);
     b->tw = dalloc_b<float2>(tw.size());
     b->d_kd = dalloc_b<KDesc>(kd.size());
     b->d_srcs = dalloc_b<int>(srcs.size());
@@ -739,7 +765,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     // ---- kernel spectra, world by world, with the single-world FFT passes
     for (int w = 0; w < n; ++w) {
         const BWorld& d = b->hw[w];
-        if (d.K == 0) continue;
+        if (d.K == 0 || !kh_owner[w]) continue;  // empty, or computed for an earlier world
         FftGeom g;
         make_plan(d.W / 2, g.pm);
         make_plan(d.H, g.ph);
@@ -755,7 +781,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         float2* d_tmp = dalloc_b<float2>(size_t(d.K) * (d.W / 2 + 1) * d.H);
         ckb(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, b->st), "copy");
         launch_fft_r2c(d_pad, d_tmp, nullptr, d.K, d.W, d.H, g, nullptr, 0, b->st);
-        launch_fft_cols(d_tmp, nullptr, b->KH + d.offT, nullptr, d.K, d.W, d.H, g, 1,
+        launch_fft_cols(d_tmp, nullptr, b->KH + d.offKH, nullptr, d.K, d.W, d.H, g, 1,
                         float(1.0 / (double(d.W) * double(d.H))), b->st);
         ckb(cudaGetLastError(), "kernel spectra");
         ckb(cudaStreamSynchronize(b->st), "sync");
@@ -1027,6 +1053,14 @@ int flp_batch_similarity(flp_batch* b, int slot_a, int slot_b, double* out, int 
         ckb(cudaGetLastError(), "similarity");
         ckb(cudaMemcpyAsync(out, b->d_stats, n * sizeof(double), cudaMemcpyDeviceToHost, b->st), "copy");
         ckb(cudaStreamSynchronize(b->st), "sync");
+    })
+}
+
+int flp_batch_kernel_spectra(flp_batch* b, int* unique_sets, size_t* bytes) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (unique_sets) *unique_sets = b->unique_spectra;
+        if (bytes) *bytes = b->kh_bytes;
     })
 }
 

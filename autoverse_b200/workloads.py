@@ -8,6 +8,8 @@ the engine's benchmark configurations.  All randomness comes from
                         1-3 random rings each, uniform-noise patches.
 * ``batched_worlds``  — many independent 2D worlds of uneven sides, channels,
                         radii and parameters (see batch.py).
+* ``sweep_worlds``    — a growth/flow parameter sweep: worlds of one grid that
+                        share their kernel shapes.
 * ``sphere3d``        — 3D, one spherical-shell kernel, Gaussian-sphere seed.
 """
 from __future__ import annotations
@@ -101,6 +103,29 @@ def batched_worlds(n=4096, sides=BATCH_SIDES, seed=DEFAULT_SEED):
         cfg = config(W, H, C, ks, dt=float(rng.uniform(0.1, 0.3)), kernel_radius=R)
         blobs = [{"center": [float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7))],
                   "radius": float(rng.uniform(0.05, 0.15)), "amplitude": 1.0, "channel": c} for c in range(C)]
+        out.append((cfg, {"pattern": {"type": "MultiBlob", "blobs": blobs}}))
+    return out
+
+
+def sweep_worlds(n=1024, side=256, channels=2, R=13, seed=DEFAULT_SEED, distinct_kernels=False):
+    """A growth/flow parameter sweep: n worlds of one grid sharing one set of
+    K = C*C kernel shapes (rings and radius drawn once), each with its own
+    weights, mu ~ U(0.1,0.3), sigma ~ U(0.01,0.05), dt ~ U(0.1,0.3) and
+    beta_a ~ U(0.5,2); one Gaussian blob per channel.  distinct_kernels gives
+    every world its own ring draw instead (the same per-step work, no shared
+    kernel spectra).  Returns [(config, seed), ...]."""
+    rng = np.random.default_rng(seed)
+    shapes = [random_rings(rng, 1, 2) for _ in range(channels * channels)]
+    out = []
+    for _ in range(n):
+        rings = [random_rings(rng, 1, 2) for _ in shapes] if distinct_kernels else shapes
+        ks = [kernel(i // channels, i % channels, rings[i], weight=float(rng.uniform(0.3, 1.0)),
+                     mu=float(rng.uniform(0.1, 0.3)), sigma=float(rng.uniform(0.01, 0.05)))
+              for i in range(channels * channels)]
+        cfg = config(side, side, channels, ks, dt=float(rng.uniform(0.1, 0.3)), kernel_radius=R,
+                     beta_a=float(rng.uniform(0.5, 2.0)))
+        blobs = [{"center": [float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7))],
+                  "radius": float(rng.uniform(0.05, 0.15)), "amplitude": 1.0, "channel": c} for c in range(channels)]
         out.append((cfg, {"pattern": {"type": "MultiBlob", "blobs": blobs}}))
     return out
 

@@ -65,6 +65,7 @@ def parse_args():
     ap.add_argument("--fitness-candidates", type=int, default=512, help="population of the fitness measurement (0 = skip)")
     ap.add_argument("--embedded-size", type=int, default=256, help="side of the parameter-embedded world (0 = skip)")
     ap.add_argument("--record-steps", type=int, default=400, help="steps of the recording measurement (0 = skip)")
+    ap.add_argument("--sweep-worlds", type=int, default=1024, help="worlds of the parameter-sweep measurement (0 = skip)")
     return ap.parse_args()
 
 
@@ -454,6 +455,37 @@ def measure_recording(args, dist, cfg, state, mode):
             "frames": stats["frame_count"], "mib_per_s_written": stats["total_bytes"] / 2**20 / t}
 
 
+def measure_sweep(args, dist):
+    """Parameter sweep: `--sweep-worlds` worlds of 256x256, 2 channels, 4
+    kernels with one set of kernel shapes and per-world weights, mu, sigma,
+    dt and beta_a, so the batch keeps one kernel-spectrum set; the same sweep
+    with a ring draw per world (the same per-step work, a spectrum set per
+    world) beside it.  Device time of 48 graph-replayed steps after 16, and
+    the host time of creating the batch."""
+    import autoverse_b200 as fl
+    from autoverse_b200 import workloads as wl
+    out = {"workload": f"{args.sweep_worlds} worlds per GPU of 256x256, C=2, K=4, R=13, per-world weight/mu/sigma/"
+                       "dt/beta_a, Gaussian blobs"}
+    for name, distinct in (("shared_kernels", False), ("distinct_kernels", True)):
+        worlds = wl.sweep_worlds(args.sweep_worlds, seed=wl.DEFAULT_SEED + 41 + RANK, distinct_kernels=distinct)
+        t0 = time.perf_counter()
+        b = fl.BatchedPropagator([c for c, _ in worlds])
+        setup = time.perf_counter() - t0
+        for i, (_, sd) in enumerate(worlds):
+            b.load_seed(i, sd)
+        b.run(16)
+        b.synchronize()
+        if dist:
+            dist.barrier()
+        ms = reduce_max(dist, b.profile_run(48, flush_l2=False, stages=False)["step_ms"])
+        info = b.info()
+        out[name] = {"ms_per_step": ms / 48, "cell_steps_per_s": WORLD * info["cells"] * 48 / (ms * 1e-3),
+                     "create_s": setup, "kernel_spectra": info["kernel_spectra"],
+                     "kernel_spectra_mib": info["kernel_spectra_bytes"] / 2**20}
+        b.close()
+    return out
+
+
 def main():
     args = parse_args()
     cfg, state, desc = workload(args.workload)
@@ -542,6 +574,7 @@ def main():
     fitness = measure_fitness(args, dist) if args.fitness_candidates > 0 else None
     embedded = measure_embedded(args, dist) if args.embedded_size > 0 else None
     recording = measure_recording(args, dist, cfg, state, p.conv_mode) if args.record_steps > 0 else None
+    sweep = measure_sweep(args, dist) if args.sweep_worlds > 0 else None
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
@@ -579,6 +612,7 @@ def main():
         "fitness": fitness,
         "embedded": embedded,
         "recording": recording,
+        "sweep": sweep,
     }
     print(json.dumps(line), flush=True)
 

@@ -178,6 +178,10 @@ FLP_API int flp_batch_synchronize(flp_batch* b);
 /* FP64 compensated total mass of every world (n = number of worlds). */
 FLP_API int flp_batch_total_mass(flp_batch* b, double* per_world, int n);
 FLP_API int flp_batch_info(flp_batch* b, int* n_worlds, size_t* cell_channels, size_t* cells);
+/* Kernel spectra in the pool: worlds with the same grid and the same kernel
+ * stencils (parameter sweeps over growth, flow or dt) share one set, computed
+ * once.  Reports the number of distinct sets and their device bytes. */
+FLP_API int flp_batch_kernel_spectra(flp_batch* b, int* unique_sets, size_t* bytes);
 FLP_API void* flp_batch_stream(flp_batch* b);
 /* Trajectory statistics for fitness evaluation (the quantities the reference's
  * FitnessEvaluator samples, src/compute/evolution/fitness.rs:96-240 and

@@ -58,3 +58,25 @@ def test_batch_mass_and_info():
         info = b.info()
         assert info["worlds"] == 5
         assert info["cells"] == sum(c["width"] * c["height"] for c, _ in worlds)
+
+
+def test_sweep_shares_kernel_spectra_and_keeps_single_world_bits():
+    """A parameter sweep (one grid, one set of kernel shapes, per-world growth,
+    flow and dt) stores one kernel-spectrum set; a world of another grid gets
+    its own.  Every world still equals the single-world engine bit for bit."""
+    worlds = wl.sweep_worlds(5, side=64, seed=5) + wl.sweep_worlds(1, side=96, seed=5)
+    with fl.BatchedPropagator([c for c, _ in worlds]) as b:
+        info = b.info()
+        assert info["kernel_spectra"] == 2
+        assert info["kernel_spectra_bytes"] == 8 * 4 * (33 * 64 + 49 * 96)
+        for i, (_, seed) in enumerate(worlds):
+            b.load_seed(i, seed)
+        b.run(11)
+        for i, (cfg, seed) in enumerate(worlds):
+            with fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT) as p:
+                p.load_seed(seed)
+                p.run_device(11)
+                assert np.array_equal(b.read_world(i), p.read_state()), i
+    distinct = wl.sweep_worlds(4, side=64, seed=6, distinct_kernels=True)
+    with fl.BatchedPropagator([c for c, _ in distinct]) as b:
+        assert b.info()["kernel_spectra"] == 4
