@@ -274,6 +274,9 @@ __global__ void __launch_bounds__(256) fft_rows_c2r_growth(const float2* __restr
 }
 
 // ---- plain (single-world) kernels over the items
+// Complex values per CTA of the single-world row passes (a CTA holds
+// E / (W/2) rows).
+constexpr int SW_R2C_ELEMS = 1024, SW_C2R_ELEMS = 1024;
 template <int M>
 __global__ void __launch_bounds__(256) k_r2c_t(const float* __restrict__ A, float2* __restrict__ S,
                                                const int* __restrict__ srcs, int H, const float2* __restrict__ twM,
@@ -285,7 +288,8 @@ __global__ void __launch_bounds__(256) k_r2c_t(const float* __restrict__ A, floa
     const int slot = blockIdx.y;
     const int c = srcs ? srcs[slot] : slot;
     constexpr int W = 2 * M, Wc = M + 1;
-    r2c_rows_item<M>(fsm, A + size_t(c) * W * H, S + size_t(slot) * Wc * H, H, blockIdx.x * RowCfg<M>::NR, twM, twW);
+    r2c_rows_item<M, SW_R2C_ELEMS>(fsm, A + size_t(c) * W * H, S + size_t(slot) * Wc * H, H,
+                                   blockIdx.x * RowCfg<M, SW_R2C_ELEMS>::NR, twM, twW);
 }
 
 template <int H>
@@ -310,7 +314,8 @@ __global__ void __launch_bounds__(256) k_c2r_t(const float2* __restrict__ T, flo
     extern __shared__ __align__(16) float2 fsm[];
     const int c = blockIdx.y;
     constexpr int W = 2 * M;
-    c2r_growth_item<M>(fsm, T, kd, K, c, U + size_t(c) * W * H, H, blockIdx.x * RowCfg<M>::NR, twM, twW);
+    c2r_growth_item<M, SW_C2R_ELEMS>(fsm, T, kd, K, c, U + size_t(c) * W * H, H, blockIdx.x * RowCfg<M, SW_C2R_ELEMS>::NR,
+                                     twM, twW);
 }
 
 template <int M>
@@ -369,8 +374,8 @@ void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W,
     const int M = W / 2;
 #define X(n)                                                                                        \
     if (M == n) {                                                                                   \
-        dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, nsrc);                                   \
-        launch_dep(k_r2c_t<n>, grid, 256, RowCfg<n>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW, reset_slot, \
+        dim3 grid((H + RowCfg<n, SW_R2C_ELEMS>::NR - 1) / RowCfg<n, SW_R2C_ELEMS>::NR, nsrc);       \
+        launch_dep(k_r2c_t<n>, grid, 256, RowCfg<n, SW_R2C_ELEMS>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW, reset_slot, \
                                                             nreset);                                \
         return;                                                                                     \
     }
@@ -406,8 +411,8 @@ void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, in
     const int M = W / 2;
 #define X(n)                                                                                     \
     if (M == n) {                                                                                \
-        dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, C);                                   \
-        launch_dep(k_c2r_t<n>, grid, 256, RowCfg<n>::smem_c2r, st, T, U, kd, K, H, g.twM, g.twW);       \
+        dim3 grid((H + RowCfg<n, SW_C2R_ELEMS>::NR - 1) / RowCfg<n, SW_C2R_ELEMS>::NR, C);       \
+        launch_dep(k_c2r_t<n>, grid, 256, RowCfg<n, SW_C2R_ELEMS>::smem_c2r, st, T, U, kd, K, H, g.twM, g.twW);       \
         return;                                                                                  \
     }
     FLP_ROW_SIZES(X)
