@@ -4,11 +4,17 @@
 // weight, beta_a, n; schema/embedding.rs:20-31) and those parameters travel
 // with the mass.
 //
-// A step is three kernels:
+// A step is three stages:
 //   * emb_conv_growth — for each target channel, the direct torus correlation
 //     of every kernel aimed at it, in kernel order, with the growth evaluated
 //     per cell from that channel's parameter grid (direct_convolution.rs:
-//     133-177, embedded_propagator.rs:235-247);
+//     133-177, embedded_propagator.rs:235-247).  For kernels of radius >= 8
+//     on grids the FFT passes serve, the correlation sums come instead from
+//     the engine's FFT convolution (rows R2C, columns with the spectrum
+//     product, raw inverse rows: one plane per kernel; the stencils are
+//     symmetric, so convolution and correlation agree) and emb_growth applies
+//     the per-cell growth; the sums then differ from the direct ones by f32
+//     rounding only;
 //   * emb_flow — channel sum, Sobel gradients of the sum and of each
 //     affinity, alpha from the cell's own beta_a and n, the flow and the
 //     destinations (embedded_propagator.rs:249-300, 353-372); it also
@@ -53,6 +59,7 @@ constexpr int EC_TW = 32, EC_TH = 16;  // direct convolution tile (32x8 threads,
 constexpr int EC_RPT = EC_TH / 8;
 constexpr int EG_T = 16;               // gather tile (16x16 threads, one destination each)
 constexpr int EG_RSM = 16;             // windows up to this R stage their sources in shared memory
+constexpr int EMB_FFT_MIN_RADIUS = 8;  // the FFT convolution serves kernels at least this wide
 
 struct EKern {
     int src, tgt, size, tap_off;  // taps: the nonzero taps in ky-major order
@@ -157,6 +164,34 @@ __global__ void __launch_bounds__(256) emb_conv_growth(const float* __restrict__
         const int y = y0 + ty + 8 * i, x = x0 + tx;
         if (x < W && y < H) U[size_t(c) * N + size_t(y) * W + x] = u[i];
     }
+}
+
+// Growth of the FFT path: conv holds one plane per kernel (the correlation
+// sums); U[c] = sum over the kernels aimed at c, in kernel order, of the
+// cell's weight times G(conv; mu, sigma) of the cell.  One thread per cell of
+// channel blockIdx.y.  slots[0 .. nslots) are cleared for the flow pass.
+__global__ void __launch_bounds__(256) emb_growth(const float* __restrict__ conv, float* __restrict__ U,
+                                                  const float* __restrict__ P, const EKern* __restrict__ ek, int K,
+                                                  int W, int H, int* slots, int nslots) {
+    dep_enter();
+    const size_t N = size_t(W) * H;
+    const int c = blockIdx.y;
+    if (slots && blockIdx.x == 0 && blockIdx.y == 0)
+        for (int i = threadIdx.x; i < nslots; i += 256) slots[i] = 0;
+    const size_t i = size_t(blockIdx.x) * 256 + threadIdx.x;
+    if (i >= N) return;
+    const float mu = P[(size_t(c) * NPAR + 0) * N + i];
+    const float sig = P[(size_t(c) * NPAR + 1) * N + i];
+    const float wgt = P[(size_t(c) * NPAR + 2) * N + i];
+    const float s2 = __fmul_rn(__fmul_rn(2.0f, sig), sig);
+    float u = 0.f;
+    for (int k = 0; k < K; ++k) {
+        if (ek[k].tgt != c) continue;
+        const float diff = __fsub_rn(conv[size_t(k) * N + i], mu);
+        const float g = __fsub_rn(__fmul_rn(2.0f, expf(__fdiv_rn(__fmul_rn(-diff, diff), s2))), 1.0f);
+        u = __fadd_rn(u, __fmul_rn(wgt, g));
+    }
+    U[size_t(c) * N + i] = u;
 }
 
 // Channel sum at (x, y) in channel order.
@@ -418,6 +453,13 @@ struct flp_embedded {
     double2* d_partial = nullptr;
     int np = 0;
     double* d_mass = nullptr;
+    // FFT convolution (kernels of radius >= EMB_FFT_MIN_RADIUS on FFT grids)
+    bool use_fft = false;
+    FftGeom geom;
+    float2 *d_tw = nullptr, *d_S = nullptr, *d_T = nullptr, *d_KH = nullptr;
+    int *d_srcs = nullptr, *d_kslot = nullptr;
+    int nsrc = 0;
+    float* d_conv = nullptr;  // K planes of correlation sums
     std::vector<float> defaults;  // EmbeddedState::from_seed's CellParams
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     float time = 0.f;
@@ -434,9 +476,17 @@ struct flp_embedded {
         float* an = A[cur ^ 1];
         const float* p = P[pcur];
         mark(0);
-        launch_dep(emb_conv_growth, dim3((W + EC_TW - 1) / EC_TW, (H + EC_TH - 1) / EC_TH, C), dim3(256),
-                   conv_smem(rmax), st, a, U, p, (const EKern*)d_ek, K, (const float*)d_taps, W, H, rmax, d_slots,
-                   1 + C);
+        if (use_fft) {
+            launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, nullptr, 0, st);
+            launch_fft_cols(d_S, d_KH, d_T, d_kslot, K, W, H, geom, 0, 1.f, st);
+            launch_fft_c2r_raw(d_T, d_conv, nullptr, K, W, H, 1.f, false, geom, st);
+            launch_dep(emb_growth, dim3(unsigned((N + 255) / 256), C), dim3(256), size_t(0), st, (const float*)d_conv,
+                       U, p, (const EKern*)d_ek, K, W, H, d_slots, 1 + C);
+        } else {
+            launch_dep(emb_conv_growth, dim3((W + EC_TW - 1) / EC_TW, (H + EC_TH - 1) / EC_TH, C), dim3(256),
+                       conv_smem(rmax), st, a, U, p, (const EKern*)d_ek, K, (const float*)d_taps, W, H, rmax,
+                       d_slots, 1 + C);
+        }
         mark(1);
         launch_dep(emb_flow, dim3((W + 31) / 32, (H + 7) / 8), dim3(256), size_t(0), st, a, (const float*)U, p, DX,
                    DY, MS, C, W, H, fp, d_slots, d_status);
@@ -516,7 +566,8 @@ struct flp_embedded {
         for (auto& row : graph)
             for (auto& g : row)
                 if (g) cudaGraphExecDestroy(g);
-        void* ptrs[] = {A[0], A[1], P[0], P[1], U, DX, DY, MS, d_slots, d_status, d_ek, d_taps, d_partial, d_mass};
+        void* ptrs[] = {A[0], A[1], P[0], P[1], U, DX, DY, MS, d_slots, d_status, d_ek, d_taps, d_partial, d_mass,
+                        d_tw, d_S, d_T, d_KH, d_srcs, d_kslot, d_conv};
         for (void* q : ptrs)
             if (q) cudaFree(q);
         if (st) cudaStreamDestroy(st);
@@ -548,8 +599,10 @@ void emb_create(flp_embedded* h, const char* json) {
     h->temperature = cfg.embedding_temperature;
     std::vector<EKern> ek;
     std::vector<float> taps;
+    std::vector<KernelStencil> stencils;
     for (const KernelConfig& kc : cfg.kernels) {
         KernelStencil ks = build_kernel(kc, cfg.kernel_radius, 2);
+        stencils.push_back(ks);
         if (ks.radius > EMB_MAX_RADIUS)
             throw UnsupportedError("embedded direct convolution supports kernel radii up to 64 cells");
         std::vector<float> vals, packed;
@@ -573,6 +626,7 @@ void emb_create(flp_embedded* h, const char* json) {
                              int(conv_smem(EMB_MAX_RADIUS)));
         cudaFuncSetAttribute((const void*)emb_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gather_smem()));
         transport_2d_set_attributes();
+        fft2d_set_attributes(200 * 1024);
     });
     cke(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking), "stream");
     const size_t CN = size_t(h->C) * h->N;
@@ -593,6 +647,63 @@ void emb_create(flp_embedded* h, const char* json) {
     h->d_taps = ealloc<float>(taps.size());
     if (!ek.empty()) cke(cudaMemcpy(h->d_ek, ek.data(), ek.size() * sizeof(EKern), cudaMemcpyHostToDevice), "upload");
     if (!taps.empty()) cke(cudaMemcpy(h->d_taps, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
+    // FFT convolution for wide kernels on grids the templated passes serve
+    const int W = h->W, H = h->H;
+    if (h->K > 0 && h->rmax >= EMB_FFT_MIN_RADIUS && W % 2 == 0 && fft_row_templated(W / 2) && fft_col_templated(H)) {
+        FftGeom g;
+        if (make_plan(W / 2, g.pm) && make_plan(H, g.ph)) {
+            const int M = W / 2, Wc = M + 1;
+            std::vector<float2> tw;
+            auto twid = [&](int L, int count) {
+                for (int t = 0; t < count; ++t) {
+                    const double ang = -2.0 * M_PI * double(t) / double(L);
+                    tw.push_back(make_float2(float(std::cos(ang)), float(std::sin(ang))));
+                }
+            };
+            twid(M, M);
+            twid(W, Wc);
+            twid(H, H);
+            h->d_tw = ealloc<float2>(tw.size());
+            cke(cudaMemcpy(h->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice), "upload");
+            g.twM = h->d_tw;
+            g.twW = h->d_tw + M;
+            g.twH = h->d_tw + M + Wc;
+            h->geom = g;
+            std::vector<int> srcs, kslot(h->K);
+            for (int k = 0; k < h->K; ++k) {
+                auto it = std::find(srcs.begin(), srcs.end(), ek[k].src);
+                if (it == srcs.end()) { kslot[k] = int(srcs.size()); srcs.push_back(ek[k].src); }
+                else kslot[k] = int(it - srcs.begin());
+            }
+            h->nsrc = int(srcs.size());
+            h->d_srcs = ealloc<int>(srcs.size());
+            h->d_kslot = ealloc<int>(kslot.size());
+            cke(cudaMemcpy(h->d_srcs, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice), "upload");
+            cke(cudaMemcpy(h->d_kslot, kslot.data(), kslot.size() * sizeof(int), cudaMemcpyHostToDevice), "upload");
+            const size_t spec = size_t(Wc) * H;
+            h->d_S = ealloc<float2>(spec * h->nsrc);
+            h->d_T = ealloc<float2>(spec * h->K);
+            h->d_KH = ealloc<float2>(spec * h->K);
+            h->d_conv = ealloc<float>(size_t(h->K) * h->N);
+            // kernel spectra of the wrap-padded stencils, scaled by 1/(W*H)
+            std::vector<float> padded(size_t(h->K) * h->N);
+            for (int k = 0; k < h->K; ++k) {
+                const std::vector<float> pk = pad_kernel(stencils[k], W, H, 1);
+                std::copy(pk.begin(), pk.end(), padded.begin() + size_t(k) * h->N);
+            }
+            float* d_pad = ealloc<float>(padded.size());
+            float2* d_tmp = ealloc<float2>(spec * h->K);
+            cke(cudaMemcpy(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
+            launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, H, g, nullptr, 0, h->st);
+            launch_fft_cols(d_tmp, nullptr, h->d_KH, nullptr, h->K, W, H, g, 1, float(1.0 / (double(W) * double(H))),
+                            h->st);
+            cke(cudaGetLastError(), "kernel spectra");
+            cke(cudaStreamSynchronize(h->st), "sync");
+            cudaFree(d_pad);
+            cudaFree(d_tmp);
+            h->use_fft = true;
+        }
+    }
     h->np = int(std::min<size_t>(1024, (CN + 255) / 256));
     h->d_partial = ealloc<double2>(h->np);
     h->d_mass = ealloc<double>(1);

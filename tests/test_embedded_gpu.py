@@ -4,7 +4,9 @@ restatement of EmbeddedPropagator::step (src/compute/embedded_propagator.rs:
 non-integer n), whose last bit may differ from the host's libm, so state and
 parameters are compared within 1e-5 after one step and 1e-4 after ten (the
 same bar as the plain engine); the direct convolution sum, the overlap
-areas and the mixing arithmetic follow the reference's operation order."""
+areas and the mixing arithmetic follow the reference's operation order.
+Kernels of radius >= 8 on FFT grids (the R = 9, 10 and 12 cases) take the FFT
+convolution, whose sums differ from the direct ones by f32 rounding."""
 import numpy as np
 import pytest
 
@@ -48,6 +50,9 @@ CASES = {
     "one_channel_square": lambda: emb_case(48, 48, C=1, R=9, seed=4),
     "disabled": lambda: emb_case(seed=5, enabled=False),
     "s075": lambda: emb_case(seed=6, s=0.75),
+    # kernels of radius >= 8 on these grids take the FFT convolution
+    "fft_two_channel": lambda: emb_case(64, 48, C=2, R=10, seed=13),
+    "fft_linear_s075": lambda: emb_case(64, 64, C=1, R=12, seed=14, linear=True, s=0.75),
 }
 
 
