@@ -78,7 +78,10 @@ struct UnsupportedError : std::runtime_error {
 size_t conv_smem(int rmax) {
     return sizeof(float) * (size_t(EC_TH + 2 * rmax) * (EC_TW + 2 * rmax) + 2 * size_t(2 * rmax + 1) * (2 * rmax + 1));
 }
-size_t gather_smem() { return sizeof(float) * 3 * size_t(EG_T + 2 * EG_RSM) * (EG_T + 2 * EG_RSM); }
+constexpr int EG_CMAX = 16;  // contributions per destination kept in shared memory
+constexpr int EG_STAGE = 3 * (EG_T + 2 * EG_RSM) * (EG_T + 2 * EG_RSM);  // floats of staged sources
+// staged sources, then per thread EG_CMAX contributions (f32) and their window offsets (u8)
+size_t gather_smem() { return sizeof(float) * (EG_STAGE + EG_CMAX * 256) + EG_CMAX * 256; }
 
 // ---------------------------------------------------------------- kernels --
 
@@ -269,8 +272,11 @@ __device__ __forceinline__ float emb_overlap(float dfx, float dfy, float s, floa
     const float cx1 = __fadd_rn(cx, 1.0f), cy1 = __fadd_rn(cy, 1.0f);
     if (point) return (cx <= dfx && dfx < cx1 && cy <= dfy && dfy < cy1) ? 1.0f : 0.0f;
     const float ox0 = fmaxf(__fsub_rn(dfx, s), cx), ox1 = fminf(__fadd_rn(dfx, s), cx1);
+    const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
+    // without x overlap the area is 0 (or NaN), which never contributes: skip the rest
+    if (!(ow > 0.f)) return 0.f;
     const float oy0 = fmaxf(__fsub_rn(dfy, s), cy), oy1 = fminf(__fadd_rn(dfy, s), cy1);
-    const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f), oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
+    const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
     const float area = __fmul_rn(ow, oh);
     return pow2 ? __fmul_rn(area, inv_area) : __fdiv_rn(area, total_area);
 }
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
                                                   const float* __restrict__ DY, const float* __restrict__ P,
                                                   float* __restrict__ An, float* __restrict__ Pn, int W, int H,
                                                   FlowParams fp, int linear, float temperature,
-                                                  const int* __restrict__ fmax_slots) {
+                                                  const int* __restrict__ slots) {
     dep_enter();
     extern __shared__ float sm[];
     const int c = blockIdx.z;
@@ -297,12 +303,24 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
     const float* dxp = DX + size_t(c) * N;
     const float* dyp = DY + size_t(c) * N;
     const float dt = fp.dt, s = fp.s;
-    const float fm = __int_as_float(fmax_slots[c]);
+    const float fm = __int_as_float(slots[1 + c]);
     const float rv = ceilf(__fadd_rn(__fmul_rn(fm, dt), s));
-    // Rust `as i32` saturates (NaN -> 0); the window is capped at twice the
-    // larger side, far beyond any mass-conserving flow.
+    // The reference's window: Rust `as i32` saturates (NaN -> 0); capped at
+    // twice the larger side, far beyond any mass-conserving flow.
     const int cap = 2 * max(W, H);
-    const int R = 1 + (rv != rv ? 0 : (rv >= float(cap) ? cap : (rv <= -float(cap) ? -cap : int(rv))));
+    const int R_ref = 1 + (rv != rv ? 0 : (rv >= float(cap) ? cap : (rv <= -float(cap) ? -cap : int(rv))));
+    // Only sources with |m| >= 1e-10 contribute, and such a source at offset o
+    // reaches the destination only if |o| <= ceil(s + D) (D: the largest
+    // |dest - x| of a mass-carrying cell, slots[0]; one more cell for the
+    // nearest-cell mode).  Visiting that sub-window in the same dy-major order
+    // gives the same contributions in the same order, unless the reference's
+    // window wraps the torus (it can then visit a source twice): keep it there.
+    int R = R_ref;
+    if (2 * R_ref + 1 <= W && 2 * R_ref + 1 <= H) {
+        const float rd = ceilf(__fadd_rn(__fadd_rn(__int_as_float(slots[0]), fp.pos_eps), s));
+        const int Rd = (rd < float(R_ref) ? int(rd) : R_ref) + (fp.point_mode ? 1 : 0);
+        R = min(R_ref, max(Rd, 0));
+    }
     const int tx = threadIdx.x & (EG_T - 1), ty = threadIdx.x / EG_T;
     const int x0 = blockIdx.x * EG_T, y0 = blockIdx.y * EG_T;
     const int dest_x = x0 + tx, dest_y = y0 + ty;
@@ -327,7 +345,6 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
     const bool pow2 = fp.area_pow2 != 0;
     const float cx = float(dest_x), cy = float(dest_y);
     const int side = 2 * R + 1;
-    const bool masked = R >= 0 && side * side <= 64;
     // window offset (dy, dx): whether the source contributes (|m| >= 1e-10 and
     // a positive overlap), its contribution m * overlap and its index
     auto contrib = [&](int dy, int dx, float& mc, size_t& src) -> bool {
@@ -350,8 +367,12 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
         if (staged) src = size_t(wrap_near(dest_y + dy, H)) * W + wrap_near(dest_x + dx, W);
         return true;
     };
-    // pass 1: mass, contribution count, largest contribution, first source
-    unsigned long long bits = 0ull;
+    // pass 1: mass, contribution count, largest contribution, first source; the
+    // first EG_CMAX contributions and their window offsets stay in shared memory
+    float* cmem = sm + EG_STAGE;                                                  // [e * 256 + thread]
+    unsigned char* cidx = reinterpret_cast<unsigned char*>(cmem + EG_CMAX * 256);  // [e * 256 + thread]
+    const int tid = threadIdx.x;
+    const bool keep = side * side <= 256;  // offsets fit a byte
     float total = 0.f, maxm = -INFINITY;
     int n = 0;
     size_t first = 0;
@@ -363,8 +384,11 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
             total = __fadd_rn(total, mc);
             maxm = fmaxf(maxm, mc);
             if (n == 0) first = src;
+            if (keep && n < EG_CMAX) {
+                cmem[n * 256 + tid] = mc;
+                cidx[n * 256 + tid] = static_cast<unsigned char>((dy + R) * side + (dx + R));
+            }
             ++n;
-            if (masked) bits |= 1ull << ((dy + R) * side + (dx + R));
         }
     const size_t dest = size_t(dest_y) * W + dest_x;
     An[size_t(c) * N + dest] = total;
@@ -376,49 +400,60 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
     } else {
 #pragma unroll
         for (int f = 0; f < NPAR; ++f) out[f] = 0.f;
-        // visit the contributing sources again in offset order
-        auto for_each = [&](auto&& fn) {
-            if (masked) {
-                unsigned long long b = bits;
-                while (b) {
-                    const int j = __ffsll(static_cast<long long>(b)) - 1;
-                    b &= b - 1;
-                    float mc;
-                    size_t src;
-                    contrib(j / side - R, j % side - R, mc, src);
-                    fn(mc, src);
-                }
+        auto accumulate = [&](size_t src, float w) {
+#pragma unroll
+            for (int f = 0; f < NPAR; ++f)
+                out[f] = __fadd_rn(out[f], __fmul_rn(P[(size_t(c) * NPAR + f) * N + src], w));
+        };
+        if (keep && n <= EG_CMAX) {
+            // the contributions from shared memory, in offset order
+            auto src_of = [&](int e) {
+                const int j = cidx[e * 256 + tid];
+                return size_t(wrap_near(dest_y + j / side - R, H)) * W + wrap_near(dest_x + j % side - R, W);
+            };
+            if (linear) {
+                // mix_linear: w = m_i / total (total > 1e-10 here, so never the default)
+                for (int e = 0; e < n; ++e) accumulate(src_of(e), __fdiv_rn(cmem[e * 256 + tid], total));
             } else {
+                // mix_softmax: the weights once, kept in place of the contributions
+                float wsum = 0.f;
+                for (int e = 0; e < n; ++e) {
+                    const float w = expf(__fdiv_rn(__fsub_rn(cmem[e * 256 + tid], maxm), temperature));
+                    cmem[e * 256 + tid] = w;
+                    wsum = __fadd_rn(wsum, w);
+                }
+                if (wsum > 0.f) {
+                    for (int e = 0; e < n; ++e) accumulate(src_of(e), __fdiv_rn(cmem[e * 256 + tid], wsum));
+                } else {
+                    const float uni = __fdiv_rn(1.0f, float(n));
+                    for (int e = 0; e < n; ++e) accumulate(src_of(e), uni);
+                }
+            }
+        } else {
+            // more contributions than kept: visit the window again in offset order
+            auto for_each = [&](auto&& fn) {
                 for (int dy = -R; dy <= R; ++dy)
                     for (int dx = -R; dx <= R; ++dx) {
                         float mc;
                         size_t src;
                         if (contrib(dy, dx, mc, src)) fn(mc, src);
                     }
-            }
-        };
-        auto accumulate = [&](size_t src, float w) {
-#pragma unroll
-            for (int f = 0; f < NPAR; ++f)
-                out[f] = __fadd_rn(out[f], __fmul_rn(P[(size_t(c) * NPAR + f) * N + src], w));
-        };
-        if (linear) {
-            // mix_linear: total of the contributions (the same sum as the mass)
-            if (total <= 0.f) {  // CellParams::default (unreachable past the total > 1e-10 test above)
-                out[0] = 0.15f, out[1] = 0.015f, out[2] = 1.0f, out[3] = 1.0f, out[4] = 2.0f;
-            } else {
+            };
+            if (linear) {
                 for_each([&](float mc, size_t src) { accumulate(src, __fdiv_rn(mc, total)); });
-            }
-        } else {
-            float wsum = 0.f;
-            for_each([&](float mc, size_t) { wsum = __fadd_rn(wsum, expf(__fdiv_rn(__fsub_rn(mc, maxm), temperature))); });
-            if (wsum > 0.f) {
-                for_each([&](float mc, size_t src) {
-                    accumulate(src, __fdiv_rn(expf(__fdiv_rn(__fsub_rn(mc, maxm), temperature)), wsum));
-                });
             } else {
-                const float uni = __fdiv_rn(1.0f, float(n));
-                for_each([&](float, size_t src) { accumulate(src, uni); });
+                float wsum = 0.f;
+                for_each([&](float mc, size_t) {
+                    wsum = __fadd_rn(wsum, expf(__fdiv_rn(__fsub_rn(mc, maxm), temperature)));
+                });
+                if (wsum > 0.f) {
+                    for_each([&](float mc, size_t src) {
+                        accumulate(src, __fdiv_rn(expf(__fdiv_rn(__fsub_rn(mc, maxm), temperature)), wsum));
+                    });
+                } else {
+                    const float uni = __fdiv_rn(1.0f, float(n));
+                    for_each([&](float, size_t src) { accumulate(src, uni); });
+                }
             }
         }
     }
@@ -494,7 +529,7 @@ struct flp_embedded {
         if (enabled) {
             launch_dep(emb_gather, dim3((W + EG_T - 1) / EG_T, (H + EG_T - 1) / EG_T, C), dim3(256), gather_smem(),
                        st, a, (const float*)DX, (const float*)DY, p, an, P[pcur ^ 1], W, H, fp, linear ? 1 : 0,
-                       temperature, (const int*)(d_slots + 1));
+                       temperature, (const int*)d_slots);
             pcur ^= 1;
         } else {
             launch_gather_2d(DX, DY, MS, an, C, W, H, fp, d_slots, st);
