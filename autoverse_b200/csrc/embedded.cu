@@ -58,7 +58,7 @@ constexpr int EMB_GRAPH_STEPS = 16;  // even: a replay returns both buffers to t
 constexpr int EC_TW = 32, EC_TH = 16;  // direct convolution tile (32x8 threads, 2 rows each)
 constexpr int EC_RPT = EC_TH / 8;
 constexpr int EG_T = 16;               // gather tile (16x16 threads, one destination each)
-constexpr int EG_RSM = 16;             // windows up to this R stage their sources in shared memory
+constexpr int EG_RSM = 8;              // windows up to this R stage their sources in shared memory
 constexpr int EMB_FFT_MIN_RADIUS = 8;  // the FFT convolution serves kernels at least this wide
 
 struct EKern {
@@ -79,7 +79,7 @@ size_t conv_smem(int rmax) {
     return sizeof(float) * (size_t(EC_TH + 2 * rmax) * (EC_TW + 2 * rmax) + 2 * size_t(2 * rmax + 1) * (2 * rmax + 1));
 }
 constexpr int EG_CMAX = 16;  // contributions per destination kept in shared memory
-constexpr int EG_STAGE = 3 * (EG_T + 2 * EG_RSM) * (EG_T + 2 * EG_RSM);  // floats of staged sources
+constexpr int EG_STAGE = (3 + NPAR) * (EG_T + 2 * EG_RSM) * (EG_T + 2 * EG_RSM);  // staged source planes
 // staged sources, then per thread EG_CMAX contributions (f32) and their window offsets (u8)
 size_t gather_smem() { return sizeof(float) * (EG_STAGE + EG_CMAX * 256) + EG_CMAX * 256; }
 
@@ -326,9 +326,12 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
     const int dest_x = x0 + tx, dest_y = y0 + ty;
     const bool staged = R >= 0 && R <= EG_RSM;
     const int SW = EG_T + 2 * max(R, 0);
+    // staged planes over the tile's window: mass, destinations, the 5 parameters
     float* sm_m = sm;
     float* sm_x = sm + SW * SW;
     float* sm_y = sm + 2 * SW * SW;
+    float* sm_p = sm + 3 * SW * SW;
+    const float* Pc = P + size_t(c) * NPAR * N;
     if (staged) {
         for (int i = threadIdx.x; i < SW * SW; i += 256) {
             const int ly = i / SW, lx = i - ly * SW;
@@ -336,9 +339,13 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
             sm_m[i] = mass[src];
             sm_x[i] = dxp[src];
             sm_y[i] = dyp[src];
+#pragma unroll
+            for (int f = 0; f < NPAR; ++f) sm_p[f * SW * SW + i] = Pc[size_t(f) * N + src];
         }
         __syncthreads();
     }
+    // field f of a source: `src` is its window index when staged, else its cell index
+    auto param = [&](int f, size_t src) { return staged ? sm_p[f * SW * SW + src] : Pc[size_t(f) * N + src]; };
     if (dest_x >= W || dest_y >= H) return;
     const float total_area = fp.total_area;  // (2s)*(2s) in f32 (param_advection.rs:290)
     const bool point = !(total_area > 1e-10f);
@@ -351,6 +358,7 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
         float m, fx, fy;
         if (staged) {
             const int li = (ty + R + dy) * SW + (tx + R + dx);
+            src = size_t(li);
             m = sm_m[li];
             fx = sm_x[li];
             fy = sm_y[li];
@@ -364,7 +372,6 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
         const float ov = emb_overlap(fx, fy, s, cx, cy, total_area, point, pow2, fp.inv_area);
         if (!(ov > 0.f)) return false;
         mc = __fmul_rn(m, ov);
-        if (staged) src = size_t(wrap_near(dest_y + dy, H)) * W + wrap_near(dest_x + dx, W);
         return true;
     };
     // pass 1: mass, contribution count, largest contribution, first source; the
@@ -396,20 +403,22 @@ __global__ void __launch_bounds__(256) emb_gather(const float* __restrict__ A, c
     float out[NPAR];
     if (n == 1) {
 #pragma unroll
-        for (int f = 0; f < NPAR; ++f) out[f] = P[(size_t(c) * NPAR + f) * N + first];
+        for (int f = 0; f < NPAR; ++f) out[f] = param(f, first);
     } else {
 #pragma unroll
         for (int f = 0; f < NPAR; ++f) out[f] = 0.f;
         auto accumulate = [&](size_t src, float w) {
 #pragma unroll
             for (int f = 0; f < NPAR; ++f)
-                out[f] = __fadd_rn(out[f], __fmul_rn(P[(size_t(c) * NPAR + f) * N + src], w));
+                out[f] = __fadd_rn(out[f], __fmul_rn(param(f, src), w));
         };
         if (keep && n <= EG_CMAX) {
             // the contributions from shared memory, in offset order
-            auto src_of = [&](int e) {
+            auto src_of = [&](int e) -> size_t {
                 const int j = cidx[e * 256 + tid];
-                return size_t(wrap_near(dest_y + j / side - R, H)) * W + wrap_near(dest_x + j % side - R, W);
+                const int dy = j / side - R, dx = j % side - R;
+                if (staged) return size_t((ty + R + dy) * SW + (tx + R + dx));
+                return size_t(wrap_coord(dest_y + dy, H)) * W + wrap_coord(dest_x + dx, W);
             };
             if (linear) {
                 // mix_linear: w = m_i / total (total > 1e-10 here, so never the default)
