@@ -125,6 +125,21 @@ __device__ __forceinline__ int next_item(int* counter, int n) {
     return it < n ? it : -1;
 }
 
+// Wrap-padding of kernel stencils onto W x H planes (Kernel::pad_to_size,
+// kernel.rs:98-117), one block per plane: desc[p] = (tap offset, side, plane).
+// The planes start zeroed; with a side no larger than the grid every tap lands
+// on its own cell, so the scatter equals the reference's sequential writes.
+__global__ void k_pad_taps(const float* __restrict__ taps, const int4* __restrict__ desc, float* __restrict__ out,
+                           int W, int H) {
+    const int4 d = desc[blockIdx.x];
+    const int side = d.y, c = side / 2;
+    float* o = out + size_t(d.z) * W * H;
+    for (int t = threadIdx.x; t < side * side; t += blockDim.x) {
+        const int ky = t / side, kx = t - ky * side;
+        o[size_t((ky - c + H) % H) * W + (kx - c + W) % W] = taps[d.x + t];
+    }
+}
+
 // Zero every queue counter and every world's displacement slot.
 __global__ void k_batch_reset(Pools p) {
     dep_enter();
@@ -669,7 +684,8 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         for (int k = 0; k < d.K; ++k) {
             const KernelConfig& kc = c.kernels[k];
             stencils[w].push_back(build_kernel(kc, c.kernel_radius, 2));
-            (void)pad_kernel(stencils[w].back(), d.W, d.H, 1);  // radius check
+            if (stencils[w].back().radius > d.W || stencils[w].back().radius > d.H)  // pad_kernel's check
+                throw ConfigError("kernel radius " + std::to_string(stencils[w].back().radius) + " exceeds a grid side");
             KDesc kdsc{};
             kdsc.src = kc.source_channel;
             kdsc.tgt = kc.target_channel;
@@ -762,31 +778,88 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     if (!srcs.empty()) ckb(cudaMemcpy(b->d_srcs, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
     if (!slots.empty()) ckb(cudaMemcpy(b->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
     ckb(cudaMemcpy(b->d_worlds, b->hw.data(), n * sizeof(BWorld), cudaMemcpyHostToDevice), "copy");
-    // ---- kernel spectra, world by world, with the single-world FFT passes
-    for (int w = 0; w < n; ++w) {
-        const BWorld& d = b->hw[w];
-        if (d.K == 0 || !kh_owner[w]) continue;  // empty, or computed for an earlier world
-        FftGeom g;
-        make_plan(d.W / 2, g.pm);
-        make_plan(d.H, g.ph);
-        g.twM = b->tw + d.twM;
-        g.twW = b->tw + d.twW;
-        g.twH = b->tw + d.twH;
-        std::vector<float> padded(size_t(d.K) * d.W * d.H);
-        for (int k = 0; k < d.K; ++k) {
-            std::vector<float> pk = pad_kernel(stencils[w][k], d.W, d.H, 1);
-            std::copy(pk.begin(), pk.end(), padded.begin() + size_t(k) * d.W * d.H);
+    // ---- kernel spectra with the single-world FFT passes, one launch pair per
+    // grid size (in chunks): the stencils are wrap-padded on the device and
+    // each world's spectra are copied to its place in the pool; one
+    // synchronisation at the end
+    {
+        std::map<std::pair<int, int>, std::vector<int>> groups;
+        for (int w = 0; w < n; ++w)
+            if (b->hw[w].K > 0 && kh_owner[w]) groups[{b->hw[w].W, b->hw[w].H}].push_back(w);
+        std::vector<void*> scratch;
+        for (const auto& gr : groups) {
+            const int W = gr.first.first, H = gr.first.second;
+            const size_t plane = size_t(W) * H, spec = size_t(W / 2 + 1) * H;
+            const BWorld& d0 = b->hw[gr.second.front()];
+            FftGeom g;
+            make_plan(W / 2, g.pm);
+            make_plan(H, g.ph);
+            g.twM = b->tw + d0.twM;
+            g.twW = b->tw + d0.twW;
+            g.twH = b->tw + d0.twH;
+            const size_t max_planes = std::max<size_t>(1, (size_t(64) << 20) / plane);  // 256 MB of padded planes
+            size_t group_planes = 0, chunk_cap = 0;
+            for (int w : gr.second) group_planes += size_t(b->hw[w].K);
+            for (int w : gr.second) chunk_cap = std::max(chunk_cap, size_t(b->hw[w].K));
+            chunk_cap = std::max(chunk_cap, std::min(group_planes, max_planes));
+            // buffers reused chunk after chunk (stream order keeps the reuse safe)
+            float* d_pad = dalloc_b<float>(chunk_cap * plane);
+            float2* d_tmp = dalloc_b<float2>(chunk_cap * spec);
+            float2* d_out = dalloc_b<float2>(chunk_cap * spec);
+            scratch.insert(scratch.end(), {d_pad, d_tmp, d_out});
+            size_t i0 = 0;
+            while (i0 < gr.second.size()) {
+                // a chunk of worlds of this size
+                size_t i1 = i0, planes = 0;
+                while (i1 < gr.second.size() && (i1 == i0 || planes + size_t(b->hw[gr.second[i1]].K) <= max_planes))
+                    planes += size_t(b->hw[gr.second[i1++]].K);
+                std::vector<float> taps;
+                std::vector<int4> desc;  // per plane: tap offset, stencil side, plane index, unused
+                bool host_pad = false;
+                for (size_t i = i0; i < i1; ++i)
+                    for (const KernelStencil& ks : stencils[gr.second[i]]) {
+                        if (ks.size > W || ks.size > H) host_pad = true;  // wrapped taps overwrite: pad on the host
+                        desc.push_back(make_int4(int(taps.size()), ks.size, int(desc.size()), 0));
+                        taps.insert(taps.end(), ks.data.begin(), ks.data.end());
+                    }
+                if (host_pad) {
+                    std::vector<float> padded(planes * plane);
+                    size_t pi = 0;
+                    for (size_t i = i0; i < i1; ++i)
+                        for (const KernelStencil& ks : stencils[gr.second[i]]) {
+                            const std::vector<float> pk = pad_kernel(ks, W, H, 1);
+                            std::copy(pk.begin(), pk.end(), padded.begin() + (pi++) * plane);
+                        }
+                    ckb(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                        b->st), "copy");
+                    ckb(cudaStreamSynchronize(b->st), "sync");  // the host buffer goes out of scope
+                } else {
+                    float* d_taps = dalloc_b<float>(taps.size());
+                    int4* d_desc = dalloc_b<int4>(desc.size());
+                    scratch.insert(scratch.end(), {d_taps, d_desc});
+                    ckb(cudaMemcpyAsync(d_taps, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice, b->st),
+                        "copy");
+                    ckb(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, b->st),
+                        "copy");
+                    ckb(cudaMemsetAsync(d_pad, 0, planes * plane * sizeof(float), b->st), "memset");
+                    k_pad_taps<<<dim3(unsigned(planes)), 256, 0, b->st>>>(d_taps, d_desc, d_pad, W, H);
+                }
+                launch_fft_r2c(d_pad, d_tmp, nullptr, int(planes), W, H, g, nullptr, 0, b->st);
+                launch_fft_cols(d_tmp, nullptr, d_out, nullptr, int(planes), W, H, g, 1,
+                                float(1.0 / (double(W) * double(H))), b->st);
+                size_t pi = 0;
+                for (size_t i = i0; i < i1; ++i) {
+                    const BWorld& d = b->hw[gr.second[i]];
+                    ckb(cudaMemcpyAsync(b->KH + d.offKH, d_out + pi * spec, size_t(d.K) * spec * sizeof(float2),
+                                        cudaMemcpyDeviceToDevice, b->st), "copy");
+                    pi += size_t(d.K);
+                }
+                ckb(cudaGetLastError(), "kernel spectra");
+                i0 = i1;
+            }
         }
-        float* d_pad = dalloc_b<float>(padded.size());
-        float2* d_tmp = dalloc_b<float2>(size_t(d.K) * (d.W / 2 + 1) * d.H);
-        ckb(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, b->st), "copy");
-        launch_fft_r2c(d_pad, d_tmp, nullptr, d.K, d.W, d.H, g, nullptr, 0, b->st);
-        launch_fft_cols(d_tmp, nullptr, b->KH + d.offKH, nullptr, d.K, d.W, d.H, g, 1,
-                        float(1.0 / (double(d.W) * double(d.H))), b->st);
-        ckb(cudaGetLastError(), "kernel spectra");
         ckb(cudaStreamSynchronize(b->st), "sync");
-        cudaFree(d_pad);
-        cudaFree(d_tmp);
+        for (void* q : scratch) cudaFree(q);
     }
     // ---- work queues, largest worlds first
     std::vector<int> order(n);
