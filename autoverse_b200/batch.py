@@ -60,6 +60,14 @@ class BatchedPropagator:
     def load_seed(self, i: int, seed: Any) -> None:
         nat.check(nat.lib().flp_batch_state_from_seed(self._h, int(i), _to_json(seed).encode()))
 
+    def load_seeds(self, seeds: Sequence[Any]) -> None:
+        """load_seed for every world at once (None leaves a world as it is)."""
+        if len(seeds) != len(self.configs):
+            raise ValueError("need one seed entry per world")
+        blobs = [None if sd is None else _to_json(sd).encode() for sd in seeds]
+        arr = (C.c_char_p * len(blobs))(*blobs)
+        nat.check(nat.lib().flp_batch_states_from_seeds(self._h, arr, len(blobs)))
+
     def read_world(self, i: int) -> np.ndarray:
         out = np.empty(self._shape(i), dtype=np.float32)
         nat.check(nat.lib().flp_batch_read_world(self._h, int(i), out.ctypes.data, out.size, None, None))

@@ -787,6 +787,26 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         for (int w = 0; w < n; ++w)
             if (b->hw[w].K > 0 && kh_owner[w]) groups[{b->hw[w].W, b->hw[w].H}].push_back(w);
         std::vector<void*> scratch;
+        // one scratch region for every size and chunk, reused in stream order:
+        // padded planes, their row spectra and their full spectra
+        size_t cap_pad = 0, cap_spec = 0;
+        for (const auto& gr : groups) {
+            const size_t plane = size_t(gr.first.first) * gr.first.second;
+            const size_t spec = size_t(gr.first.first / 2 + 1) * gr.first.second;
+            const size_t max_planes = std::max<size_t>(1, (size_t(64) << 20) / plane);
+            size_t group_planes = 0, kmax = 0;
+            for (int w : gr.second) {
+                group_planes += size_t(b->hw[w].K);
+                kmax = std::max(kmax, size_t(b->hw[w].K));
+            }
+            const size_t cap = std::max(kmax, std::min(group_planes, max_planes));
+            cap_pad = std::max(cap_pad, cap * plane);
+            cap_spec = std::max(cap_spec, cap * spec);
+        }
+        float* d_pad = groups.empty() ? nullptr : dalloc_b<float>(cap_pad);
+        float2* d_tmp = groups.empty() ? nullptr : dalloc_b<float2>(cap_spec);
+        float2* d_out = groups.empty() ? nullptr : dalloc_b<float2>(cap_spec);
+        scratch.insert(scratch.end(), {d_pad, d_tmp, d_out});
         for (const auto& gr : groups) {
             const int W = gr.first.first, H = gr.first.second;
             const size_t plane = size_t(W) * H, spec = size_t(W / 2 + 1) * H;
@@ -798,15 +818,6 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
             g.twW = b->tw + d0.twW;
             g.twH = b->tw + d0.twH;
             const size_t max_planes = std::max<size_t>(1, (size_t(64) << 20) / plane);  // 256 MB of padded planes
-            size_t group_planes = 0, chunk_cap = 0;
-            for (int w : gr.second) group_planes += size_t(b->hw[w].K);
-            for (int w : gr.second) chunk_cap = std::max(chunk_cap, size_t(b->hw[w].K));
-            chunk_cap = std::max(chunk_cap, std::min(group_planes, max_planes));
-            // buffers reused chunk after chunk (stream order keeps the reuse safe)
-            float* d_pad = dalloc_b<float>(chunk_cap * plane);
-            float2* d_tmp = dalloc_b<float2>(chunk_cap * spec);
-            float2* d_out = dalloc_b<float2>(chunk_cap * spec);
-            scratch.insert(scratch.end(), {d_pad, d_tmp, d_out});
             size_t i0 = 0;
             while (i0 < gr.second.size()) {
                 // a chunk of worlds of this size
@@ -1019,6 +1030,39 @@ int flp_batch_state_from_seed(flp_batch* b, int world, const char* seed_json) {
         ckb(cudaStreamSynchronize(b->st), "sync");
         b->time[world] = 0.f;
         b->steps[world] = 0;
+    })
+}
+
+int flp_batch_states_from_seeds(flp_batch* b, const char* const* seed_jsons, int n) {
+    BATCH_HANDLE(b);
+    BATCH_TRY({
+        if (!seed_jsons || n != b->n) throw std::invalid_argument("need one seed entry per world");
+        // generate on the host into one staging copy of the state pool; worlds
+        // without a seed keep their device state, so copy runs of seeded worlds
+        std::vector<float> pool(b->cells_total);
+        std::vector<char> seeded(n, 0);
+        for (int w = 0; w < n; ++w) {
+            if (!seed_jsons[w]) continue;
+            const std::vector<float> g = generate_seed(seed_jsons[w], b->cfgs[w]);
+            std::copy(g.begin(), g.end(), pool.begin() + b->hw[w].offA);
+            seeded[w] = 1;
+        }
+        for (int w = 0; w < n;) {
+            if (!seeded[w]) { ++w; continue; }
+            int e = w;
+            while (e < n && seeded[e]) ++e;
+            const long long off = b->hw[w].offA;
+            const long long end = e < n ? b->hw[e].offA : (long long)b->cells_total;
+            ckb(cudaMemcpyAsync(b->A[b->cur] + off, pool.data() + off, size_t(end - off) * sizeof(float),
+                                cudaMemcpyHostToDevice, b->st), "copy");
+            w = e;
+        }
+        ckb(cudaStreamSynchronize(b->st), "sync");
+        for (int w = 0; w < n; ++w)
+            if (seeded[w]) {
+                b->time[w] = 0.f;
+                b->steps[w] = 0;
+            }
     })
 }
 

@@ -146,8 +146,7 @@ def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: d
     sample_steps = [0] + list(range(interval, steps + 1, interval))
     snaps = any(k in ("Periodicity", "OscillatorScore") for k in kinds)
     with BatchedPropagator(configs) as b:
-        for i, sd in enumerate(seeds):
-            b.load_seed(i, sd)
+        b.load_seeds(list(seeds))
         n = len(b)
         if snaps:
             b.reserve_snapshots(1 + len(sample_steps))

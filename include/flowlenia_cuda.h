@@ -170,6 +170,9 @@ FLP_API int flp_batch_create(const char* const* config_jsons, int n_worlds, flp_
 FLP_API int flp_batch_destroy(flp_batch* b);
 /* SimulationState::from_seed for one world (time and step reset to 0). */
 FLP_API int flp_batch_state_from_seed(flp_batch* b, int world, const char* seed_json);
+/* The same for every world at once: seed_jsons[w] (NULL leaves world w as it
+ * is), n = number of worlds; one host-to-device copy per run of seeded worlds. */
+FLP_API int flp_batch_states_from_seeds(flp_batch* b, const char* const* seed_jsons, int n);
 FLP_API int flp_batch_write_world(flp_batch* b, int world, const float* state, size_t n);
 FLP_API int flp_batch_read_world(flp_batch* b, int world, float* out, size_t n, float* time, uint64_t* step);
 /* CpuPropagator::run for every world at once; replays a captured CUDA graph. */

@@ -80,3 +80,18 @@ def test_sweep_shares_kernel_spectra_and_keeps_single_world_bits():
     distinct = wl.sweep_worlds(4, side=64, seed=6, distinct_kernels=True)
     with fl.BatchedPropagator([c for c, _ in distinct]) as b:
         assert b.info()["kernel_spectra"] == 4
+
+
+def test_batch_seeds_in_one_call_match_per_world_loads():
+    worlds = small_batch(7, seed=8)
+    seeds = [sd for _, sd in worlds]
+    with fl.BatchedPropagator([c for c, _ in worlds]) as a, fl.BatchedPropagator([c for c, _ in worlds]) as b:
+        for i, sd in enumerate(seeds):
+            a.load_seed(i, sd)
+        b.load_seeds([sd if i % 3 else None for i, sd in enumerate(seeds)])  # worlds 0, 3, 6 left empty
+        for i in range(len(worlds)):
+            got = b.read_world(i)
+            assert np.array_equal(got, a.read_world(i) if i % 3 else np.zeros_like(got)), i
+        b.load_seeds([seeds[i] if i % 3 == 0 else None for i in range(len(seeds))])
+        for i in range(len(worlds)):
+            assert np.array_equal(b.read_world(i), a.read_world(i)), i
