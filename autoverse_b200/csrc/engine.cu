@@ -220,6 +220,8 @@ struct flp_propagator {
     void free_all() {
         for (auto& g : graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        for (auto& g : graph1)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_dmax, d_DX, d_DY, d_MS, d_DZ, d_status, d_partial, d_mass,
                         d_tw, d_S, d_T, d_KH, d_srcs, d_slot};
         for (void* p : ptrs)
