@@ -160,6 +160,31 @@ __device__ __forceinline__ int rot_window(int j, int c, int RN, int size) {
     return -RN + (j - (NW - n_lo));
 }
 
+// rot_window as a rotation: offset j of the wrapped-ascending order is the
+// natural offset (j + r) mod NW (natural index i = k + RN).  At most one of
+// n_hi and n_lo is nonzero when NW <= size.
+__device__ __forceinline__ int window_rotation(int c, int RN, int size) {
+    const int NW = 2 * RN + 2;
+    const int n_hi = max(0, c + RN + 2 - size);
+    const int n_lo = max(0, RN - c);
+    return n_lo > 0 ? n_lo : (NW - n_hi) % NW;
+}
+
+// t[j] <- t[(j + r) mod NW] with selects only (NW a power of two, 0 <= r < NW).
+template <int NW>
+__device__ __forceinline__ void rotate_left(float (&t)[NW], int r) {
+    static_assert((NW & (NW - 1)) == 0, "window width must be a power of two");
+#pragma unroll
+    for (int b = 1; b < NW; b <<= 1) {
+        const bool on = (r & b) != 0;
+        float u[NW];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) u[j] = on ? t[(j + b) % NW] : t[j];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) t[j] = u[j];
+    }
+}
+
 // One 32x8 block of destinations in plane Z of one channel.
 template <int RN, bool POW2>
 __device__ void gather3d_plane(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
@@ -319,6 +344,10 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
     for (int gz = z0 - RN; gz <= z0 + RN; ++gz) load_plane(gz);
     const int lx = tid & (G3_W - 1), ly = tid / G3_W;
     const int X = x0 + lx, Y = y0 + ly;
+    // The wrapped-ascending x order (rot_window) is the natural order
+    // kx = -RN..RN+1 rotated left by rx, so the terms are computed at fixed
+    // shared-memory offsets and rotated in registers before they are added.
+    const int rx = window_rotation(X, RN, W);
     for (int zz = 0; zz < nz; ++zz) {
         const int Z = z0 + zz;
         load_plane(Z + RN + 1);
@@ -332,20 +361,22 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
                 const float* OHk = P + NW * NS;
                 const float* ODk = P + 2 * NW * NS + (kz + RN) * NS;
                 const float* Mm = P + 3 * NW * NS;
+#pragma unroll
                 for (int jy = 0; jy < NW; ++jy) {
                     const int ky = rot_window(jy, Y, RN, H);
-                    const int row = (ly + ky + RN) * SW + lx + RN;
-                    const float* OHr = OHk + (ky + RN) * NS;
+                    const int base = (ly + ky + RN) * SW + lx;  // source of kx = -RN
+                    const float* OHr = OHk + (ky + RN) * NS + base;
+                    float t[NW];
 #pragma unroll
-                    for (int jx = 0; jx < NW; ++jx) {
-                        const int kx = rot_window(jx, X, RN, W);
-                        const int si = row + kx;
-                        const float m = Mm[si];
-                        if (!POW2 && m == 0.f) continue;
-                        const float vol = __fmul_rn(__fmul_rn(OW[(kx + RN) * NS + si], OHr[si]), ODk[si]);
-                        if (POW2) acc = __fadd_rn(acc, __fmul_rn(m, vol));
-                        else if (vol > 0.f) acc = __fadd_rn(acc, __fmul_rn(m, __fdiv_rn(vol, fp.total_area)));
+                    for (int i = 0; i < NW; ++i) {
+                        const float m = Mm[base + i];
+                        const float vol = __fmul_rn(__fmul_rn(OW[i * NS + base + i], OHr[i]), ODk[base + i]);
+                        if (POW2) t[i] = __fmul_rn(m, vol);
+                        else t[i] = (m != 0.f && vol > 0.f) ? __fmul_rn(m, __fdiv_rn(vol, fp.total_area)) : 0.f;
                     }
+                    rotate_left<NW>(t, rx);
+#pragma unroll
+                    for (int i = 0; i < NW; ++i) acc = __fadd_rn(acc, t[i]);
                 }
             }
             out[(size_t(Z) * H + Y) * W + X] = acc;
