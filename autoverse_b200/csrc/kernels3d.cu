@@ -315,33 +315,58 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
     else if (tid < SW + SH) rowy[tid - SW] = wrap_near(y0 - RN + (tid - SW), H);
     __syncthreads();
     const float s = fp.s;
-    auto load_plane = [&](int gz) {  // gz: unwrapped source plane, >= z0 - RN
+    // A source plane is fetched into registers (NSP sources per thread) one
+    // output plane ahead, so its global loads are in flight while the current
+    // plane is gathered, and stored as overlap tables after that.
+    constexpr int NSP = (NS + 255) / 256;
+    auto fetch = [&](int gz, float (&r)[4][NSP]) {  // gz: unwrapped source plane, >= z0 - RN
+        const size_t zoff = size_t(wrap_near(gz, D)) * H;
+#pragma unroll
+        for (int p = 0; p < NSP; ++p) {
+            const int i = tid + 256 * p;
+            if (i < NS) {
+                const int ly = i / SW, lx = i - ly * SW;
+                const size_t idx = (zoff + rowy[ly]) * W + colx[lx];
+                r[0][p] = DX[idx];
+                r[1][p] = DY[idx];
+                r[2][p] = DZ[idx];
+                r[3][p] = MS[idx];
+            }
+        }
+    };
+    auto store = [&](int gz, const float (&r)[4][NSP]) {
         float* P = sm + ((gz - (z0 - RN)) % SD) * M::PLANE;
         float* OW = P;
         float* OH = P + NW * NS;
         float* OD = P + 2 * NW * NS;
         float* Mm = P + 3 * NW * NS;
         const int zw = wrap_near(gz, D);
-        const size_t zoff = size_t(zw) * H;
-        for (int i = tid; i < NS; i += 256) {
-            const int ly = i / SW, lx = i - ly * SW;
-            const int xw = colx[lx], yw = rowy[ly];
-            const size_t idx = (zoff + yw) * W + xw;
-            const float dx = DX[idx], dy = DY[idx], dz = DZ[idx];
-            Mm[i] = MS[idx];
-            const float xa = __fsub_rn(dx, s), xb = __fadd_rn(dx, s);
-            const float ya = __fsub_rn(dy, s), yb = __fadd_rn(dy, s);
-            const float za = __fsub_rn(dz, s), zb = __fadd_rn(dz, s);
 #pragma unroll
-            for (int k = 0; k < NW; ++k) {
-                const int ix = xw - (k - RN), iy = yw - (k - RN), iz = zw - (k - RN);
-                OW[k * NS + i] = fmaxf(__fsub_rn(fminf(float(ix + 1), xb), fmaxf(float(ix), xa)), 0.f);
-                OH[k * NS + i] = fmaxf(__fsub_rn(fminf(float(iy + 1), yb), fmaxf(float(iy), ya)), 0.f);
-                OD[k * NS + i] = fmaxf(__fsub_rn(fminf(float(iz + 1), zb), fmaxf(float(iz), za)), 0.f);
+        for (int p = 0; p < NSP; ++p) {
+            const int i = tid + 256 * p;
+            if (i < NS) {
+                const int ly = i / SW, lx = i - ly * SW;
+                const int xw = colx[lx], yw = rowy[ly];
+                Mm[i] = r[3][p];
+                const float xa = __fsub_rn(r[0][p], s), xb = __fadd_rn(r[0][p], s);
+                const float ya = __fsub_rn(r[1][p], s), yb = __fadd_rn(r[1][p], s);
+                const float za = __fsub_rn(r[2][p], s), zb = __fadd_rn(r[2][p], s);
+#pragma unroll
+                for (int k = 0; k < NW; ++k) {
+                    const int ix = xw - (k - RN), iy = yw - (k - RN), iz = zw - (k - RN);
+                    OW[k * NS + i] = fmaxf(__fsub_rn(fminf(float(ix + 1), xb), fmaxf(float(ix), xa)), 0.f);
+                    OH[k * NS + i] = fmaxf(__fsub_rn(fminf(float(iy + 1), yb), fmaxf(float(iy), ya)), 0.f);
+                    OD[k * NS + i] = fmaxf(__fsub_rn(fminf(float(iz + 1), zb), fmaxf(float(iz), za)), 0.f);
+                }
             }
         }
     };
-    for (int gz = z0 - RN; gz <= z0 + RN; ++gz) load_plane(gz);
+    float raw[4][NSP];
+    for (int gz = z0 - RN; gz <= z0 + RN; ++gz) {
+        fetch(gz, raw);
+        store(gz, raw);
+    }
+    fetch(z0 + RN + 1, raw);
     const int lx = tid & (G3_W - 1), ly = tid / G3_W;
     const int X = x0 + lx, Y = y0 + ly;
     // The wrapped-ascending x order (rot_window) is the natural order
@@ -350,8 +375,9 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
     const int rx = window_rotation(X, RN, W);
     for (int zz = 0; zz < nz; ++zz) {
         const int Z = z0 + zz;
-        load_plane(Z + RN + 1);
+        store(Z + RN + 1, raw);
         __syncthreads();
+        if (zz + 1 < nz) fetch(Z + RN + 2, raw);
         if (X < W && Y < H) {
             float acc = 0.f;
             for (int jz = 0; jz < NW; ++jz) {
