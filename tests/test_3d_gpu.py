@@ -27,11 +27,30 @@ def sphere_case(W=32, H=32, D=32, R=5, C=1, seed=0, steps_in=2, **flow):
     return cfg, st
 
 
+def noise_case(W=32, H=48, D=32, seed=3):
+    """Mass in every cell (0.05 + U(0, 0.1)): every destination's window and
+    every wrapped window order across all six faces carries nonzero terms."""
+    cfg, _ = sphere_case(W, H, D, R=4, steps_in=0)
+    st = (0.05 + 0.1 * np.random.default_rng(seed).random((1, W * H * D))).astype(np.float32)
+    return cfg, st
+
+
+def corner_case():
+    """A sphere centred on a corner of the torus, spread over all eight octants."""
+    cfg, _ = sphere_case(steps_in=0)
+    sd = {"pattern": {"type": "GaussianSphere", "center": [0.02, 0.97, 0.01], "radius": 0.2, "amplitude": 1.0,
+                      "channel": 0}}
+    st = O.OraclePropagator(cfg).run(O.seed_generate(sd, cfg), 2)
+    return cfg, st
+
+
 CASES = {
     "cube32": lambda: sphere_case(),
     "box48x32x64_2ch": lambda: sphere_case(48, 32, 64, R=4, C=2, seed=1),
     "cube32_s05": lambda: sphere_case(distribution_size=0.5),
     "cube32_s075_n3": lambda: sphere_case(distribution_size=0.75, n=3.0),
+    "box32x48x32_noise": noise_case,
+    "cube32_corner": corner_case,
 }
 
 
