@@ -332,6 +332,9 @@ static void setup_fft3d(flp_propagator* h, const std::vector<KernelStencil>& ks)
     if (W % 2 != 0 || !fft_row_templated(W / 2) || !fft_col_templated(H) || !fft_z_templated(D))
         throw FlpError(FLP_ERR_UNSUPPORTED,
                        "3D worlds need an even width with W/2 in {16..256}, H in {32..512}, D in {32..256} (factors 2, 3)");
+    if (h->C > flow3d_max_channels())
+        throw FlpError(FLP_ERR_UNSUPPORTED,
+                       "3D worlds support at most " + std::to_string(flow3d_max_channels()) + " channels");
     FftGeom g;
     make_plan(W / 2, g.pm);
     make_plan(H, g.ph);

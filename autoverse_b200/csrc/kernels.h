@@ -99,6 +99,7 @@ void launch_fft_z(const float2* S, const float2* KH, float2* T, const int* slot_
 
 // 3D transport
 size_t flow3d_smem_bytes(int C);
+int flow3d_max_channels();
 size_t gather3d_smem_bytes();
 void transport_3d_set_attributes();
 void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,

@@ -15,16 +15,21 @@
 namespace flp {
 
 // ------------------------------------------------------------- flow_3d ----
-constexpr int F3_W = 32, F3_H = 8;
-constexpr int F3_RW = F3_W + 2, F3_RH = F3_H + 2, F3_PL = F3_RW * F3_RH, F3_RC = 3 * F3_PL;
+// A CTA owns a 32x8 block of columns in F3_NZ consecutive planes and stages
+// the F3_NZ + 2 planes of A, U and the channel sum that their stencils read.
+constexpr int F3_W = 32, F3_H = 8, F3_NZ = 2;
+constexpr int F3_RW = F3_W + 2, F3_RH = F3_H + 2, F3_PL = F3_RW * F3_RH, F3_NP = F3_NZ + 2, F3_RC = F3_NP * F3_PL;
 
 size_t flow3d_smem_bytes(int C) { return sizeof(float) * (size_t(2 * C + 1) * F3_RC); }
+// Channels whose staged A and U blocks plus the channel sum fit one CTA's
+// shared memory (227 KB).
+int flow3d_max_channels() { return int((227 * 1024 / (sizeof(float) * F3_RC) - 1) / 2); }
 
 // 3D Sobel of a field at the centre of a 3x3x3 window w[z][y][x] (region
 // indices), gradient3d.rs:106-138: each line sum (a + 2b) + c, each gradient
 // ((l_m + 2 l_0) + l_p) / 32, all in f32 without contraction.
 struct Win3 {
-    const float* p;  // element (dz, dy, dx) at p[dz*F3_PL + dy*F3_RW + dx], dz,dy,dx in 0..2
+    const float* p;  // element (dz, dy, dx) at p[dz*F3_PL + dy*F3_RW + dx], dz in 0..F3_NZ+1, dy,dx in 0..2
     __device__ float at(int z, int y, int x) const { return p[z * F3_PL + y * F3_RW + x]; }
 };
 __device__ __forceinline__ float line3(float a, float b, float c) { return __fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, b)), c); }
@@ -32,20 +37,32 @@ __device__ __forceinline__ float diff3(float lm, float lp) { return __fadd_rn(-l
 __device__ __forceinline__ float comb3(float m, float z, float p) {
     return __fmul_rn(__fadd_rn(__fadd_rn(m, __fmul_rn(2.0f, z)), p), 0.03125f);
 }
-__device__ __forceinline__ void sobel3(const Win3& w, float& gx, float& gy, float& gz) {
-    // x gradient: for each z layer, -(column x-1 over y) + (column x+1 over y)
-    float l[3];
-    for (int z = 0; z < 3; ++z)
-        l[z] = diff3(line3(w.at(z, 0, 0), w.at(z, 1, 0), w.at(z, 2, 0)), line3(w.at(z, 0, 2), w.at(z, 1, 2), w.at(z, 2, 2)));
-    gx = comb3(l[0], l[1], l[2]);
-    // y gradient: for each z layer, -(row y-1 over x) + (row y+1 over x)
-    for (int z = 0; z < 3; ++z)
-        l[z] = diff3(line3(w.at(z, 0, 0), w.at(z, 0, 1), w.at(z, 0, 2)), line3(w.at(z, 2, 0), w.at(z, 2, 1), w.at(z, 2, 2)));
-    gy = comb3(l[0], l[1], l[2]);
-    // z gradient: for each x column, -(layer z-1 over y) + (layer z+1 over y)
-    for (int x = 0; x < 3; ++x)
-        l[x] = diff3(line3(w.at(0, 0, x), w.at(0, 1, x), w.at(0, 2, x)), line3(w.at(2, 0, x), w.at(2, 1, x), w.at(2, 2, x)));
-    gz = comb3(l[0], l[1], l[2]);
+
+// The Sobel gradients of the NZ windows that start at layers 0..NZ-1 of an
+// (NZ+2)-layer block (cells at layers 1..NZ).  Per layer z the column sums
+// over y, Ly[z][x] = line3(w(z,0,x), w(z,1,x), w(z,2,x)), and the row sums
+// over x, Lx[z][y] = line3(w(z,y,0), w(z,y,1), w(z,y,2)), are formed once;
+// the reference's terms are exactly these:
+//   x gradient: per layer diff3(Ly[z][0], Ly[z][2]), combined over the window's layers;
+//   y gradient: per layer diff3(Lx[z][0], Lx[z][2]), combined over the window's layers;
+//   z gradient: per column diff3(Ly[first][x], Ly[last][x]), combined over x.
+template <int NZ>
+__device__ __forceinline__ void sobel3_run(const Win3& w, float (&gx)[NZ], float (&gy)[NZ], float (&gz)[NZ]) {
+    constexpr int NL = NZ + 2;
+    float ly[NL][3], dx[NL], dy[NL];
+#pragma unroll
+    for (int z = 0; z < NL; ++z) {
+#pragma unroll
+        for (int x = 0; x < 3; ++x) ly[z][x] = line3(w.at(z, 0, x), w.at(z, 1, x), w.at(z, 2, x));
+        dx[z] = diff3(ly[z][0], ly[z][2]);
+        dy[z] = diff3(line3(w.at(z, 0, 0), w.at(z, 0, 1), w.at(z, 0, 2)), line3(w.at(z, 2, 0), w.at(z, 2, 1), w.at(z, 2, 2)));
+    }
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+        gx[k] = comb3(dx[k], dx[k + 1], dx[k + 2]);
+        gy[k] = comb3(dy[k], dy[k + 1], dy[k + 2]);
+        gz[k] = comb3(diff3(ly[k][0], ly[k + 2][0]), diff3(ly[k][1], ly[k + 2][1]), diff3(ly[k][2], ly[k + 2][2]));
+    }
 }
 
 template <bool POW2>
@@ -55,24 +72,24 @@ __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, cons
                                                int D, FlowParams fp, int* dmax_slot, int* status) {
     dep_enter();
     extern __shared__ __align__(16) float sm[];
-    float* as = sm;                    // C staged A blocks (3 planes each)
+    float* as = sm;                    // C staged A blocks (F3_NP planes each)
     float* us = sm + C * F3_RC;        // C staged U blocks
     float* asum = sm + 2 * C * F3_RC;  // channel sum
-    __shared__ int colx[F3_RW], rowy[F3_RH], plz[3];
+    __shared__ int colx[F3_RW], rowy[F3_RH], plz[F3_NP];
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * F3_W, y0 = blockIdx.y * F3_H, z = blockIdx.z;
+    const int x0 = blockIdx.x * F3_W, y0 = blockIdx.y * F3_H, z0 = blockIdx.z * F3_NZ;
     const size_t N = size_t(W) * H * D;
     if (tid < F3_RW) colx[tid] = wrap_near(x0 - 1 + tid, W);
     else if (tid < F3_RW + F3_RH) rowy[tid - F3_RW] = wrap_near(y0 - 1 + (tid - F3_RW), H);
-    else if (tid < F3_RW + F3_RH + 3) plz[tid - F3_RW - F3_RH] = wrap_near(z - 1 + (tid - F3_RW - F3_RH), D);
+    else if (tid < F3_RW + F3_RH + F3_NP) plz[tid - F3_RW - F3_RH] = wrap_near(z0 - 1 + (tid - F3_RW - F3_RH), D);
     __syncthreads();
     // one staged row (field k, plane pz, row ly) per warp and pass, lanes over
     // its 34 columns: no index division per element
     {
         const int lane = tid & 31, warp = tid >> 5;
         const int x_a = colx[lane], x_b = lane < F3_RW - 32 ? colx[32 + lane] : 0;
-        for (int row = warp; row < 2 * C * 3 * F3_RH; row += 8) {
-            const int k = row / (3 * F3_RH), q = row - k * (3 * F3_RH);
+        for (int row = warp; row < 2 * C * F3_NP * F3_RH; row += 8) {
+            const int k = row / (F3_NP * F3_RH), q = row - k * (F3_NP * F3_RH);
             const int pz = q / F3_RH, ly = q - pz * F3_RH;
             const float* src = (k < C ? A + size_t(k) * N : U + size_t(k - C) * N) +
                                (size_t(plz[pz]) * H + rowy[ly]) * W;
@@ -91,34 +108,45 @@ __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, cons
     __syncthreads();
     const int lx = tid & (F3_W - 1), ly = tid / F3_W;
     const int X = x0 + lx, Y = y0 + ly;
+    const int nz = min(F3_NZ, D - z0);
     float dmax = 0.f;
     bool bad = false;
     if (X < W && Y < H) {
-        const int o = ly * F3_RW + lx;  // (0,0,0) corner of the window
-        float gax, gay, gaz;
-        sobel3(Win3{asum + o}, gax, gay, gaz);
-        const float alpha = alpha_fp(asum[F3_PL + o + F3_RW + 1], fp);
-        const float oma = __fsub_rn(1.0f, alpha);
-        const float agx = __fmul_rn(alpha, gax), agy = __fmul_rn(alpha, gay), agz = __fmul_rn(alpha, gaz);
-        const size_t cell = (size_t(z) * H + Y) * W + X;
+        const int o = ly * F3_RW + lx;  // (0,0,0) corner of the first window
+        float gax[F3_NZ], gay[F3_NZ], gaz[F3_NZ], oma[F3_NZ], agx[F3_NZ], agy[F3_NZ], agz[F3_NZ];
+        sobel3_run<F3_NZ>(Win3{asum + o}, gax, gay, gaz);
+#pragma unroll
+        for (int k = 0; k < F3_NZ; ++k) {
+            const float alpha = alpha_fp(asum[(k + 1) * F3_PL + o + F3_RW + 1], fp);
+            oma[k] = __fsub_rn(1.0f, alpha);
+            agx[k] = __fmul_rn(alpha, gax[k]);
+            agy[k] = __fmul_rn(alpha, gay[k]);
+            agz[k] = __fmul_rn(alpha, gaz[k]);
+        }
         for (int c = 0; c < C; ++c) {
-            float gux, guy, guz;
-            sobel3(Win3{us + c * F3_RC + o}, gux, guy, guz);
-            const float fx = __fsub_rn(__fmul_rn(oma, gux), agx);
-            const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
-            const float fz = __fsub_rn(__fmul_rn(oma, guz), agz);
-            const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
-            const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
-            const float dz = __fadd_rn(float(z), __fmul_rn(fp.dt, fz));
-            float mass = as[c * F3_RC + F3_PL + o + F3_RW + 1];
-            bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy) && isfinite(dz));
-            if (fabsf(mass) < 1e-10f) mass = 0.f;
-            if (mass != 0.f)
-                dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fmaxf(fabsf(dy - float(Y)), fabsf(dz - float(z)))));
-            DX[size_t(c) * N + cell] = dx;
-            DY[size_t(c) * N + cell] = dy;
-            DZ[size_t(c) * N + cell] = dz;
-            MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
+            float gux[F3_NZ], guy[F3_NZ], guz[F3_NZ];
+            sobel3_run<F3_NZ>(Win3{us + c * F3_RC + o}, gux, guy, guz);
+#pragma unroll
+            for (int k = 0; k < F3_NZ; ++k) {
+                if (k >= nz) break;
+                const int z = z0 + k;
+                const size_t cell = (size_t(z) * H + Y) * W + X;
+                const float fx = __fsub_rn(__fmul_rn(oma[k], gux[k]), agx[k]);
+                const float fy = __fsub_rn(__fmul_rn(oma[k], guy[k]), agy[k]);
+                const float fz = __fsub_rn(__fmul_rn(oma[k], guz[k]), agz[k]);
+                const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
+                const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
+                const float dz = __fadd_rn(float(z), __fmul_rn(fp.dt, fz));
+                float mass = as[c * F3_RC + (k + 1) * F3_PL + o + F3_RW + 1];
+                bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy) && isfinite(dz));
+                if (fabsf(mass) < 1e-10f) mass = 0.f;
+                if (mass != 0.f)
+                    dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fmaxf(fabsf(dy - float(Y)), fabsf(dz - float(z)))));
+                DX[size_t(c) * N + cell] = dx;
+                DY[size_t(c) * N + cell] = dy;
+                DZ[size_t(c) * N + cell] = dz;
+                MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
+            }
         }
     }
     if (status && __syncthreads_or(bad ? 1 : 0) && tid == 0) atomicOr(status, STATUS_NONFINITE);
@@ -457,7 +485,7 @@ size_t gather3d_smem_bytes() { return gather3d_dyn_smem(); }
 
 void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
                     int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
-    dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, D);
+    dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, (D + F3_NZ - 1) / F3_NZ);
     if (fp.area_pow2)
         launch_dep(flow_3d<true>, grid, 256, flow3d_smem_bytes(C), st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
     else
@@ -478,8 +506,8 @@ void transport_3d_set_attributes() {
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
-    set((const void*)flow_3d<true>, flow3d_smem_bytes(32));
-    set((const void*)flow_3d<false>, flow3d_smem_bytes(32));
+    set((const void*)flow_3d<true>, flow3d_smem_bytes(flow3d_max_channels()));
+    set((const void*)flow_3d<false>, flow3d_smem_bytes(flow3d_max_channels()));
     set((const void*)gather_3d<true>, gather3d_smem_bytes());
     set((const void*)gather_3d<false>, gather3d_smem_bytes());
 }

@@ -99,3 +99,12 @@ def test_mass3d_conservation():
         p.run_device(50)
         p.synchronize()
         assert abs(p.total_mass() - m0) / m0 < 1e-4
+
+
+def test_3d_channel_limit_is_refused():
+    """A 3D world whose stencil staging does not fit one CTA's shared memory
+    is refused at creation with UNSUPPORTED, not at its first launch."""
+    cfg, _ = sphere_case(steps_in=0)
+    cfg["channels"] = 21
+    with pytest.raises(fl._native.FlpError, match="at most 20 channels"):
+        fl.CudaPropagator(cfg)
