@@ -44,6 +44,18 @@ def corner_case():
     return cfg, st
 
 
+def many_channels_case(C=8, seed=5):
+    """C channels (each with its own kernel and one cross kernel from the
+    previous channel) on a 32^3 torus filled with low-amplitude noise: the
+    flow pass stages 2C+1 blocks (about 93 KB of shared memory at C=8)."""
+    rng = np.random.default_rng(seed)
+    ks = [wl.kernel(c, c, mu=float(rng.uniform(0.1, 0.2)), sigma=0.02) for c in range(C)]
+    ks += [wl.kernel(c - 1, c, weight=0.5) for c in range(1, C)]
+    cfg = wl.config(32, 32, C, ks, kernel_radius=4, depth=32)
+    st = (0.02 + 0.05 * rng.random((C, 32 * 32 * 32))).astype(np.float32)
+    return cfg, st
+
+
 CASES = {
     "cube32": lambda: sphere_case(),
     "box48x32x64_2ch": lambda: sphere_case(48, 32, 64, R=4, C=2, seed=1),
@@ -51,6 +63,7 @@ CASES = {
     "cube32_s075_n3": lambda: sphere_case(distribution_size=0.75, n=3.0),
     "box32x48x32_noise": noise_case,
     "cube32_corner": corner_case,
+    "cube32_8ch_noise": many_channels_case,
 }
 
 
