@@ -92,6 +92,7 @@ SIGNATURES = {
     "flp_batch_destroy": (I, [P]),
     "flp_batch_state_from_seed": (I, [P, I, S]),
     "flp_batch_states_from_seeds": (I, [P, C.POINTER(C.c_char_p), I]),
+    "flp_batch_reconfigure": (I, [P, C.POINTER(C.c_char_p), I]),
     "flp_batch_write_world": (I, [P, I, P, Z]),
     "flp_batch_read_world": (I, [P, I, P, Z, C.POINTER(F), C.POINTER(U64)]),
     "flp_batch_run": (I, [P, U64]),

@@ -20,14 +20,53 @@ from . import _native as nat
 from .propagator import SimulationConfig, _to_json
 
 
+def _load_configs(configs: Sequence[Any]) -> tuple[list[SimulationConfig], list[bytes]]:
+    """Each config as a SimulationConfig and as the JSON text passed to the
+    engine, which parses and validates it.  A dict is serialised once and kept
+    as a shallow copy (the batch reads only its sides and channel count);
+    JSON text or a path is parsed once."""
+    texts = [_to_json(c) for c in configs]
+    cfgs = []
+    for c, t in zip(configs, texts):
+        d = SimulationConfig(c) if isinstance(c, dict) else SimulationConfig(json.loads(t))
+        d.setdefault("depth", 1)
+        cfgs.append(d)
+    return cfgs, [t.encode() for t in texts]
+
+
 class BatchedPropagator:
     def __init__(self, configs: Sequence[Any]):
-        self.configs = [SimulationConfig.load(c) for c in configs]
-        blobs = [json.dumps(c).encode() for c in self.configs]
+        self.configs, blobs = _load_configs(configs)
         arr = (C.c_char_p * len(blobs))(*blobs)
         h = C.c_void_p()
         nat.check(nat.lib().flp_batch_create(arr, len(blobs), C.byref(h)))
         self._h = h
+
+    def reconfigure(self, configs: Sequence[Any]) -> None:
+        """New configs for the same worlds (flp_batch_reconfigure): each world
+        keeps its sides, channel count and kernels' (source, target) channel
+        pairs; growth, ring, radius, flow and dt parameters may change.  The
+        device pools, work queues and step graphs are reused; states are zeroed
+        and clocks reset.  Raises FlpError (INVALID_ARGUMENT) when a world's
+        layout differs, ConfigError for an invalid config; either way the
+        batch is left unchanged."""
+        cfgs, blobs = _load_configs(configs)
+        arr = (C.c_char_p * len(blobs))(*blobs)
+        nat.check(nat.lib().flp_batch_reconfigure(self._h, arr, len(blobs)))
+        self.configs = cfgs
+
+    def layout_matches(self, configs: Sequence[Any]) -> bool:
+        """Whether reconfigure(configs) keeps every world's layout."""
+        if len(configs) != len(self.configs):
+            return False
+        for old, c in zip(self.configs, (c if isinstance(c, dict) else SimulationConfig.load(c) for c in configs)):
+            if (c["width"], c["height"], c.get("depth", 1), c["channels"]) != \
+                    (old["width"], old["height"], old.get("depth", 1), old["channels"]):
+                return False
+            pairs = lambda cfg: [(k.get("source_channel"), k.get("target_channel")) for k in cfg.get("kernels", [])]
+            if pairs(c) != pairs(old):
+                return False
+        return True
 
     def close(self) -> None:
         if getattr(self, "_h", None):

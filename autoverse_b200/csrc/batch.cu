@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "fft_items.cuh"
+#include "host_pool.h"
 #include "flowlenia_cuda.h"
 #include "kernels.h"
 #include "schema.h"
@@ -479,6 +480,7 @@ struct flp_batch {
     size_t cells_total = 0;  // sum of C*N
     int unique_spectra = 0;  // distinct kernel-spectrum sets in the pool
     size_t kh_bytes = 0;
+    size_t kh_cap = 0;       // float2 allocated for KH
     cudaStream_t st = nullptr;
     BWorld* d_worlds = nullptr;
     int2* d_items = nullptr;
@@ -596,9 +598,13 @@ struct flp_batch {
         }
     }
 
-    void free_all() {
+    void drop_graphs() {
         for (auto& g : graph)
-            if (g) cudaGraphExecDestroy(g);
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    void free_all() {
+        drop_graphs();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : pev) cudaEventDestroy(e);
@@ -618,6 +624,46 @@ struct flp_batch {
 
 namespace flp {
 namespace {
+
+// The kernel descriptor of one kernel (growth parameters and stencil radius).
+KDesc make_kdesc(const KernelConfig& kc, int radius) {
+    KDesc k{};
+    k.src = kc.source_channel;
+    k.tgt = kc.target_channel;
+    k.r = radius;
+    k.weight = kc.weight;
+    k.mu = kc.mu;
+    const float sigma_sq_2 = 2.0f * kc.sigma * kc.sigma;
+    k.inv2s2 = 1.0f / sigma_sq_2;
+    return k;
+}
+
+// Kernel spectra depend only on the grid and the stencils: the key of a
+// world's spectrum set.
+std::string kh_key(int W, int H, const std::vector<KernelStencil>& st) {
+    std::string key = std::to_string(W) + "x" + std::to_string(H);
+    for (const KernelStencil& ks : st) {
+        key += "|" + std::to_string(ks.size) + ":";
+        key.append(reinterpret_cast<const char*>(ks.data.data()), ks.data.size() * sizeof(float));
+    }
+    return key;
+}
+
+// The stencils of world w's config, each checked against the grid like
+// pad_kernel (kernel.rs:98-117).
+std::vector<KernelStencil> world_stencils(const SimulationConfig& c, int w) {
+    std::vector<KernelStencil> out;
+    for (const KernelConfig& kc : c.kernels) {
+        out.push_back(build_kernel(kc, c.kernel_radius, 2));
+        if (out.back().radius > c.width || out.back().radius > c.height)
+            throw ConfigError("world " + std::to_string(w) + ": kernel radius " + std::to_string(out.back().radius) +
+                              " exceeds a grid side");
+    }
+    return out;
+}
+
+void batch_spectra(flp_batch* b, const std::vector<std::vector<KernelStencil>>& stencils,
+                   const std::vector<char>& kh_owner);
 
 void batch_create(flp_batch* b, const char* const* jsons, int n) {
     if (n <= 0) throw std::invalid_argument("need at least one world");
@@ -664,17 +710,26 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     std::map<std::string, long long> kh_of;
     std::vector<char> kh_owner(n, 0);
     int cmax = 1;
+    // parsing, the per-world checks and the kernel stencils are independent
+    // per world: host threads
+    std::vector<SimulationConfig> parsed(n);
     std::vector<std::vector<KernelStencil>> stencils(n);
-    for (int w = 0; w < n; ++w) {
+    parallel_for(n, [&](int w) {
         if (!jsons[w]) throw ConfigError("null config for world " + std::to_string(w));
         SimulationConfig c = parse_config(jsons[w]);
         if (c.is_3d()) throw ConfigError("world " + std::to_string(w) + ": the batched engine serves 2D worlds");
+        const int mcls = (c.width % 2 == 0) ? row_class(c.width / 2) : -1;
+        if (mcls < 0 || col_class(c.height) < 0)
+            throw ConfigError("world " + std::to_string(w) + ": batched sides must be even widths with W/2 in {16..256} and H in {32..512} of factors 2 and 3");
+        stencils[w] = world_stencils(c, w);
+        parsed[w] = std::move(c);
+    });
+    for (int w = 0; w < n; ++w) {
+        const SimulationConfig& c = parsed[w];
         BWorld d{};
         d.W = c.width; d.H = c.height; d.C = c.channels; d.K = int(c.kernels.size());
-        d.mcls = (d.W % 2 == 0) ? row_class(d.W / 2) : -1;
+        d.mcls = row_class(d.W / 2);
         d.hcls = col_class(d.H);
-        if (d.mcls < 0 || d.hcls < 0)
-            throw ConfigError("world " + std::to_string(w) + ": batched sides must be even widths with W/2 in {16..256} and H in {32..512} of factors 2 and 3");
         cmax = std::max(cmax, d.C);
         d.offA = offA;
         offA += (long long)d.C * d.W * d.H;
@@ -683,18 +738,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         std::vector<int> my_src;
         for (int k = 0; k < d.K; ++k) {
             const KernelConfig& kc = c.kernels[k];
-            stencils[w].push_back(build_kernel(kc, c.kernel_radius, 2));
-            if (stencils[w].back().radius > d.W || stencils[w].back().radius > d.H)  // pad_kernel's check
-                throw ConfigError("kernel radius " + std::to_string(stencils[w].back().radius) + " exceeds a grid side");
-            KDesc kdsc{};
-            kdsc.src = kc.source_channel;
-            kdsc.tgt = kc.target_channel;
-            kdsc.r = stencils[w].back().radius;
-            kdsc.weight = kc.weight;
-            kdsc.mu = kc.mu;
-            const float sigma_sq_2 = 2.0f * kc.sigma * kc.sigma;
-            kdsc.inv2s2 = 1.0f / sigma_sq_2;
-            kd.push_back(kdsc);
+            kd.push_back(make_kdesc(kc, stencils[w][k].radius));
             auto it = std::find(my_src.begin(), my_src.end(), kc.source_channel);
             int slot;
             if (it == my_src.end()) { slot = int(my_src.size()); my_src.push_back(kc.source_channel); }
@@ -709,11 +753,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         d.offT = offT;
         offT += spec * std::max(d.K, 1);
         {
-            std::string key = std::to_string(d.W) + "x" + std::to_string(d.H);
-            for (const KernelStencil& ks : stencils[w]) {
-                key += "|" + std::to_string(ks.size) + ":";
-                key.append(reinterpret_cast<const char*>(ks.data.data()), ks.data.size() * sizeof(float));
-            }
+            std::string key = kh_key(d.W, d.H, stencils[w]);
             auto it = kh_of.find(key);
             if (it != kh_of.end()) {
                 d.offKH = it->second;
@@ -750,6 +790,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     b->KH = dalloc_b<float2>(size_t(offKH));
     b->unique_spectra = int(kh_of.size());
     b->kh_bytes = size_t(offKH) * sizeof(float2);
+    b->kh_cap = size_t(offKH);
     b->tw = dalloc_b<float2>(tw.size());
     b->d_kd = dalloc_b<KDesc>(kd.size());
     b->d_srcs = dalloc_b<int>(srcs.size());
@@ -778,10 +819,78 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     if (!srcs.empty()) ckb(cudaMemcpy(b->d_srcs, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
     if (!slots.empty()) ckb(cudaMemcpy(b->d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
     ckb(cudaMemcpy(b->d_worlds, b->hw.data(), n * sizeof(BWorld), cudaMemcpyHostToDevice), "copy");
-    // ---- kernel spectra with the single-world FFT passes, one launch pair per
-    // grid size (in chunks): the stencils are wrap-padded on the device and
-    // each world's spectra are copied to its place in the pool; one
-    // synchronisation at the end
+    batch_spectra(b, stencils, kh_owner);
+    // ---- work queues, largest worlds first
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return size_t(b->hw[a].W) * b->hw[a].H > size_t(b->hw[c].W) * b->hw[c].H;
+    });
+    std::vector<int2> items[NQUEUE];
+    for (int w : order) {
+        const BWorld& d = b->hw[w];
+        const int nr = row_nr(d.W / 2), nc = col_nc(d.H), Wc = d.W / 2 + 1;
+        for (int s2 = 0; s2 < d.nsrc; ++s2)
+            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[0 * NCLS + d.mcls].push_back(make_int2(w, (s2 << 16) | g));
+        for (int k = 0; k < d.K; ++k)
+            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (k << 16) | g));
+        for (int c = 0; c < d.C; ++c)
+            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
+        const int fth = d.C <= 4 ? FR_H : FL_H;
+        const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + fth - 1) / fth);
+        for (int t = 0; t < ftiles; ++t) items[flow_queue(d.C)].push_back(make_int2(w, t));
+        const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + gt_h(BATCH_GBY) - 1) / gt_h(BATCH_GBY));
+        for (int c = 0; c < d.C; ++c)
+            for (int t = 0; t < gtiles; ++t) items[QG].push_back(make_int2(w, (c << 16) | t));
+    }
+    std::vector<int2> all;
+    std::vector<int> qoff(NQUEUE + 1, 0);
+    for (int q = 0; q < NQUEUE; ++q) {
+        qoff[q] = int(all.size());
+        all.insert(all.end(), items[q].begin(), items[q].end());
+        b->n_q[q] = int(items[q].size());
+    }
+    qoff[NQUEUE] = int(all.size());
+    b->d_items = dalloc_b<int2>(all.size());
+    b->d_qoff = dalloc_b<int>(qoff.size());
+    if (!all.empty()) ckb(cudaMemcpy(b->d_items, all.data(), all.size() * sizeof(int2), cudaMemcpyHostToDevice), "copy");
+    ckb(cudaMemcpy(b->d_qoff, qoff.data(), qoff.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
+    // ---- persistent grids: one wave of resident CTAs per queue
+    int dev = 0, sms = 0;
+    ckb(cudaGetDevice(&dev), "device");
+    ckb(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
+    for (int q = 0; q < NQUEUE; ++q) {
+        const int stage = q < QF ? q / NCLS : (q < QG ? 3 : 4);
+        const int cls = q % NCLS;
+        switch (stage) {
+            case 0: b->q_fn[q] = r2c_fn(cls); b->q_smem[q] = r2c_smem(cls); break;
+            case 1: b->q_fn[q] = cols_fn(cls); b->q_smem[q] = cols_smem(cls); break;
+            case 2: b->q_fn[q] = c2r_fn(cls); b->q_smem[q] = c2r_smem(cls); break;
+            case 3: {
+                const void* fns[NFLOWQ] = {(const void*)k_batch_flow<0>, (const void*)k_batch_flow<1>,
+                                           (const void*)k_batch_flow<2>, (const void*)k_batch_flow<3>,
+                                           (const void*)k_batch_flow<4>};
+                b->q_fn[q] = fns[q - QF];
+                b->q_smem[q] = q == QF ? flow_smem_bytes_inl(cmax) : 0;
+                break;
+            }
+            default: b->q_fn[q] = (const void*)k_batch_gather; b->q_smem[q] = gather_smem_bytes_inl(BATCH_GBY); break;
+        }
+        if (!b->n_q[q]) continue;
+        int per_sm = 0;
+        ckb(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->q_fn[q], 256, b->q_smem[q]), "occupancy");
+        b->q_grid[q] = std::max(1, std::min(per_sm * sms, b->n_q[q]));
+    }
+    ckb(cudaStreamSynchronize(b->st), "sync");
+}
+
+// Kernel spectra with the single-world FFT passes, one launch pair per grid
+// size (in chunks): the stencils are wrap-padded on the device and each
+// world's spectra are copied to its place in the pool (worlds with kh_owner
+// set own a set; the others share one); one synchronisation at the end.
+void batch_spectra(flp_batch* b, const std::vector<std::vector<KernelStencil>>& stencils,
+                   const std::vector<char>& kh_owner) {
+    const int n = b->n;
     {
         std::map<std::pair<int, int>, std::vector<int>> groups;
         for (int w = 0; w < n; ++w)
@@ -872,68 +981,83 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         ckb(cudaStreamSynchronize(b->st), "sync");
         for (void* q : scratch) cudaFree(q);
     }
-    // ---- work queues, largest worlds first
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-        return size_t(b->hw[a].W) * b->hw[a].H > size_t(b->hw[c].W) * b->hw[c].H;
-    });
-    std::vector<int2> items[NQUEUE];
-    for (int w : order) {
-        const BWorld& d = b->hw[w];
-        const int nr = row_nr(d.W / 2), nc = col_nc(d.H), Wc = d.W / 2 + 1;
-        for (int s2 = 0; s2 < d.nsrc; ++s2)
-            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[0 * NCLS + d.mcls].push_back(make_int2(w, (s2 << 16) | g));
-        for (int k = 0; k < d.K; ++k)
-            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (k << 16) | g));
-        for (int c = 0; c < d.C; ++c)
-            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
-        const int fth = d.C <= 4 ? FR_H : FL_H;
-        const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + fth - 1) / fth);
-        for (int t = 0; t < ftiles; ++t) items[flow_queue(d.C)].push_back(make_int2(w, t));
-        const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + gt_h(BATCH_GBY) - 1) / gt_h(BATCH_GBY));
-        for (int c = 0; c < d.C; ++c)
-            for (int t = 0; t < gtiles; ++t) items[QG].push_back(make_int2(w, (c << 16) | t));
-    }
-    std::vector<int2> all;
-    std::vector<int> qoff(NQUEUE + 1, 0);
-    for (int q = 0; q < NQUEUE; ++q) {
-        qoff[q] = int(all.size());
-        all.insert(all.end(), items[q].begin(), items[q].end());
-        b->n_q[q] = int(items[q].size());
-    }
-    qoff[NQUEUE] = int(all.size());
-    b->d_items = dalloc_b<int2>(all.size());
-    b->d_qoff = dalloc_b<int>(qoff.size());
-    if (!all.empty()) ckb(cudaMemcpy(b->d_items, all.data(), all.size() * sizeof(int2), cudaMemcpyHostToDevice), "copy");
-    ckb(cudaMemcpy(b->d_qoff, qoff.data(), qoff.size() * sizeof(int), cudaMemcpyHostToDevice), "copy");
-    // ---- persistent grids: one wave of resident CTAs per queue
-    int dev = 0, sms = 0;
-    ckb(cudaGetDevice(&dev), "device");
-    ckb(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
-    for (int q = 0; q < NQUEUE; ++q) {
-        const int stage = q < QF ? q / NCLS : (q < QG ? 3 : 4);
-        const int cls = q % NCLS;
-        switch (stage) {
-            case 0: b->q_fn[q] = r2c_fn(cls); b->q_smem[q] = r2c_smem(cls); break;
-            case 1: b->q_fn[q] = cols_fn(cls); b->q_smem[q] = cols_smem(cls); break;
-            case 2: b->q_fn[q] = c2r_fn(cls); b->q_smem[q] = c2r_smem(cls); break;
-            case 3: {
-                const void* fns[NFLOWQ] = {(const void*)k_batch_flow<0>, (const void*)k_batch_flow<1>,
-                                           (const void*)k_batch_flow<2>, (const void*)k_batch_flow<3>,
-                                           (const void*)k_batch_flow<4>};
-                b->q_fn[q] = fns[q - QF];
-                b->q_smem[q] = q == QF ? flow_smem_bytes_inl(cmax) : 0;
-                break;
-            }
-            default: b->q_fn[q] = (const void*)k_batch_gather; b->q_smem[q] = gather_smem_bytes_inl(BATCH_GBY); break;
-        }
-        if (!b->n_q[q]) continue;
-        int per_sm = 0;
-        ckb(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->q_fn[q], 256, b->q_smem[q]), "occupancy");
-        b->q_grid[q] = std::max(1, std::min(per_sm * sms, b->n_q[q]));
-    }
+}
+
+// New configs for the worlds of an existing batch (an evolution engine's next
+// generation).  Every world keeps its sides, channel count and kernels'
+// (source, target) channel pairs, so the pools, the work queues and the
+// captured step graphs stay valid; the kernel descriptors, stencils, flow
+// parameters and kernel spectra are rebuilt, the states zeroed and the clocks
+// reset.  All configs are parsed and checked before anything changes.
+void batch_reconfigure(flp_batch* b, const char* const* jsons, int n) {
+    if (n != b->n)
+        throw std::invalid_argument("reconfigure needs one config per world (" + std::to_string(b->n) + ")");
     ckb(cudaStreamSynchronize(b->st), "sync");
+    std::vector<SimulationConfig> cfgs;
+    cfgs.reserve(n);
+    std::vector<BWorld> hw = b->hw;
+    std::vector<KDesc> kd;
+    std::vector<std::vector<KernelStencil>> stencils(n);
+    std::map<std::string, long long> kh_of;
+    std::vector<char> kh_owner(n, 0);
+    long long offKH = 0;
+    std::vector<SimulationConfig> parsed(n);
+    parallel_for(n, [&](int w) {
+        if (!jsons[w]) throw ConfigError("null config for world " + std::to_string(w));
+        SimulationConfig c = parse_config(jsons[w]);
+        const BWorld& d = hw[w];
+        const SimulationConfig& old = b->cfgs[w];
+        bool same = !c.is_3d() && c.width == d.W && c.height == d.H && c.channels == d.C &&
+                    int(c.kernels.size()) == d.K;
+        for (int k = 0; same && k < d.K; ++k)
+            same = c.kernels[k].source_channel == old.kernels[k].source_channel &&
+                   c.kernels[k].target_channel == old.kernels[k].target_channel;
+        if (!same)
+            throw std::invalid_argument("world " + std::to_string(w) +
+                                        ": a reconfigured world keeps its sides, channels and kernel channel pairs");
+        stencils[w] = world_stencils(c, w);
+        parsed[w] = std::move(c);
+    });
+    for (int w = 0; w < n; ++w) {
+        SimulationConfig& c = parsed[w];
+        BWorld& d = hw[w];
+        for (int k = 0; k < d.K; ++k) kd.push_back(make_kdesc(c.kernels[k], stencils[w][k].radius));
+        const std::string key = kh_key(d.W, d.H, stencils[w]);
+        auto it = kh_of.find(key);
+        if (it != kh_of.end()) {
+            d.offKH = it->second;
+        } else {
+            d.offKH = offKH;
+            kh_of.emplace(key, offKH);
+            kh_owner[w] = 1;
+            offKH += (long long)(d.W / 2 + 1) * d.H * std::max(d.K, 1);
+        }
+        d.fp = flow_params_of(c);
+        cfgs.push_back(std::move(c));
+    }
+    if (size_t(offKH) > b->kh_cap) {
+        // a larger spectrum pool (allocated first, so that a failure leaves
+        // the batch as it was); the captured graphs hold the old pointer
+        float2* kh = dalloc_b<float2>(size_t(offKH));
+        b->drop_graphs();
+        cudaFree(b->KH);
+        b->KH = kh;
+        b->kh_cap = size_t(offKH);
+    }
+    b->hw = std::move(hw);
+    b->cfgs = std::move(cfgs);
+    b->unique_spectra = int(kh_of.size());
+    b->kh_bytes = size_t(offKH) * sizeof(float2);
+    if (!kd.empty()) ckb(cudaMemcpy(b->d_kd, kd.data(), kd.size() * sizeof(KDesc), cudaMemcpyHostToDevice), "copy");
+    ckb(cudaMemcpy(b->d_worlds, b->hw.data(), n * sizeof(BWorld), cudaMemcpyHostToDevice), "copy");
+    const size_t CN = b->cells_total;
+    ckb(cudaMemsetAsync(b->A[0], 0, CN * sizeof(float), b->st), "memset");
+    ckb(cudaMemsetAsync(b->A[1], 0, CN * sizeof(float), b->st), "memset");
+    ckb(cudaMemsetAsync(b->U, 0, CN * sizeof(float), b->st), "memset");
+    ckb(cudaMemsetAsync(b->d_status, 0, sizeof(int), b->st), "memset");
+    batch_spectra(b, stencils, kh_owner);
+    b->time.assign(n, 0.f);
+    b->steps.assign(n, 0);
 }
 
 void batch_build_graph(flp_batch* b) {
@@ -997,6 +1121,12 @@ int flp_batch_create(const char* const* config_jsons, int n_worlds, flp_batch** 
     return FLP_OK;
 }
 
+int flp_batch_reconfigure(flp_batch* b, const char* const* config_jsons, int n_worlds) {
+    BATCH_HANDLE(b);
+    if (!config_jsons) return fail(FLP_ERR_INVALID_ARGUMENT, "null argument");
+    BATCH_TRY(batch_reconfigure(b, config_jsons, n_worlds));
+}
+
 int flp_batch_destroy(flp_batch* b) {
     if (!b) return FLP_OK;
     cudaStreamSynchronize(b->st);
@@ -1041,12 +1171,12 @@ int flp_batch_states_from_seeds(flp_batch* b, const char* const* seed_jsons, int
         // without a seed keep their device state, so copy runs of seeded worlds
         std::vector<float> pool(b->cells_total);
         std::vector<char> seeded(n, 0);
-        for (int w = 0; w < n; ++w) {
-            if (!seed_jsons[w]) continue;
+        parallel_for(n, [&](int w) {  // worlds write disjoint ranges of the pool
+            if (!seed_jsons[w]) return;
             const std::vector<float> g = generate_seed(seed_jsons[w], b->cfgs[w]);
             std::copy(g.begin(), g.end(), pool.begin() + b->hw[w].offA);
             seeded[w] = 1;
-        }
+        });
         for (int w = 0; w < n;) {
             if (!seeded[w]) { ++w; continue; }
             int e = w;

@@ -12,6 +12,10 @@ similarities are reduced there too.  Only a few numbers per world and sample
 cross to the host, where the reference's metric formulas (fitness.rs:243-520)
 combine them.
 
+``PopulationEvaluator`` keeps its batch from one generation to the next: a
+generation with the previous one's world layouts only rebuilds parameters,
+kernel spectra and states on the device (flp_batch_reconfigure).
+
 Configs follow the reference's JSON schema (schema/evolution.rs:273-514):
 fitness = {"metrics": [{"metric": {"type": "Persistence"}, "weight": 1.0}, ...],
 "normalize": true}; evaluation = {"steps": 200, "warmup_steps": 0,
@@ -26,7 +30,10 @@ from typing import Any, Sequence
 
 import numpy as np
 
+from ._native import FlpError
 from .batch import BatchedPropagator
+
+INVALID_ARGUMENT = -2  # FLP_ERR_INVALID_ARGUMENT: the engine refused a world's new layout
 
 DEFAULT_FITNESS = {"metrics": [{"metric": {"type": "Persistence"}, "weight": 1.0},
                                {"metric": {"type": "Compactness"}, "weight": 0.5}], "normalize": True}
@@ -128,6 +135,52 @@ def _concentration(final: np.ndarray) -> float:
     return min(final[MAX] / final[MEAN] / 100.0, 1.0)
 
 
+class PopulationEvaluator:
+    """FitnessEvaluator::evaluate (fitness.rs:26-88) for whole populations,
+    generation after generation, on one BatchedPropagator.  A generation whose
+    candidates keep the previous generation's world layouts (sides, channels,
+    kernels' channel pairs) reuses the batch through reconfigure: its device
+    pools, work queues and step graphs, with only the parameters, kernel
+    spectra and states rebuilt.  Any other generation builds a new batch."""
+
+    def __init__(self, fitness: dict | None = None, evaluation: dict | None = None):
+        self.fitness = fitness or DEFAULT_FITNESS
+        self.evaluation = {**DEFAULT_EVALUATION, **(evaluation or {})}
+        self._batch: BatchedPropagator | None = None
+        self.batches_built = 0
+        self.batches_reused = 0
+
+    def close(self) -> None:
+        if self._batch is not None:
+            self._batch.close()
+            self._batch = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def evaluate(self, configs: Sequence[Any], seeds: Sequence[Any], timings: dict | None = None) -> list[dict]:
+        """Every (config, seed) pair at once; see evaluate_population."""
+        t_start = time.perf_counter()
+        reused = False
+        if self._batch is not None and self._batch.layout_matches(configs):
+            try:
+                self._batch.reconfigure(configs)
+                reused = True
+            except FlpError as e:
+                if e.code != INVALID_ARGUMENT:  # not a layout change: a real error
+                    raise
+        if reused:
+            self.batches_reused += 1
+        else:
+            self.close()
+            self._batch = BatchedPropagator(configs)
+            self.batches_built += 1
+        return _evaluate(self._batch, seeds, self.fitness, self.evaluation, timings, t_start)
+
+
 def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: dict | None = None,
                         evaluation: dict | None = None, timings: dict | None = None) -> list[dict]:
     """FitnessEvaluator::evaluate for every (config, seed) pair at once.
@@ -135,9 +188,12 @@ def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: d
     "behavior": {...}} in the reference's shapes.  `timings`, when given,
     receives the wall-clock seconds of the set-up (batch creation and seeds),
     the simulation with its sampling, and the metric evaluation."""
-    t_start = time.perf_counter()
-    fitness = fitness or DEFAULT_FITNESS
-    evaluation = {**DEFAULT_EVALUATION, **(evaluation or {})}
+    with PopulationEvaluator(fitness, evaluation) as ev:
+        return ev.evaluate(configs, seeds, timings)
+
+
+def _evaluate(b: BatchedPropagator, seeds: Sequence[Any], fitness: dict, evaluation: dict, timings: dict | None,
+              t_start: float) -> list[dict]:
     metrics = fitness.get("metrics", [])
     kinds = [m["metric"]["type"] for m in metrics]
     steps = int(evaluation["steps"])
@@ -145,87 +201,86 @@ def evaluate_population(configs: Sequence[Any], seeds: Sequence[Any], fitness: d
     interval = max(int(evaluation["sample_interval"]), 1)
     sample_steps = [0] + list(range(interval, steps + 1, interval))
     snaps = any(k in ("Periodicity", "OscillatorScore") for k in kinds)
-    with BatchedPropagator(configs) as b:
-        b.load_seeds(list(seeds))
-        n = len(b)
-        if snaps:
-            b.reserve_snapshots(1 + len(sample_steps))
-            b.snapshot(0)  # the initial state's channel sum
-        t_setup = time.perf_counter()
-        init = b.stats()
-        traj = [_Trajectory(c["width"], c["height"], init[i]) for i, c in enumerate(b.configs)]
-        if warm:
-            b.run(warm)
-        done = 0
-        for k, step in enumerate(sample_steps):
-            if step > done:
-                b.run(step - done)
-                done = step
-            st = b.stats()
-            for i in range(n):
-                traj[i].record(st[i], step)
-            if snaps:
-                b.snapshot(1 + k)
-        if done < steps:
-            b.run(steps - done)
-        final = b.stats()
-        t_run = time.perf_counter()
-        sim = {}
-
-        def similarity(sa: int, sb: int) -> np.ndarray:
-            if (sa, sb) not in sim:
-                sim[(sa, sb)] = b.similarity(sa, sb)
-            return sim[(sa, sb)]
-
-        results = []
+    b.load_seeds(list(seeds))
+    n = len(b)
+    if snaps:
+        b.reserve_snapshots(1 + len(sample_steps))
+        b.snapshot(0)  # the initial state's channel sum
+    t_setup = time.perf_counter()
+    init = b.stats()
+    traj = [_Trajectory(c["width"], c["height"], init[i]) for i, c in enumerate(b.configs)]
+    if warm:
+        b.run(warm)
+    done = 0
+    for k, step in enumerate(sample_steps):
+        if step > done:
+            b.run(step - done)
+            done = step
+        st = b.stats()
         for i in range(n):
-            t = traj[i]
-            scores = []
-            for m in metrics:
-                spec = m["metric"]
-                kind = spec["type"]
-                if kind == "Persistence":
-                    v = _persistence(t)
-                elif kind == "Compactness":
-                    v = _compactness(t)
-                elif kind == "Locomotion":
-                    v = _locomotion(t)
-                elif kind == "Periodicity":  # fitness.rs:300-334
-                    v = None
-                    for k, step in enumerate(sample_steps):
-                        if step == int(spec["period"]):
-                            s = similarity(0, 1 + k)[i]
-                            if s > 1.0 - float(spec["tolerance"]):
-                                v = s
-                                break
-                    if v is None:
-                        v = max([0.0] + [similarity(0, 1 + k)[i] for k, s in enumerate(sample_steps) if s > 0])
-                elif kind == "Complexity":
-                    v = _complexity(final[i])
-                elif kind == "MassConcentration":
-                    v = _concentration(final[i])
-                elif kind == "GliderScore":
-                    v = _glider(t, float(spec["min_displacement"]))
-                elif kind == "OscillatorScore":  # fitness.rs:468-495
-                    v = 0.0
-                    maxp, thr = int(spec["max_period"]), float(spec["threshold"])
-                    for a in range(len(sample_steps)):
-                        for c in range(a + 1, len(sample_steps)):
-                            period = sample_steps[c] - sample_steps[a]
-                            if 1 <= period <= maxp:
-                                s = similarity(1 + a, 1 + c)[i]
-                                if s > thr:
-                                    v = max(v, s * (1.0 - period / maxp * 0.5))
-                elif kind == "Stability":
-                    v = _stability(t, final[i])
-                else:  # Custom: scored by the caller
-                    v = 0.0
-                scores.append((kind, float(v), float(m["weight"])))
-            vals = [_clamp(s) if fitness.get("normalize", True) else s for _, s, _ in scores]
-            tw = sum(w for _, _, w in scores)
-            f = sum(v * w for v, (_, _, w) in zip(vals, scores)) / max(tw, 1e-6)
-            results.append({"fitness": float(f), "scores": scores, "behavior": t.behavior()})
-        if timings is not None:
-            t_end = time.perf_counter()
-            timings.update(setup_s=t_setup - t_start, simulate_s=t_run - t_setup, metrics_s=t_end - t_run)
-        return results
+            traj[i].record(st[i], step)
+        if snaps:
+            b.snapshot(1 + k)
+    if done < steps:
+        b.run(steps - done)
+    final = b.stats()
+    t_run = time.perf_counter()
+    sim = {}
+
+    def similarity(sa: int, sb: int) -> np.ndarray:
+        if (sa, sb) not in sim:
+            sim[(sa, sb)] = b.similarity(sa, sb)
+        return sim[(sa, sb)]
+
+    results = []
+    for i in range(n):
+        t = traj[i]
+        scores = []
+        for m in metrics:
+            spec = m["metric"]
+            kind = spec["type"]
+            if kind == "Persistence":
+                v = _persistence(t)
+            elif kind == "Compactness":
+                v = _compactness(t)
+            elif kind == "Locomotion":
+                v = _locomotion(t)
+            elif kind == "Periodicity":  # fitness.rs:300-334
+                v = None
+                for k, step in enumerate(sample_steps):
+                    if step == int(spec["period"]):
+                        s = similarity(0, 1 + k)[i]
+                        if s > 1.0 - float(spec["tolerance"]):
+                            v = s
+                            break
+                if v is None:
+                    v = max([0.0] + [similarity(0, 1 + k)[i] for k, s in enumerate(sample_steps) if s > 0])
+            elif kind == "Complexity":
+                v = _complexity(final[i])
+            elif kind == "MassConcentration":
+                v = _concentration(final[i])
+            elif kind == "GliderScore":
+                v = _glider(t, float(spec["min_displacement"]))
+            elif kind == "OscillatorScore":  # fitness.rs:468-495
+                v = 0.0
+                maxp, thr = int(spec["max_period"]), float(spec["threshold"])
+                for a in range(len(sample_steps)):
+                    for c in range(a + 1, len(sample_steps)):
+                        period = sample_steps[c] - sample_steps[a]
+                        if 1 <= period <= maxp:
+                            s = similarity(1 + a, 1 + c)[i]
+                            if s > thr:
+                                v = max(v, s * (1.0 - period / maxp * 0.5))
+            elif kind == "Stability":
+                v = _stability(t, final[i])
+            else:  # Custom: scored by the caller
+                v = 0.0
+            scores.append((kind, float(v), float(m["weight"])))
+        vals = [_clamp(s) if fitness.get("normalize", True) else s for _, s, _ in scores]
+        tw = sum(w for _, _, w in scores)
+        f = sum(v * w for v, (_, _, w) in zip(vals, scores)) / max(tw, 1e-6)
+        results.append({"fitness": float(f), "scores": scores, "behavior": t.behavior()})
+    if timings is not None:
+        t_end = time.perf_counter()
+        timings.update(setup_s=t_setup - t_start, simulate_s=t_run - t_setup, metrics_s=t_end - t_run)
+    return results

@@ -10,9 +10,13 @@ the engine's benchmark configurations.  All randomness comes from
                         radii and parameters (see batch.py).
 * ``sweep_worlds``    — a growth/flow parameter sweep: worlds of one grid that
                         share their kernel shapes.
+* ``mutated_worlds``  — the next generation of a population: the same world
+                        layouts with new kernel, growth and flow parameters.
 * ``sphere3d``        — 3D, one spherical-shell kernel, Gaussian-sphere seed.
 """
 from __future__ import annotations
+
+import json
 
 import numpy as np
 
@@ -104,6 +108,27 @@ def batched_worlds(n=4096, sides=BATCH_SIDES, seed=DEFAULT_SEED):
         blobs = [{"center": [float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7))],
                   "radius": float(rng.uniform(0.05, 0.15)), "amplitude": 1.0, "channel": c} for c in range(C)]
         out.append((cfg, {"pattern": {"type": "MultiBlob", "blobs": blobs}}))
+    return out
+
+
+def mutated_worlds(worlds, seed=DEFAULT_SEED):
+    """The next generation of an evolution run over `worlds`: the same world
+    layouts (sides, channels, kernels' channel pairs) with new rings (1-2),
+    mu ~ U(0.1,0.3), sigma ~ U(0.01,0.05), weight ~ U(0.3,1), kernel_radius
+    ~ U{8..20}, dt ~ U(0.1,0.3) and beta_a ~ U(0.5,2); seeds unchanged."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for cfg, sd in worlds:
+        c = json.loads(json.dumps(cfg))
+        c["kernel_radius"] = int(rng.integers(8, 21))
+        c["dt"] = float(rng.uniform(0.1, 0.3))
+        c["flow"]["beta_a"] = float(rng.uniform(0.5, 2.0))
+        for k in c["kernels"]:
+            k["rings"] = random_rings(rng, 1, 2)
+            k["mu"] = float(rng.uniform(0.1, 0.3))
+            k["sigma"] = float(rng.uniform(0.01, 0.05))
+            k["weight"] = float(rng.uniform(0.3, 1.0))
+        out.append((c, sd))
     return out
 
 

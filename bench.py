@@ -354,6 +354,18 @@ def measure_fitness(args, dist):
                        "metrics Persistence 1.0 + Compactness 0.5",
            "candidates_per_s": WORLD * len(cfgs) / t, "cell_steps_per_s": WORLD * cells * 200 / t, "seconds": t,
            "mean_fitness": float(np.mean([r["fitness"] for r in res])), "seconds_split": tm}
+    # the next generation of an evolution run (same layouts, mutated kernel,
+    # growth and flow parameters) on the evaluator's batch of the first one
+    nxt = wl.mutated_worlds(pop, wl.DEFAULT_SEED + 24 + RANK)
+    with FT.PopulationEvaluator() as ev:
+        ev.evaluate(cfgs, seeds)
+        t0 = time.perf_counter()
+        tm2 = {}
+        ev.evaluate([c for c, _ in nxt], [s for _, s in nxt], timings=tm2)
+        t2 = reduce_max(dist, time.perf_counter() - t0)
+        reused = ev.batches_reused
+    out["next_generation"] = {"candidates_per_s": WORLD * len(cfgs) / t2, "seconds": t2, "seconds_split": tm2,
+                              "batch_reused": bool(reused)}
     if RANK == 0 and not args.skip_cpu:
         from oracle import fitness_ref as FR
         t0 = time.perf_counter()

@@ -168,6 +168,16 @@ typedef struct flp_batch flp_batch;
 
 FLP_API int flp_batch_create(const char* const* config_jsons, int n_worlds, flp_batch** out);
 FLP_API int flp_batch_destroy(flp_batch* b);
+/* New configs for an existing batch's worlds (the next generation of an
+ * evolution run, evolution/search.rs:152-172, which builds one CpuPropagator
+ * per candidate each generation): n_worlds must be the batch's count and every
+ * world must keep its width, height, channel count and kernels' (source,
+ * target) channel pairs, else FLP_ERR_INVALID_ARGUMENT and nothing changes;
+ * an invalid config gives FLP_ERR_INVALID_CONFIG, also with nothing changed.
+ * Growth and ring parameters, kernel radius, flow parameters and dt may all
+ * change.  States are zeroed and time/step reset; the device pools, work
+ * queues and captured graphs are reused. */
+FLP_API int flp_batch_reconfigure(flp_batch* b, const char* const* config_jsons, int n_worlds);
 /* SimulationState::from_seed for one world (time and step reset to 0). */
 FLP_API int flp_batch_state_from_seed(flp_batch* b, int world, const char* seed_json);
 /* The same for every world at once: seed_jsons[w] (NULL leaves world w as it

@@ -95,3 +95,70 @@ def test_batch_seeds_in_one_call_match_per_world_loads():
         b.load_seeds([seeds[i] if i % 3 == 0 else None for i in range(len(seeds))])
         for i in range(len(worlds)):
             assert np.array_equal(b.read_world(i), a.read_world(i)), i
+
+
+def assert_single_world_bits(b, worlds, steps):
+    for i, (cfg, seed) in enumerate(worlds):
+        with fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT) as p:
+            p.load_seed(seed)
+            p.run_device(steps)
+            assert np.array_equal(b.read_world(i), p.read_state()), i
+
+
+def test_reconfigure_keeps_single_world_bits():
+    """flp_batch_reconfigure (the next generation of an evolution run): new
+    parameters in the same layouts give the single-world engine's bits, with
+    the pools and the step graphs of the first generation reused."""
+    worlds = small_batch(6, seed=7)
+    nxt = wl.mutated_worlds(worlds, 8)
+    with fl.BatchedPropagator([c for c, _ in worlds]) as b:
+        b.load_seeds([s for _, s in worlds])
+        b.run(18)  # the step graphs of the first generation
+        b.reconfigure([c for c, _ in nxt])
+        assert np.all(b.total_mass() == 0.0)  # states zeroed
+        b.load_seeds([s for _, s in nxt])
+        b.run(19)
+        assert_single_world_bits(b, nxt, 19)
+
+
+def test_reconfigure_grows_and_shrinks_the_spectrum_pool():
+    """A sweep (one shared spectrum set) reconfigured to distinct kernels needs
+    a larger pool, which drops the captured graphs; back to shared kernels
+    reuses it."""
+    shared = wl.sweep_worlds(4, side=64, channels=1, R=9, seed=9)
+    distinct = wl.sweep_worlds(4, side=64, channels=1, R=9, seed=10, distinct_kernels=True)
+    with fl.BatchedPropagator([c for c, _ in shared]) as b:
+        assert b.info()["kernel_spectra"] == 1
+        b.load_seeds([s for _, s in shared])
+        b.run(16)
+        b.reconfigure([c for c, _ in distinct])
+        assert b.info()["kernel_spectra"] == 4
+        b.load_seeds([s for _, s in distinct])
+        b.run(17)
+        assert_single_world_bits(b, distinct, 17)
+        b.reconfigure([c for c, _ in shared])
+        assert b.info()["kernel_spectra"] == 1
+        b.load_seeds([s for _, s in shared])
+        b.run(17)
+        assert_single_world_bits(b, shared, 17)
+
+
+def test_reconfigure_refuses_other_layouts_and_bad_configs_unchanged():
+    import json
+    worlds = small_batch(3, seed=11)
+    with fl.BatchedPropagator([c for c, _ in worlds]) as b:
+        wider = json.loads(json.dumps([c for c, _ in worlds]))
+        wider[1]["width"] = 2 * wider[1]["width"]
+        with pytest.raises(fl._native.FlpError) as e:
+            b.reconfigure(wider)
+        assert e.value.code == -2 and "keeps its sides" in str(e.value)
+        bad = json.loads(json.dumps([c for c, _ in worlds]))
+        bad[2]["dt"] = -0.1
+        with pytest.raises(fl._native.ConfigError):
+            b.reconfigure(bad)
+        with pytest.raises(fl._native.FlpError):
+            b.reconfigure([c for c, _ in worlds][:2])
+        # the batch still runs its original worlds
+        b.load_seeds([s for _, s in worlds])
+        b.run(5)
+        assert_single_world_bits(b, worlds, 5)

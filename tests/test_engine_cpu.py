@@ -109,3 +109,25 @@ def test_no_cpu_fallback_without_device():
     cfg, _ = wl.single_blob(32)
     with pytest.raises(fl.FlpError):
         fl.CudaPropagator(cfg)
+
+
+def test_batch_layout_match_rules():
+    """BatchedPropagator.layout_matches: reconfigure keeps sides, channels and
+    the kernels' (source, target) pairs; every other parameter may change."""
+    from autoverse_b200 import workloads as wl
+    from autoverse_b200.batch import BatchedPropagator
+    from autoverse_b200.propagator import SimulationConfig
+    worlds = wl.batched_worlds(4, sides=(64, 96), seed=1)
+    b = BatchedPropagator.__new__(BatchedPropagator)  # layout logic only: no device batch
+    b.configs = [SimulationConfig.load(c) for c, _ in worlds]
+    nxt = wl.mutated_worlds(worlds, 2)
+    assert b.layout_matches([c for c, _ in nxt])
+    assert not b.layout_matches([c for c, _ in nxt][:3])
+    other = [dict(c) for c, _ in nxt]
+    other[0] = dict(other[0], height=other[0]["height"] * 2)
+    assert not b.layout_matches(other)
+    two = next(i for i, (c, _) in enumerate(nxt) if c["channels"] == 2)  # kernels (0,0), (0,1), (1,0), (1,1)
+    swapped = [SimulationConfig.load(c) for c, _ in nxt]
+    ks = swapped[two]["kernels"]
+    ks[0], ks[1] = ks[1], ks[0]
+    assert not b.layout_matches(swapped)

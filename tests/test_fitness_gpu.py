@@ -58,3 +58,19 @@ def test_default_configs_and_statistics_shape():
         b.run(5)
         b.snapshot(1)
         assert np.all(b.similarity(0, 0) > 1 - 1e-12) and np.all(b.similarity(0, 1) <= 1 + 1e-12)
+
+
+def test_evaluator_reuses_its_batch_across_generations():
+    """PopulationEvaluator: a generation with the previous one's layouts is
+    evaluated on the same batch (reconfigured), with the scores of a fresh
+    evaluation; a generation with other layouts builds a new batch."""
+    gen1 = wl.batched_worlds(5, sides=(64, 96), seed=33)
+    gen2 = wl.mutated_worlds(gen1, 34)
+    gen3 = wl.batched_worlds(5, sides=(128,), seed=35)
+    with FT.PopulationEvaluator(ALL_METRICS, EVAL) as ev:
+        for gen in (gen1, gen2, gen3):
+            got = ev.evaluate([c for c, _ in gen], [s for _, s in gen])
+            fresh = FT.evaluate_population([c for c, _ in gen], [s for _, s in gen], ALL_METRICS, EVAL)
+            for g, f in zip(got, fresh):
+                assert g["fitness"] == f["fitness"] and g["scores"] == f["scores"]
+        assert (ev.batches_built, ev.batches_reused) == (2, 1)
