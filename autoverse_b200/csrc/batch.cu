@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -1167,14 +1168,15 @@ int flp_batch_states_from_seeds(flp_batch* b, const char* const* seed_jsons, int
     BATCH_HANDLE(b);
     BATCH_TRY({
         if (!seed_jsons || n != b->n) throw std::invalid_argument("need one seed entry per world");
-        // generate on the host into one staging copy of the state pool; worlds
+        // generate on the host straight into one staging copy of the state pool
+        // (left uninitialised: each seeded world fills its whole range); worlds
         // without a seed keep their device state, so copy runs of seeded worlds
-        std::vector<float> pool(b->cells_total);
+        std::unique_ptr<float[]> staging(new float[std::max<size_t>(b->cells_total, 1)]);
+        float* pool = staging.get();
         std::vector<char> seeded(n, 0);
         parallel_for(n, [&](int w) {  // worlds write disjoint ranges of the pool
             if (!seed_jsons[w]) return;
-            const std::vector<float> g = generate_seed(seed_jsons[w], b->cfgs[w]);
-            std::copy(g.begin(), g.end(), pool.begin() + b->hw[w].offA);
+            generate_seed_into(seed_jsons[w], b->cfgs[w], pool + b->hw[w].offA);
             seeded[w] = 1;
         });
         for (int w = 0; w < n;) {
@@ -1183,7 +1185,7 @@ int flp_batch_states_from_seeds(flp_batch* b, const char* const* seed_jsons, int
             while (e < n && seeded[e]) ++e;
             const long long off = b->hw[w].offA;
             const long long end = e < n ? b->hw[e].offA : (long long)b->cells_total;
-            ckb(cudaMemcpyAsync(b->A[b->cur] + off, pool.data() + off, size_t(end - off) * sizeof(float),
+            ckb(cudaMemcpyAsync(b->A[b->cur] + off, pool + off, size_t(end - off) * sizeof(float),
                                 cudaMemcpyHostToDevice, b->st), "copy");
             w = e;
         }

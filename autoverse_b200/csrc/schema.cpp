@@ -2,6 +2,7 @@
 // kernel construction.  Arithmetic is f32 in the reference's statement order
 // (the translation unit is built with -ffp-contract=off) so that the initial
 // state and the kernel taps are bit-identical to the reference's.
+#include <algorithm>
 #include "schema.h"
 
 #include <cmath>
@@ -280,8 +281,8 @@ namespace {
 
 struct Grid {
     int W, H, D, C;
-    std::vector<float>& g;
-    float* plane(int c) { return g.data() + size_t(c) * W * H * D; }
+    float* g;
+    float* plane(int c) { return g + size_t(c) * W * H * D; }
 };
 
 void gaussian_2d(Grid& G, int channel, float cx, float cy, float radius, float amplitude) {
@@ -354,13 +355,13 @@ float fpair(const Json& a, size_t i) { return a.at(i).f32(); }
 
 }  // namespace
 
-std::vector<float> generate_seed(const std::string& seed_json, const SimulationConfig& cfg) {
+void generate_seed_into(const std::string& seed_json, const SimulationConfig& cfg, float* grid) {
     Json j = parse_json(seed_json);
     const Json& pat = j.at("pattern");
     if (!pat.has("type")) throw ConfigError("seed pattern needs a \"type\" tag");
     const std::string t = pat.at("type").str;
     const int W = cfg.width, H = cfg.height, D = cfg.depth, Cn = cfg.channels;
-    std::vector<float> grid(size_t(Cn) * W * H * D, 0.f);
+    std::fill(grid, grid + size_t(Cn) * W * H * D, 0.f);
     Grid G{W, H, D, Cn, grid};
     const float min_xy = float(std::min(W, H));
     const float min_dim = float(std::min(std::min(W, H), D));
@@ -444,6 +445,11 @@ std::vector<float> generate_seed(const std::string& seed_json, const SimulationC
     } else {
         throw ConfigError("unknown seed pattern type '" + t + "'");
     }
+}
+
+std::vector<float> generate_seed(const std::string& seed_json, const SimulationConfig& cfg) {
+    std::vector<float> grid(size_t(cfg.channels) * cfg.width * cfg.height * cfg.depth);
+    generate_seed_into(seed_json, cfg, grid.data());
     return grid;
 }
 

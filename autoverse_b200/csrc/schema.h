@@ -75,6 +75,8 @@ void validate(const SimulationConfig& c);
 // ----------------------------------------------------------------- seed ----
 // Seed::generate (seed.rs:160-304): returns C planes of depth*height*width.
 std::vector<float> generate_seed(const std::string& seed_json, const SimulationConfig& cfg);
+// The same into out (channels * width * height * depth floats, zero-filled first).
+void generate_seed_into(const std::string& seed_json, const SimulationConfig& cfg, float* out);
 
 // --------------------------------------------------------------- kernel ----
 // Kernel::from_config / Kernel3D::from_config (kernel.rs:32-92,

@@ -344,7 +344,9 @@ def measure_fitness(args, dist):
     from autoverse_b200 import workloads as wl
     pop = wl.batched_worlds(args.fitness_candidates, sides=(64, 96, 128), seed=wl.DEFAULT_SEED + 23 + RANK)
     cfgs, seeds = [c for c, _ in pop], [s for _, s in pop]
-    FT.evaluate_population(cfgs[:8], seeds[:8], evaluation={"steps": 10})  # warm-up
+    # warm-up: 64 candidates cover every size class, so no kernel is first
+    # loaded inside the timed evaluation
+    FT.evaluate_population(cfgs[:64], seeds[:64], evaluation={"steps": 10})
     t0 = time.perf_counter()
     tm = {}
     res = FT.evaluate_population(cfgs, seeds, timings=tm)
