@@ -204,6 +204,12 @@ __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
     }
 }
 
+// Rows per thread of the batched row-walking flow (tile height 8 * that): the
+// persistent kernel is throughput-bound, so a taller walk that reloads fewer
+// halo rows pays, where the single-world kernel wants more, shorter tiles.
+constexpr int BATCH_FR_RPT = 4;
+constexpr int BATCH_FR_H = 8 * BATCH_FR_RPT;
+
 template <int CV>
 __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
     dep_enter();
@@ -215,7 +221,7 @@ __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
         const int2 item = p.items[base + it];
         const BWorld w = p.worlds[item.x];
         const int tiles_x = (w.W + FL_W - 1) / FL_W;
-        const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * (CV ? FR_H : FL_H);
+        const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * (CV ? BATCH_FR_H : FL_H);
         const float* A = p.A + w.offA;
         const float* U = p.U + w.offA;
         float *DX = p.DX + w.offA, *DY = p.DY + w.offA, *MS = p.MS + w.offA;
@@ -223,8 +229,10 @@ __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
             if (w.fp.area_pow2) flow_item<true>(sm, A, U, DX, DY, MS, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
             else flow_item<false>(sm, A, U, DX, DY, MS, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
         } else {
-            if (w.fp.area_pow2) flow_rows_item<CV, true>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
-            else flow_rows_item<CV, false>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+            if (w.fp.area_pow2)
+                flow_rows_item<CV, true, BATCH_FR_RPT>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+            else
+                flow_rows_item<CV, false, BATCH_FR_RPT>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
         }
     }
 }
@@ -837,7 +845,7 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
             for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (k << 16) | g));
         for (int c = 0; c < d.C; ++c)
             for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
-        const int fth = d.C <= 4 ? FR_H : FL_H;
+        const int fth = d.C <= 4 ? BATCH_FR_H : FL_H;
         const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + fth - 1) / fth);
         for (int t = 0; t < ftiles; ++t) items[flow_queue(d.C)].push_back(make_int2(w, t));
         const int gtiles = ((d.W + GT_W - 1) / GT_W) * ((d.H + gt_h(BATCH_GBY) - 1) / gt_h(BATCH_GBY));

@@ -180,16 +180,16 @@ __device__ void flow_item(float* sm, const float* __restrict__ A, const float* _
 
 // ------------------------------------------------- flow_2d, row-walking ----
 // Register-resident variant for C <= 4 (same arithmetic as flow_item): a warp
-// covers 32 columns and each thread walks FR_RPT rows of its column, keeping a
+// covers 32 columns and each thread walks RPT rows of its column, keeping a
 // 3-row window of the channel sum and of every U_c in registers.  Horizontal
 // neighbours come from warp shuffles; the two columns just outside the warp
 // (x0-1 for lane 0, x0+32 for lane 31) from one extra load per row and field.
 // Every lane loads the wrapped column of its position, so partial tiles and
 // grids narrower than a warp see the torus neighbours.
-constexpr int FR_RPT = 2;            // rows per thread
+constexpr int FR_RPT = 2;            // rows per thread of the single-world kernels
 constexpr int FR_H = 8 * FR_RPT;     // tile height: 8 warps of 32 columns
 
-template <int C, bool POW2>
+template <int C, bool POW2, int RPT = FR_RPT>
 __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, const float* __restrict__ U,
                                                float* __restrict__ DX, float* __restrict__ DY,
                                                float* __restrict__ MS, int W, int H, const FlowParams& fp, int x0,
@@ -200,12 +200,12 @@ __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, cons
     const int X = x0 + lane;
     const int xc = wrap_near(X, W);
     const int xh = wrap_near(lane == 0 ? x0 - 1 : x0 + 32, W);
-    const int yb = y0 + FR_RPT * wp;
+    const int yb = y0 + RPT * wp;
     float sw[3][3], uw[C][3][3], ac[C], an[C];
     float dmax = 0.f;
     bool bad = false;
 #pragma unroll
-    for (int r = 0; r < FR_RPT + 2; ++r) {
+    for (int r = 0; r < RPT + 2; ++r) {
         const size_t row = size_t(wrap_near(yb - 1 + r, H)) * W;
         float av[C], ah[C], uv[C], uh[C];
 #pragma unroll
