@@ -118,16 +118,37 @@ __global__ void __launch_bounds__(256) flow_2d(const float* __restrict__ A, cons
     flow_item<POW2>(sm, A, U, DX, DY, MS, C, W, H, fp, blockIdx.x * FL_W, blockIdx.y * FL_H, dmax_slot, status);
 }
 
+// Tile of a gather block: the launch is one wave and a half, and tiles on the
+// torus edges (whose threads take the wrap passes) are the slowest, so the
+// block index enumerates them first: tiles on an x and a y edge, on an x edge
+// only, on a y edge only, then the rest, each category row by row with the
+// channels innermost.  ntx x nty tiles per channel, C channels.
+__device__ __forceinline__ void gather_tile_of(int b, int ntx, int nty, int C, int& tx, int& ty, int& c) {
+    const int ex = min(2, ntx), ix = ntx - ex, ey = min(2, nty), iy = nty - ey;
+    const int ncol[4] = {ex, ex, ix, ix}, nrow[4] = {ey, iy, ey, iy};
+    int k = 0;
+    for (; k < 3; ++k) {
+        const int n = ncol[k] * nrow[k] * C;
+        if (b < n) break;
+        b -= n;
+    }
+    c = b % C;
+    const int t = b / C, col = t % ncol[k], row = t / ncol[k];
+    tx = k < 2 ? (col == 0 ? 0 : ntx - 1) : 1 + col;   // edge columns 0 and ntx-1, interior 1..ntx-2
+    ty = (k == 0 || k == 2) ? (row == 0 ? 0 : nty - 1) : 1 + row;
+}
+
 template <bool POW2>
 __global__ void __launch_bounds__(256, 3) gather_2d(const float* __restrict__ DX, const float* __restrict__ DY,
                                                     const float* __restrict__ MS, float* __restrict__ Anext, int W,
-                                                    int H, FlowParams fp, const int* __restrict__ dmax_slot) {
+                                                    int H, int C, FlowParams fp, const int* __restrict__ dmax_slot) {
     dep_enter();
     extern __shared__ __align__(16) float sm[];
-    const int c = blockIdx.z;
+    int tx, ty, c;
+    gather_tile_of(blockIdx.x, (W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), C, tx, ty, c);
     const size_t N = size_t(W) * H;
     gather_item<POW2, 1>(sm, DX + size_t(c) * N, DY + size_t(c) * N, MS + size_t(c) * N, Anext + size_t(c) * N, W, H,
-                      fp, *dmax_slot, blockIdx.x * GT_W, blockIdx.y * gt_h(1));
+                      fp, *dmax_slot, tx * GT_W, ty * gt_h(1));
 }
 
 template <int C, bool POW2>
@@ -163,11 +184,11 @@ void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float*
 
 void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
                       const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
-    dim3 grid((W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), C);
+    const int tiles = ((W + GT_W - 1) / GT_W) * ((H + gt_h(1) - 1) / gt_h(1)) * C;
     if (fp.area_pow2)
-        launch_dep(gather_2d<true>, grid, 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, fp, dmax_slot);
+        launch_dep(gather_2d<true>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
     else
-        launch_dep(gather_2d<false>, grid, 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, fp, dmax_slot);
+        launch_dep(gather_2d<false>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
 }
 
 void transport_2d_set_attributes() {
