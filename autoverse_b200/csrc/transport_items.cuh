@@ -355,13 +355,18 @@ __device__ __forceinline__ bool gather_column_major(int x0, int W, int RN) {
 // float(X0+i).  Sources are streamed one float4 chunk (4 columns) at a time.
 // CHECK adds the wrap-pass predicate for threads whose source columns wrap the
 // torus.
-template <int RN, bool POW2, bool CHECK, int DM, int GBY>
+// JA..JB (compile time, inside the window's JLO..JHI) restrict the row to a
+// column range, and SHIFTED moves the destinations by xs (a multiple of W) into
+// the frame of wrapped sources: an edge thread's passes over exactly the
+// chunks that hold their columns, without per-column pass tests.
+template <int RN, bool POW2, bool CHECK, int DM, int GBY, int JA = TP - RN, int JB = TP + 3 + RN + 1,
+          bool SHIFTED = false>
 __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, const float* __restrict__ rxmax,
                                            const float* __restrict__ rymin, const float* __restrict__ rymax,
                                            const float* __restrict__ rm, const float (&fy)[GBY + 1],
                                            const float (&fxs)[5], int X0, int gx_base, int W, int cp,
-                                           float total_area, float (&acc)[GBY][4]) {
-    constexpr int JLO = TP - RN, JHI = TP + 3 + RN + 1;
+                                           float total_area, float (&acc)[GBY][4], float xs = 0.f) {
+    constexpr int JLO = JA, JHI = JB;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
         if (4 * q + 3 < JLO || 4 * q > JHI) continue;
@@ -395,7 +400,8 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
             for (int i = 0; i < 4; ++i) {
                 if (j - TP - i < -RN || j - TP - i > RN + 1) continue;
                 // exact: integers below 2^24
-                const float cx0 = CHECK ? fx0 + float(i) : fxs[i], cx1 = CHECK ? fx0 + float(i + 1) : fxs[i + 1];
+                const float cx0 = CHECK ? fx0 + float(i) : (SHIFTED ? fxs[i] + xs : fxs[i]);
+                const float cx1 = CHECK ? fx0 + float(i + 1) : (SHIFTED ? fxs[i + 1] + xs : fxs[i + 1]);
                 const float ox0 = fmaxf(cx0, xa[jj]), ox1 = fminf(cx1, xb[jj]);
                 const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
 #pragma unroll
@@ -436,6 +442,13 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
     const int rp_lo = (Y0 + GBY + RN >= H) ? 0 : 1, rp_hi = (Y0 - RN < 0) ? 2 : 1;
     const int cp_lo = (X0 + 4 + RN >= W) ? 0 : 1, cp_hi = (X0 - RN < 0) ? 2 : 1;
     const bool xin = cp_lo == 1 && cp_hi == 1;
+    // A window that wraps at one side only, with X0 a multiple of 4 and RN <= 3:
+    // at the left edge X0 = 0 (sources j < TP wrap), at the right edge of a width
+    // divisible by 4 X0 = W - 4 (sources j >= 2 TP wrap); other windows take the
+    // generic passes.
+    static_assert(RN <= 3 && TP == 4, "edge column ranges assume RN <= 3 and 4-column chunks");
+    const bool xleft = cp_hi == 2 && cp_lo == 1 && X0 == 0;
+    const bool xright = cp_lo == 0 && cp_hi == 1 && X0 == W - 4 && (W & 3) == 0;
     const int gx_base = x0 - TP + 4 * tx;
     float fxs[5];
 #pragma unroll
@@ -454,6 +467,22 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
         if (xin) {
             gather_row<RN, POW2, false, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
                                                  fy, fxs, X0, gx_base, W, 1, fp.total_area, acc);
+        } else if (GBY == 1 && xleft) {
+            // X0 = 0: columns j >= TP are inside, j < TP wrap to the right edge and come last
+            gather_row<RN, POW2, false, DM, GBY, TP, TP + 3 + RN + 1>(sxmin + off, sxmax + off, symin + off,
+                                                                     symax + off, smass + off, fy, fxs, X0, gx_base,
+                                                                     W, 1, fp.total_area, acc);
+            gather_row<RN, POW2, false, DM, GBY, TP - RN, TP - 1, true>(sxmin + off, sxmax + off, symin + off,
+                                                                       symax + off, smass + off, fy, fxs, X0,
+                                                                       gx_base, W, 2, fp.total_area, acc, float(W));
+        } else if (GBY == 1 && xright) {
+            // X0 = W - 4: columns j >= 2 TP wrap to the left edge and come first, j < 2 TP are inside
+            gather_row<RN, POW2, false, DM, GBY, 2 * TP, TP + 3 + RN + 1, true>(
+                sxmin + off, sxmax + off, symin + off, symax + off, smass + off, fy, fxs, X0, gx_base, W, 0,
+                fp.total_area, acc, -float(W));
+            gather_row<RN, POW2, false, DM, GBY, TP - RN, 2 * TP - 1>(sxmin + off, sxmax + off, symin + off,
+                                                                     symax + off, smass + off, fy, fxs, X0, gx_base,
+                                                                     W, 1, fp.total_area, acc);
         } else {
             for (int cp = cp_lo; cp <= cp_hi; ++cp)
                 gather_row<RN, POW2, true, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
