@@ -467,7 +467,7 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
         if (xin) {
             gather_row<RN, POW2, false, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
                                                  fy, fxs, X0, gx_base, W, 1, fp.total_area, acc);
-        } else if (GBY == 1 && xleft) {
+        } else if (xleft) {
             // X0 = 0: columns j >= TP are inside, j < TP wrap to the right edge and come last
             gather_row<RN, POW2, false, DM, GBY, TP, TP + 3 + RN + 1>(sxmin + off, sxmax + off, symin + off,
                                                                      symax + off, smass + off, fy, fxs, X0, gx_base,
@@ -475,7 +475,7 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
             gather_row<RN, POW2, false, DM, GBY, TP - RN, TP - 1, true>(sxmin + off, sxmax + off, symin + off,
                                                                        symax + off, smass + off, fy, fxs, X0,
                                                                        gx_base, W, 2, fp.total_area, acc, float(W));
-        } else if (GBY == 1 && xright) {
+        } else if (xright) {
             // X0 = W - 4: columns j >= 2 TP wrap to the left edge and come first, j < 2 TP are inside
             gather_row<RN, POW2, false, DM, GBY, 2 * TP, TP + 3 + RN + 1, true>(
                 sxmin + off, sxmax + off, symin + off, symax + off, smass + off, fy, fxs, X0, gx_base, W, 0,
@@ -538,8 +538,11 @@ __device__ __forceinline__ void gather_thread(bool cm, int& tx, int& ty) {
     }
 }
 
+// Out of line: each (RN, POW2, GBY) instantiation gets its own register
+// allocation instead of sharing the calling kernel's with the wider windows
+// (inlined together, the batched gather spilled in its common RN = 1 path).
 template <int RN, bool POW2, int GBY>
-__device__ void gather_body(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
+__device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
                             const float* __restrict__ MS, float* __restrict__ out, int W, int H, const FlowParams& fp,
                             int x0, int y0) {
     constexpr int SRH = gt_h(GBY) + 2 * RN + 1;
