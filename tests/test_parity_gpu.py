@@ -39,7 +39,22 @@ def species_case(W=96, H=64, C=3, R=9, seed=1, patches=6, patch=16, **flow):
     return cfg, st
 
 
+def noise_case(W, H, C=2, seed=11):
+    """Mass in every cell (0.05 + U(0, 0.1)): every gather tile's edge threads,
+    both torus edges and every wrapped window order carry nonzero terms.
+    Widths divisible by 4 take the one-sided edge column ranges, others the
+    generic wrap passes."""
+    cfg, _ = species_case(W=W, H=H, C=C, seed=seed)
+    st = (0.05 + 0.1 * np.random.default_rng(seed).random((C, W * H))).astype(np.float32)
+    return cfg, st
+
+
 TRANSPORT_CASES = {
+    "noise64x48": lambda: noise_case(64, 48),
+    "noise68x40": lambda: noise_case(68, 40, seed=12),
+    "noise70x36": lambda: noise_case(70, 36, seed=13),
+    "noise36x36": lambda: noise_case(36, 36, seed=14),
+    "noise100x52_1ch": lambda: noise_case(100, 52, C=1, seed=15),
     "blob64": lambda: blob_case(),
     "blob_nonsquare": lambda: blob_case(80, R=8, height=48),
     "species96x64": lambda: species_case(),
