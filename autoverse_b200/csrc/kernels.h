@@ -98,7 +98,7 @@ void launch_fft_z(const float2* S, const float2* KH, float2* T, const int* slot_
                   int D, const float2* twD, int mode, float scale, cudaStream_t st);
 
 // 3D transport
-size_t flow3d_smem_bytes(int C);
+size_t flow3d_smem_bytes(int C, int nz);
 int flow3d_max_channels();
 size_t gather3d_smem_bytes();
 void transport_3d_set_attributes();

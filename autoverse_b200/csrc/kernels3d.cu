@@ -15,21 +15,26 @@
 namespace flp {
 
 // ------------------------------------------------------------- flow_3d ----
-// A CTA owns a 32x8 block of columns in F3_NZ consecutive planes and stages
-// the F3_NZ + 2 planes of A, U and the channel sum that their stencils read.
-constexpr int F3_W = 32, F3_H = 8, F3_NZ = 2;
-constexpr int F3_RW = F3_W + 2, F3_RH = F3_H + 2, F3_PL = F3_RW * F3_RH, F3_NP = F3_NZ + 2, F3_RC = F3_NP * F3_PL;
+// A CTA owns a 32x8 block of columns in NZ consecutive planes and stages the
+// NZ + 2 planes of A, U and the channel sum that their stencils read: NZ = 4
+// when those blocks fit one CTA's shared memory (up to 13 channels; fewer
+// halo planes per output plane), else NZ = 2 (up to 20 channels).
+constexpr int F3_W = 32, F3_H = 8;
+constexpr int F3_RW = F3_W + 2, F3_RH = F3_H + 2, F3_PL = F3_RW * F3_RH;
+__host__ __device__ constexpr int f3_rc(int nz) { return (nz + 2) * F3_PL; }  // floats of one staged block
+constexpr size_t F3_SMEM_MAX = 227 * 1024 - 1024;  // a CTA's 227 KB less room for the static arrays
 
-size_t flow3d_smem_bytes(int C) { return sizeof(float) * (size_t(2 * C + 1) * F3_RC); }
+size_t flow3d_smem_bytes(int C, int nz) { return sizeof(float) * (size_t(2 * C + 1) * f3_rc(nz)); }
+static int flow3d_nz(int C) { return flow3d_smem_bytes(C, 4) <= F3_SMEM_MAX ? 4 : 2; }
 // Channels whose staged A and U blocks plus the channel sum fit one CTA's
-// shared memory (227 KB).
-int flow3d_max_channels() { return int((227 * 1024 / (sizeof(float) * F3_RC) - 1) / 2); }
+// shared memory with two planes per CTA.
+int flow3d_max_channels() { return int((F3_SMEM_MAX / (sizeof(float) * f3_rc(2)) - 1) / 2); }
 
 // 3D Sobel of a field at the centre of a 3x3x3 window w[z][y][x] (region
 // indices), gradient3d.rs:106-138: each line sum (a + 2b) + c, each gradient
 // ((l_m + 2 l_0) + l_p) / 32, all in f32 without contraction.
 struct Win3 {
-    const float* p;  // element (dz, dy, dx) at p[dz*F3_PL + dy*F3_RW + dx], dz in 0..F3_NZ+1, dy,dx in 0..2
+    const float* p;  // element (dz, dy, dx) at p[dz*F3_PL + dy*F3_RW + dx], dz in 0..NZ+1, dy,dx in 0..2
     __device__ float at(int z, int y, int x) const { return p[z * F3_PL + y * F3_RW + x]; }
 };
 __device__ __forceinline__ float line3(float a, float b, float c) { return __fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, b)), c); }
@@ -65,12 +70,13 @@ __device__ __forceinline__ void sobel3_run(const Win3& w, float (&gx)[NZ], float
     }
 }
 
-template <bool POW2>
+template <bool POW2, int F3_NZ>
 __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, const float* __restrict__ U,
                                                float* __restrict__ DX, float* __restrict__ DY,
                                                float* __restrict__ DZ, float* __restrict__ MS, int C, int W, int H,
                                                int D, FlowParams fp, int* dmax_slot, int* status) {
     dep_enter();
+    constexpr int F3_NP = F3_NZ + 2, F3_RC = f3_rc(F3_NZ);
     extern __shared__ __align__(16) float sm[];
     float* as = sm;                    // C staged A blocks (F3_NP planes each)
     float* us = sm + C * F3_RC;        // C staged U blocks
@@ -485,11 +491,16 @@ size_t gather3d_smem_bytes() { return gather3d_dyn_smem(); }
 
 void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
                     int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
-    dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, (D + F3_NZ - 1) / F3_NZ);
-    if (fp.area_pow2)
-        launch_dep(flow_3d<true>, grid, 256, flow3d_smem_bytes(C), st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
-    else
-        launch_dep(flow_3d<false>, grid, 256, flow3d_smem_bytes(C), st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+    const int nz = flow3d_nz(C);
+    dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, (D + nz - 1) / nz);
+    const size_t smem = flow3d_smem_bytes(C, nz);
+    if (nz == 4) {
+        if (fp.area_pow2) launch_dep(flow_3d<true, 4>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+        else launch_dep(flow_3d<false, 4>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+    } else {
+        if (fp.area_pow2) launch_dep(flow_3d<true, 2>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+        else launch_dep(flow_3d<false, 2>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
+    }
 }
 
 void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
@@ -506,8 +517,11 @@ void transport_3d_set_attributes() {
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
-    set((const void*)flow_3d<true>, flow3d_smem_bytes(flow3d_max_channels()));
-    set((const void*)flow_3d<false>, flow3d_smem_bytes(flow3d_max_channels()));
+    const int c4 = int((F3_SMEM_MAX / (sizeof(float) * f3_rc(4)) - 1) / 2);  // most channels with four planes
+    set((const void*)flow_3d<true, 4>, flow3d_smem_bytes(c4, 4));
+    set((const void*)flow_3d<false, 4>, flow3d_smem_bytes(c4, 4));
+    set((const void*)flow_3d<true, 2>, flow3d_smem_bytes(flow3d_max_channels(), 2));
+    set((const void*)flow_3d<false, 2>, flow3d_smem_bytes(flow3d_max_channels(), 2));
     set((const void*)gather_3d<true>, gather3d_smem_bytes());
     set((const void*)gather_3d<false>, gather3d_smem_bytes());
 }

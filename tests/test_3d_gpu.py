@@ -47,7 +47,8 @@ def corner_case():
 def many_channels_case(C=8, seed=5):
     """C channels (each with its own kernel and one cross kernel from the
     previous channel) on a 32^3 torus filled with low-amplitude noise: the
-    flow pass stages 2C+1 blocks (about 93 KB of shared memory at C=8)."""
+    flow pass stages 2C+1 blocks (about 136 KB of shared memory at C=8 with
+    four planes per CTA; at C=16 it falls back to two planes, 181 KB)."""
     rng = np.random.default_rng(seed)
     ks = [wl.kernel(c, c, mu=float(rng.uniform(0.1, 0.2)), sigma=0.02) for c in range(C)]
     ks += [wl.kernel(c - 1, c, weight=0.5) for c in range(1, C)]
@@ -64,6 +65,7 @@ CASES = {
     "box32x48x32_noise": noise_case,
     "cube32_corner": corner_case,
     "cube32_8ch_noise": many_channels_case,
+    "cube32_16ch_noise": lambda: many_channels_case(C=16, seed=6),  # two planes per flow CTA (above 13 channels)
 }
 
 
