@@ -63,6 +63,7 @@ SIGNATURES = {
     "flp_run": (I, [P, U64]),
     "flp_step_host": (I, [P, P, Z, C.POINTER(F), C.POINTER(U64), U64]),
     "flp_synchronize": (I, [P]),
+    "flp_synchronize_for": (I, [P, C.c_double]),
     "flp_total_mass": (I, [P, C.POINTER(C.c_double)]),
     "flp_total_mass_f32": (I, [P, C.POINTER(F)]),
     "flp_get_info": (I, [P, C.POINTER(Info)]),
@@ -97,6 +98,7 @@ SIGNATURES = {
     "flp_batch_read_world": (I, [P, I, P, Z, C.POINTER(F), C.POINTER(U64)]),
     "flp_batch_run": (I, [P, U64]),
     "flp_batch_synchronize": (I, [P]),
+    "flp_batch_synchronize_for": (I, [P, C.c_double]),
     "flp_batch_total_mass": (I, [P, P, I]),
     "flp_batch_info": (I, [P, C.POINTER(I), C.POINTER(Z), C.POINTER(Z)]),
     "flp_batch_stream": (P, [P]),
@@ -119,6 +121,8 @@ SIGNATURES = {
     "flp_rec_run": (I, [P, U64]),
     "flp_rec_frames_written": (I, [P, C.POINTER(U64)]),
     "flp_rec_finalize": (I, [P, C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]),
+    "flp_debug_fail_device_alloc": (I, [C.c_int64]),
+    "flp_debug_live_device_allocs": (I, [C.POINTER(C.c_int64)]),
 }
 
 

@@ -115,8 +115,11 @@ class BatchedPropagator:
     def run(self, steps: int) -> None:
         nat.check(nat.lib().flp_batch_run(self._h, C.c_uint64(int(steps))))
 
-    def synchronize(self) -> None:
-        nat.check(nat.lib().flp_batch_synchronize(self._h))
+    def synchronize(self, timeout_ms: float | None = None) -> None:
+        if timeout_ms is None:
+            nat.check(nat.lib().flp_batch_synchronize(self._h))
+        else:
+            nat.check(nat.lib().flp_batch_synchronize_for(self._h, float(timeout_ms)))
 
     def total_mass(self) -> np.ndarray:
         out = np.empty(len(self), dtype=np.float64)

@@ -27,6 +27,7 @@
 #include <string>
 #include <vector>
 
+#include "device_mem.h"
 #include "adjoint.h"
 #include "flowlenia_cuda.h"
 #include "kernels.h"
@@ -53,7 +54,7 @@ void ck(cudaError_t e, const char* what) {
 template <class T>
 T* dalloc_a(size_t n) {
     void* p = nullptr;
-    CKA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    CKA(flp::dmalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
     return static_cast<T*>(p);
 }
 
@@ -137,9 +138,9 @@ struct flp_adjoint {
                         CB, MBAR, FXB, FYB, GUX, GUY, UBAR, GSX, GSY, SBL, G[0], G[1], state0, fin, work[0], work[1],
                         pg};
         for (void* p : ptrs)
-            if (p) cudaFree(p);
-        for (float* p : ckpt) cudaFree(p);
-        for (float* p : seg) cudaFree(p);
+            if (p) flp::dfree(p);
+        for (float* p : ckpt) flp::dfree(p);
+        for (float* p : seg) flp::dfree(p);
         ckpt.clear();
         seg.clear();
         for (cudaEvent_t e : {e0, e1, e2, e3})

@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "device_mem.h"
 #include "fft_items.cuh"
 #include "host_pool.h"
 #include "flowlenia_cuda.h"
@@ -293,14 +294,11 @@ __global__ void __launch_bounds__(256) k_batch_mass(const BWorld* worlds, const 
 template <class T>
 T* dalloc_b(size_t n) {
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(T));
-    if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    throw_cuda(flp::dmalloc(&p, (n ? n : 1) * sizeof(T)), "cudaMalloc");
     return static_cast<T*>(p);
 }
 
-void ckb(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
+void ckb(cudaError_t e, const char* what) { throw_cuda(e, what); }
 
 std::once_flag g_battr_once;
 
@@ -626,7 +624,7 @@ struct flp_batch {
         void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, MS, S, T,
                         KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf, d_stats, d_celloff, d_snaps};
         for (void* q : ptrs)
-            if (q) cudaFree(q);
+            if (q) flp::dfree(q);
         if (st) cudaStreamDestroy(st);
     }
 };
@@ -904,7 +902,7 @@ void batch_spectra(flp_batch* b, const std::vector<std::vector<KernelStencil>>& 
         std::map<std::pair<int, int>, std::vector<int>> groups;
         for (int w = 0; w < n; ++w)
             if (b->hw[w].K > 0 && kh_owner[w]) groups[{b->hw[w].W, b->hw[w].H}].push_back(w);
-        std::vector<void*> scratch;
+        DevScratch scratch;
         // one scratch region for every size and chunk, reused in stream order:
         // padded planes, their row spectra and their full spectra
         size_t cap_pad = 0, cap_spec = 0;
@@ -921,10 +919,9 @@ void batch_spectra(flp_batch* b, const std::vector<std::vector<KernelStencil>>& 
             cap_pad = std::max(cap_pad, cap * plane);
             cap_spec = std::max(cap_spec, cap * spec);
         }
-        float* d_pad = groups.empty() ? nullptr : dalloc_b<float>(cap_pad);
-        float2* d_tmp = groups.empty() ? nullptr : dalloc_b<float2>(cap_spec);
-        float2* d_out = groups.empty() ? nullptr : dalloc_b<float2>(cap_spec);
-        scratch.insert(scratch.end(), {d_pad, d_tmp, d_out});
+        float* d_pad = groups.empty() ? nullptr : scratch.add(dalloc_b<float>(cap_pad));
+        float2* d_tmp = groups.empty() ? nullptr : scratch.add(dalloc_b<float2>(cap_spec));
+        float2* d_out = groups.empty() ? nullptr : scratch.add(dalloc_b<float2>(cap_spec));
         for (const auto& gr : groups) {
             const int W = gr.first.first, H = gr.first.second;
             const size_t plane = size_t(W) * H, spec = size_t(W / 2 + 1) * H;
@@ -963,9 +960,8 @@ void batch_spectra(flp_batch* b, const std::vector<std::vector<KernelStencil>>& 
                                         b->st), "copy");
                     ckb(cudaStreamSynchronize(b->st), "sync");  // the host buffer goes out of scope
                 } else {
-                    float* d_taps = dalloc_b<float>(taps.size());
-                    int4* d_desc = dalloc_b<int4>(desc.size());
-                    scratch.insert(scratch.end(), {d_taps, d_desc});
+                    float* d_taps = scratch.add(dalloc_b<float>(taps.size()));
+                    int4* d_desc = scratch.add(dalloc_b<int4>(desc.size()));
                     ckb(cudaMemcpyAsync(d_taps, taps.data(), taps.size() * sizeof(float), cudaMemcpyHostToDevice, b->st),
                         "copy");
                     ckb(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, b->st),
@@ -988,7 +984,6 @@ void batch_spectra(flp_batch* b, const std::vector<std::vector<KernelStencil>>& 
             }
         }
         ckb(cudaStreamSynchronize(b->st), "sync");
-        for (void* q : scratch) cudaFree(q);
     }
 }
 
@@ -1049,7 +1044,7 @@ void batch_reconfigure(flp_batch* b, const char* const* jsons, int n) {
         // the batch as it was); the captured graphs hold the old pointer
         float2* kh = dalloc_b<float2>(size_t(offKH));
         b->drop_graphs();
-        cudaFree(b->KH);
+        flp::dfree(b->KH);
         b->KH = kh;
         b->kh_cap = size_t(offKH);
     }
@@ -1106,6 +1101,10 @@ int fail(int code, const std::string& msg) {
         return flp::fail(FLP_ERR_INVALID_CONFIG, e.what());      \
     } catch (const std::invalid_argument& e) {                   \
         return flp::fail(FLP_ERR_INVALID_ARGUMENT, e.what());    \
+    } catch (const flp::DeviceOom& e) {                          \
+        return flp::fail(FLP_ERR_OOM, e.what());                 \
+    } catch (const std::bad_alloc&) {                            \
+        return flp::fail(FLP_ERR_OOM, "host allocation failed"); \
     } catch (const std::exception& e) {                          \
         return flp::fail(FLP_ERR_CUDA, e.what());                \
     }
@@ -1252,6 +1251,17 @@ int flp_batch_synchronize(flp_batch* b) {
     })
 }
 
+int flp_batch_synchronize_for(flp_batch* b, double timeout_ms) {
+    BATCH_HANDLE(b);
+    try {
+        if (!wait_stream_for(b->st, timeout_ms))
+            return fail(FLP_ERR_TIMEOUT, "the batch's stream did not finish within " + std::to_string(timeout_ms) + " ms");
+    } catch (const std::exception& e) {
+        return fail(FLP_ERR_CUDA, e.what());
+    }
+    return flp_batch_synchronize(b);
+}
+
 int flp_batch_total_mass(flp_batch* b, double* per_world, int n) {
     BATCH_HANDLE(b);
     BATCH_TRY({
@@ -1281,7 +1291,7 @@ int flp_batch_reserve_snapshots(flp_batch* b, int n_slots) {
         if (n_slots < 0) throw std::invalid_argument("negative slot count");
         if (n_slots <= b->n_snap) return FLP_OK;
         ckb(cudaStreamSynchronize(b->st), "sync");
-        if (b->d_snaps) cudaFree(b->d_snaps);
+        if (b->d_snaps) flp::dfree(b->d_snaps);
         b->d_snaps = nullptr;
         b->n_snap = 0;
         b->d_snaps = dalloc_b<float>(size_t(n_slots) * b->cells);
@@ -1345,7 +1355,7 @@ int flp_batch_profile_run(flp_batch* b, int steps, int flush_l2, float* stage_ms
             ckb(cudaGetDevice(&dev), "device");
             ckb(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "attr");
             b->flush_bytes = std::max<size_t>(size_t(2) * size_t(l2), size_t(64) << 20);
-            ckb(cudaMalloc(&b->flush_buf, b->flush_bytes), "flush buffer");
+            ckb(flp::dmalloc(&b->flush_buf, b->flush_bytes), "flush buffer");
         }
         // Up to RING steps in flight, each with its own events, so the host
         // enqueues ahead of the device; without stage_ms only whole steps are

@@ -9,7 +9,6 @@ namespace flp {
 // Status word bits written by kernels (never trapped; read by the host).
 enum : int {
     STATUS_NONFINITE = 1,  // a non-finite total mass reached the flow bound
-    STATUS_TIMEOUT = 2,    // a bounded wait gave up
 };
 
 // One convolution kernel (KernelConfig, src/schema/config.rs:54-70) as the

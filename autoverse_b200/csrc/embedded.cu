@@ -40,6 +40,7 @@
 #include <string>
 #include <vector>
 
+#include "device_mem.h"
 #include "common.cuh"
 #include "flowlenia_cuda.h"
 #include "kernels.h"
@@ -66,9 +67,7 @@ struct EKern {
     int n_taps;
 };
 
-void cke(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
+void cke(cudaError_t e, const char* what) { throw_cuda(e, what); }
 
 struct UnsupportedError : std::runtime_error {
     using std::runtime_error::runtime_error;
@@ -613,7 +612,7 @@ struct flp_embedded {
         void* ptrs[] = {A[0], A[1], P[0], P[1], U, DX, DY, MS, d_slots, d_status, d_ek, d_taps, d_partial, d_mass,
                         d_tw, d_S, d_T, d_KH, d_srcs, d_kslot, d_conv};
         for (void* q : ptrs)
-            if (q) cudaFree(q);
+            if (q) flp::dfree(q);
         if (st) cudaStreamDestroy(st);
     }
 };
@@ -624,7 +623,7 @@ namespace {
 template <class T>
 T* ealloc(size_t n) {
     void* p = nullptr;
-    cke(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "allocation");
+    cke(flp::dmalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "allocation");
     return static_cast<T*>(p);
 }
 
@@ -735,16 +734,15 @@ void emb_create(flp_embedded* h, const char* json) {
                 const std::vector<float> pk = pad_kernel(stencils[k], W, H, 1);
                 std::copy(pk.begin(), pk.end(), padded.begin() + size_t(k) * h->N);
             }
-            float* d_pad = ealloc<float>(padded.size());
-            float2* d_tmp = ealloc<float2>(spec * h->K);
+            DevScratch scratch;
+            float* d_pad = scratch.add(ealloc<float>(padded.size()));
+            float2* d_tmp = scratch.add(ealloc<float2>(spec * h->K));
             cke(cudaMemcpy(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
             launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, H, g, nullptr, 0, h->st);
             launch_fft_cols(d_tmp, nullptr, h->d_KH, nullptr, h->K, W, H, g, 1, float(1.0 / (double(W) * double(H))),
                             h->st);
             cke(cudaGetLastError(), "kernel spectra");
             cke(cudaStreamSynchronize(h->st), "sync");
-            cudaFree(d_pad);
-            cudaFree(d_tmp);
             h->use_fft = true;
         }
     }
@@ -780,6 +778,8 @@ int efail(int code, const std::string& msg) {
         return flp::efail(FLP_ERR_INVALID_ARGUMENT, e.what());   \
     } catch (const std::bad_alloc&) {                            \
         return flp::efail(FLP_ERR_OOM, "host allocation failed"); \
+    } catch (const flp::DeviceOom& e) {                          \
+        return flp::efail(FLP_ERR_OOM, e.what());                \
     } catch (const std::exception& e) {                          \
         return flp::efail(FLP_ERR_CUDA, e.what());               \
     }

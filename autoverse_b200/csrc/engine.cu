@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "device_mem.h"
 #include "flowlenia_cuda.h"
 #include "kernels.h"
 #include "schema.h"
@@ -49,7 +50,7 @@ template <class T>
 T* dalloc(size_t n) {
     if (n == 0) n = 1;
     void* p = nullptr;
-    CK(cudaMalloc(&p, n * sizeof(T)));
+    CK(flp::dmalloc(&p, n * sizeof(T)));
     return static_cast<T*>(p);
 }
 
@@ -225,11 +226,11 @@ struct flp_propagator {
         void* ptrs[] = {A[0], A[1], U, d_kd, d_taps, d_dmax, d_DX, d_DY, d_MS, d_DZ, d_status, d_partial, d_mass,
                         d_tw, d_S, d_T, d_KH, d_srcs, d_slot};
         for (void* p : ptrs)
-            if (p) cudaFree(p);
+            if (p) flp::dfree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto e : prof_ev) cudaEventDestroy(e);
-        if (flush_buf) cudaFree(flush_buf);
+        if (flush_buf) flp::dfree(flush_buf);
         if (st) cudaStreamDestroy(st);
     }
 };
@@ -314,15 +315,14 @@ static void setup_fft(flp_propagator* h, const std::vector<KernelStencil>& ks) {
         std::vector<float> p = pad_kernel(ks[k], W, H, 1);
         std::copy(p.begin(), p.end(), padded.begin() + size_t(k) * W * H);
     }
-    float* d_pad = dalloc<float>(padded.size());
-    float2* d_tmp = dalloc<float2>(spec * h->K);
+    DevScratch scratch;
+    float* d_pad = scratch.add(dalloc<float>(padded.size()));
+    float2* d_tmp = scratch.add(dalloc<float2>(spec * h->K));
     CK(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
     launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, H, g, nullptr, 0, h->st);
     launch_fft_cols(d_tmp, nullptr, h->d_KH, nullptr, h->K, W, H, g, 1, float(1.0 / (double(W) * double(H))), h->st);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
-    cudaFree(d_pad);
-    cudaFree(d_tmp);
     h->fft_ok = true;
 }
 
@@ -373,8 +373,9 @@ static void setup_fft3d(flp_propagator* h, const std::vector<KernelStencil>& ks)
             std::vector<float> p = pad_kernel(ks[k], W, H, D);
             std::copy(p.begin(), p.end(), padded.begin() + size_t(k) * W * H * D);
         }
-        float* d_pad = dalloc<float>(padded.size());
-        float2* d_tmp = dalloc<float2>(spec * h->K);
+        DevScratch scratch;
+        float* d_pad = scratch.add(dalloc<float>(padded.size()));
+        float2* d_tmp = scratch.add(dalloc<float2>(spec * h->K));
         CK(cudaMemcpyAsync(d_pad, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
         launch_fft_r2c(d_pad, d_tmp, nullptr, h->K, W, D * H, g, nullptr, 0, h->st);
         launch_fft_lines(d_tmp, nullptr, d_tmp, nullptr, h->K, Wc * D, H, g, 1, 1.f, h->st);
@@ -382,8 +383,6 @@ static void setup_fft3d(flp_propagator* h, const std::vector<KernelStencil>& ks)
                      float(1.0 / (double(W) * double(H) * double(D))), h->st);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(h->st));
-        cudaFree(d_pad);
-        cudaFree(d_tmp);
     }
     h->fft_ok = true;
 }
@@ -637,7 +636,7 @@ static void profile_run(flp_propagator* h, int steps, int flush, float* stage_ms
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
         h->flush_bytes = std::max<size_t>(size_t(2) * size_t(l2), size_t(64) << 20);
-        CK(cudaMalloc(&h->flush_buf, h->flush_bytes));
+        CK(flp::dmalloc(&h->flush_buf, h->flush_bytes));
     }
     std::vector<double> acc(ns, 0.0);
     double total = 0.0;
@@ -682,6 +681,16 @@ static void profile_run(flp_propagator* h, int steps, int flush, float* stage_ms
         for (int i = 0; i < ns; ++i) joined += (i ? "," : "") + nm[i];
         std::strncpy(names, joined.c_str(), names_len - 1);
         names[names_len - 1] = 0;
+    }
+}
+
+// Status words written by the kernels: reported once, then cleared.
+static void check_status(flp_propagator* h) {
+    int status = 0;
+    CK(cudaMemcpy(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) {
+        CK(cudaMemset(h->d_status, 0, sizeof(int)));
+        if (status & STATUS_NONFINITE) throw FlpError(FLP_ERR_NONFINITE, "non-finite mass in the state");
     }
 }
 
@@ -816,13 +825,17 @@ int flp_synchronize(flp_propagator* h) {
     FLP_CHECK_HANDLE(h);
     FLP_TRY({
         CK(cudaStreamSynchronize(h->st));
-        int status = 0;
-        CK(cudaMemcpy(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-        if (status) {
-            CK(cudaMemset(h->d_status, 0, sizeof(int)));
-            if (status & STATUS_NONFINITE) throw FlpError(FLP_ERR_NONFINITE, "non-finite mass in the state");
-            if (status & STATUS_TIMEOUT) throw FlpError(FLP_ERR_TIMEOUT, "a bounded device wait timed out");
-        }
+        check_status(h);
+    })
+}
+
+int flp_synchronize_for(flp_propagator* h, double timeout_ms) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!wait_stream_for(h->st, timeout_ms))
+            throw FlpError(FLP_ERR_TIMEOUT, "the handle's stream did not finish within " +
+                                                std::to_string(timeout_ms) + " ms");
+        check_status(h);
     })
 }
 
@@ -944,21 +957,17 @@ int flp_debug_transport(flp_propagator* h, const float* state, const float* aff,
         if (!state || !aff || !out || n != CN) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "size mismatch");
         // The handle's own scratch planes are reused; the live state is untouched
         // (3D worlds go through the same entry: enqueue_transport dispatches).
-        float* a = dalloc<float>(CN);
-        float* o = dalloc<float>(CN);
-        try {
-            CK(cudaMemcpyAsync(a, state, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
-            CK(cudaMemcpyAsync(h->U, aff, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
-            launch_zero_ints(h->d_dmax, 1, h->st);
-            h->enqueue_transport(a, o);
-            CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(out, o, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
-            CK(cudaStreamSynchronize(h->st));
-        } catch (...) {
-            cudaFree(a); cudaFree(o);
-            throw;
-        }
-        cudaFree(a); cudaFree(o);
+        DevScratch scratch;
+        float* a = scratch.add(dalloc<float>(CN));
+        float* o = scratch.add(dalloc<float>(CN));
+        CK(cudaMemcpyAsync(a, state, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(h->U, aff, CN * sizeof(float), cudaMemcpyHostToDevice, h->st));
+        launch_zero_ints(h->d_dmax, 1, h->st);
+        h->enqueue_transport(a, o);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, o, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        flp::dfree(a); flp::dfree(o);
     })
 }
 

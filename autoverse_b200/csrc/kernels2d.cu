@@ -66,15 +66,21 @@ __global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __rest
             loaded_r = r;
         }
         __syncthreads();
+        // Each stencil row is summed on its own (fused multiply-adds), then the
+        // row sums are added: two chains of 2r+1 roundings instead of one of
+        // (2r+1)^2, which keeps the sum's rounding error near that of an f32 FFT.
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
         for (int dy = 0; dy < side; ++dy) {
             const float* trow = tsm + dy * side;
             const float* base = tile + (ty + dy) * P + tx;
+            float row[4] = {0.f, 0.f, 0.f, 0.f};
             for (int dx = 0; dx < side; ++dx) {
                 const float t = trow[dx];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = fmaf(t, base[(8 * i) * P + dx], acc[i]);
+                for (int i = 0; i < 4; ++i) row[i] = fmaf(t, base[(8 * i) * P + dx], row[i]);
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = __fadd_rn(acc[i], row[i]);
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {

@@ -114,6 +114,8 @@ __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, cons
     __syncthreads();
     const int lx = tid & (F3_W - 1), ly = tid / F3_W;
     const int X = x0 + lx, Y = y0 + ly;
+    // Depths are the z-transform sizes (multiples of 16), so every plane block
+    // is full; the bound only guards the stores.
     const int nz = min(F3_NZ, D - z0);
     float dmax = 0.f;
     bool bad = false;

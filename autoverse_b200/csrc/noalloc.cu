@@ -3,12 +3,12 @@
 // Some callers must not allocate device memory: code that enqueues work from
 // inside another framework's operator or plugin (an inference-engine plugin's
 // enqueue, a compiler runtime's custom call) runs on that framework's stream
-// and memory pool, where a cudaMalloc would synchronise the whole device,
-// cannot be recorded into the caller's CUDA graph, and fragments the pool the
-// framework manages.  For them this file runs the direct convolution + growth
-// kernel (the same kernel flp_debug_affinity launches on the direct path)
-// with its scratch -- the kernel descriptors and the wrap-padded stencil taps
-// -- placed in one file-scope device array instead of cudaMalloc'd buffers.
+// and memory pool, where a cudaMalloc would synchronise the whole device and
+// fragment the pool the framework manages.  For them this file runs the
+// direct convolution + growth kernel (the same kernel flp_debug_affinity
+// launches on the direct path) with its scratch -- the kernel descriptors and
+// the wrap-padded stencil taps -- placed in one file-scope device array
+// instead of cudaMalloc'd buffers.
 //
 // The array is NOALLOC_SCRATCH_BYTES (1 MiB) on every device that loads the
 // library and lives until the process exits.  It is shared by all calls: each

@@ -26,6 +26,7 @@
 #include <thread>
 #include <vector>
 
+#include "device_mem.h"
 #include "flowlenia_cuda.h"
 #include "kernels.h"
 
@@ -39,9 +40,7 @@ constexpr uint32_t FLWA_VERSION = 1;   // format.rs:9
 constexpr size_t FLWA_HEADER = 52;     // format.rs:78-81
 constexpr int REC_SLOTS = 4;           // frames in flight
 
-void ckr(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
+void ckr(cudaError_t e, const char* what) { throw_cuda(e, what); }
 
 struct UnsupportedRec : std::runtime_error {
     using std::runtime_error::runtime_error;
@@ -170,7 +169,7 @@ struct flp_recorder {
         shutdown();
         if (copy) cudaStreamSynchronize(copy);
         for (int i = 0; i < REC_SLOTS; ++i) {
-            if (dslot[i]) cudaFree(dslot[i]);
+            if (dslot[i]) flp::dfree(dslot[i]);
             if (hslot[i]) cudaFreeHost(hslot[i]);
             if (ev_snap[i]) cudaEventDestroy(ev_snap[i]);
             if (ev_host[i]) cudaEventDestroy(ev_host[i]);
@@ -207,7 +206,7 @@ void rec_create(flp_recorder* r, flp_propagator* h, const char* path, int compre
     if (std::fwrite(hdr, 1, FLWA_HEADER, r->f) != FLWA_HEADER) throw std::runtime_error("header write failed");
     ckr(cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking), "stream");
     for (int i = 0; i < REC_SLOTS; ++i) {
-        ckr(cudaMalloc(&r->dslot[i], r->frame_bytes), "frame slot");
+        ckr(flp::dmalloc(&r->dslot[i], r->frame_bytes), "frame slot");
         ckr(cudaMallocHost(&r->hslot[i], r->frame_bytes), "pinned frame slot");
         ckr(cudaEventCreateWithFlags(&r->ev_snap[i], cudaEventDisableTiming), "event");
         ckr(cudaEventCreateWithFlags(&r->ev_host[i], cudaEventDisableTiming), "event");
@@ -254,6 +253,8 @@ int rfail(int code, const std::string& msg) {
         return flp::rfail(FLP_ERR_UNSUPPORTED, e.what());        \
     } catch (const std::invalid_argument& e) {                   \
         return flp::rfail(FLP_ERR_INVALID_ARGUMENT, e.what());   \
+    } catch (const flp::DeviceOom& e) {                          \
+        return flp::rfail(FLP_ERR_OOM, e.what());                \
     } catch (const std::exception& e) {                          \
         return flp::rfail(FLP_ERR_CUDA, e.what());               \
     }

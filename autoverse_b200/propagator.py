@@ -209,8 +209,13 @@ class CudaPropagator:
     def run_device(self, steps: int) -> None:
         nat.check(nat.lib().flp_run(self._h, C.c_uint64(int(steps))))
 
-    def synchronize(self) -> None:
-        nat.check(nat.lib().flp_synchronize(self._h))
+    def synchronize(self, timeout_ms: float | None = None) -> None:
+        """Wait for the handle's stream; with timeout_ms, at most that long
+        (FlpError with code TIMEOUT when work is still pending)."""
+        if timeout_ms is None:
+            nat.check(nat.lib().flp_synchronize(self._h))
+        else:
+            nat.check(nat.lib().flp_synchronize_for(self._h, float(timeout_ms)))
 
     def step_host(self, channels: np.ndarray, steps: int = 1, time: float | None = None,
                   step: int | None = None) -> tuple[float, int]:

@@ -69,7 +69,18 @@ def parse_args():
     return ap.parse_args()
 
 
-def workload(name):
+def seed_state(seed, cfg, engine: bool):
+    """Initial state from a seed: the engine's generator (flp_seed_generate)
+    on the GPU arm, the oracle's restatement on the reference arm; both give
+    the same bits (tests/test_engine_cpu.py)."""
+    if engine:
+        import autoverse_b200 as fl
+        return fl.SimulationState.from_seed(seed, cfg).channels
+    from oracle import oracle as O
+    return O.seed_generate(seed, cfg)
+
+
+def workload(name, engine: bool = True):
     from autoverse_b200 import workloads as wl
     if name == "multispecies512":
         cfg, state = wl.multispecies(512, channels=3, R=15)
@@ -77,16 +88,14 @@ def workload(name):
                             "R=15, dt=0.2, beta_a=1, n=2, s=1, 20 U(0,1) 40x40 patches per channel",
                 "width": 512, "height": 512, "channels": 3, "kernels": 9, "kernel_radius": 15}
     elif name == "sphere128":
-        from oracle import oracle as O
         cfg, seed = wl.sphere3d(128)
-        state = O.seed_generate(seed, cfg)
+        state = seed_state(seed, cfg, engine)
         desc = {"workload": "3D sphere 128^3 torus, 1 channel, 1 spherical-shell kernel (ring 1.0/0.5/0.15), R=10, "
                             "mu=0.15, sigma=0.017, dt=0.2, Gaussian sphere r=0.12",
                 "width": 128, "height": 128, "depth": 128, "channels": 1, "kernels": 1, "kernel_radius": 10}
     else:
-        from oracle import oracle as O
         cfg, seed = wl.single_blob(256)
-        state = O.seed_generate(seed, cfg)
+        state = seed_state(seed, cfg, engine)
         desc = {"workload": "single blob 256x256 torus, 1 channel, 1 kernel (ring 1.0/0.5/0.15), R=13, mu=0.15, "
                             "sigma=0.015, dt=0.2, Gaussian blob r=0.1",
                 "width": 256, "height": 256, "channels": 1, "kernels": 1, "kernel_radius": 13}
@@ -222,6 +231,28 @@ def cpu_reference_run(cfg, state, seconds: float, max_steps: int, warmup: int = 
     return n, dt, threads
 
 
+def cpu_worlds_run(worlds, seconds: float):
+    """The oracle on all host cores over worlds (one world per thread, as the
+    reference's evolution search runs one CpuPropagator per candidate on a
+    rayon pool, search.rs:152-172), on the first worlds of the batch: time-
+    bounded rounds of one step of every sampled world."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    sample = worlds[:4 * threads]
+    props = [O.OraclePropagator(c) for c, _ in sample]
+    states = O.run_many(props, [seed_state(sd, c, False) for c, sd in sample], 1, threads)  # warm-up step
+    t0 = time.perf_counter()
+    rounds = 0
+    while rounds == 0 or time.perf_counter() - t0 < seconds:
+        states = O.run_many(props, states, 1, threads)
+        rounds += 1
+    dt = time.perf_counter() - t0
+    cells = sum(c["width"] * c["height"] for c, _ in sample)
+    return {"value": cells * rounds / dt, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} of the batch's worlds, {rounds} steps each (time-bounded at {seconds:.0f} s), "
+                      "one world per host thread, C restatement of CpuPropagator in f32"}
+
+
 def measure_batched(args, dist):
     """Batched worlds: `--batch-worlds` independent worlds (sides from
     {64..512} per axis, 1-2 channels, K = C*C, radius 8..20, per-world growth
@@ -247,14 +278,33 @@ def measure_batched(args, dist):
     b.synchronize()
     t = reduce_max(dist, prof["step_ms"] / 1e3)
     sprof = b.profile_run(min(args.batch_steps, 50), flush_l2=False, stages=True)
+    stage_ms = {k: v / sprof["steps"] for k, v in sprof["stages"].items()}
+    # per-stage algorithmic bytes: the single-world figures summed over the worlds
+    names = {"r2c": "fft_rows_r2c", "cols": "fft_cols_conv", "c2r": "fft_rows_c2r_growth", "flow": "flow_2d",
+             "gather": "gather_2d"}
+    sbytes = {k: sum(stage_bytes(c, names[k]) for c, _ in worlds) for k in stage_ms if k in names}
+    dom = max(stage_ms, key=stage_ms.get)
+    peak, peak_kind = hbm_peak()
+    step_min = sum(4 * c["width"] * c["height"] * (len({k["source_channel"] for k in c["kernels"]}) +
+                                                   4 * c["channels"]) for c, _ in worlds)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": sbytes[dom] / (stage_ms[dom] * 1e-3) / 1e9, "peak": peak,
+            "unit": "GB/s", "algorithmic_bytes_per_launch": sbytes[dom],
+            "per_stage_gbs": {k: sbytes[k] / (stage_ms[k] * 1e-3) / 1e9 for k in sbytes},
+            "step_minimum_bytes": step_min,
+            "step_minimum_frac": step_min / (1e-3 * t / args.batch_steps) / 1e9 / peak,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6.65 TB/s"}
+    roof["frac"] = roof["achieved"] / peak
     out = {"workload": f"{args.batch_worlds} worlds per GPU (LPT-sharded by step cost), sides {{64..512}} per axis, C in {{1,2}}, K=C*C, R~U{{8..20}}, "
                        "mu~U(0.1,0.3), sigma~U(0.01,0.05), dt~U(0.1,0.3), Gaussian-blob seeds",
            "cells_per_gpu": info["cells"], "cell_channels_per_gpu": info["cell_channels"], "steps": args.batch_steps,
            "value": sum(c["width"] * c["height"] for c, _ in everything) * args.batch_steps / t, "unit": "cell-steps/s",
            "ms_per_step": 1e3 * t / args.batch_steps,
-           "stage_ms_per_step": {k: v / sprof["steps"] for k, v in sprof["stages"].items()},
+           "stage_ms_per_step": stage_ms, "roofline": roof,
            "gpu_launches_per_step": 1 + 3 * 7 + 2, "l2": "working set above L2 (pooled state and spectra)"}
     b.close()
+    if RANK == 0 and not args.skip_cpu:
+        out["cpu_baseline"] = cpu_worlds_run(worlds, args.cpu_seconds)
     # batched vs plain on small uneven worlds
     small = wl.batched_worlds(1024, sides=(64, 96, 128), seed=wl.DEFAULT_SEED + 17)
     b = fl.BatchedPropagator([c for c, _ in small])
@@ -369,14 +419,20 @@ def measure_fitness(args, dist):
     out["next_generation"] = {"candidates_per_s": WORLD * len(cfgs) / t2, "seconds": t2, "seconds_split": tm2,
                               "batch_reused": bool(reused)}
     if RANK == 0 and not args.skip_cpu:
+        import multiprocessing as mp
         from oracle import fitness_ref as FR
-        t0 = time.perf_counter()
-        for c, sd in zip(cfgs[:4], seeds[:4]):
-            FR.evaluate(c, sd, FT.DEFAULT_FITNESS, FT.DEFAULT_EVALUATION)
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"candidates_per_s": 4 / dt, "cores": 1, "kind": "port",
-                               "sample": "4 candidates, one after another (the reference runs candidates in "
-                                         "parallel over a rayon pool, one per core)"}
+        threads = os.cpu_count() or 1
+        n = 2 * threads
+        work = [(c, sd, FT.DEFAULT_FITNESS, FT.DEFAULT_EVALUATION) for c, sd in zip(cfgs[:n], seeds[:n])]
+        # worker processes are spawned (not forked: this process holds a CUDA context)
+        with mp.get_context("spawn").Pool(threads) as pool:
+            pool.starmap(FR.evaluate, work[:threads])  # warm-up: workers import and load the oracle
+            t0 = time.perf_counter()
+            pool.starmap(FR.evaluate, work, chunksize=1)
+            dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"candidates_per_s": n / dt, "cores": threads, "kind": "port",
+                               "sample": f"the first {n} candidates, one per host process on {threads} cores (the "
+                                         "reference evaluates candidates in parallel on a rayon pool)"}
     return out
 
 
@@ -502,7 +558,7 @@ def measure_sweep(args, dist):
 
 def main():
     args = parse_args()
-    cfg, state, desc = workload(args.workload)
+    cfg, state, desc = workload(args.workload, engine=args.impl == "engine")
     W, H, C = cfg["width"], cfg["height"], cfg["channels"]
     cells = W * H * cfg.get("depth", 1)
     metric = "cell-steps/s on 1 B200, batched vs plain at \u22641e-5 err; backward/forward ratio"
@@ -583,6 +639,14 @@ def main():
         e2e_step(s)
     e2e_t = reduce_max(dist, time.perf_counter() - t0)
     e2e_value = WORLD * cells * args.e2e_steps / e2e_t
+    # the same host-state call advancing 10 steps per call (run(&mut state, 10))
+    calls = max(1, args.e2e_steps // 10)
+    p.step_host(pin.array, steps=10)
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        p.step_host(pin.array, steps=10)
+    e2e10_t = reduce_max(dist, time.perf_counter() - t0)
+    e2e10_value = WORLD * cells * 10 * calls / e2e10_t
 
     batched = measure_batched(args, dist) if args.batch_worlds > 0 else None
     adjoint = measure_adjoint(args, dist) if args.adjoint_worlds > 0 else None
@@ -617,6 +681,8 @@ def main():
                      else "fallback 6.65 TB/s", "algorithmic_bytes_per_launch": dom_bytes},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(state.nbytes),
                 "d2h_bytes_per_step": int(state.nbytes), "steps": args.e2e_steps},
+        "e2e_10_steps_per_call": {"value": e2e10_value, "unit": "cell-steps/s", "calls": calls,
+                                  "h2d_bytes_per_call": int(state.nbytes), "d2h_bytes_per_call": int(state.nbytes)},
         "gpu_launches": prof["launches_per_step"] * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,

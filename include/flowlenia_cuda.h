@@ -39,7 +39,7 @@ extern "C" {
 #define FLP_ERR_INVALID_ARGUMENT -2
 #define FLP_ERR_OOM -3
 #define FLP_ERR_CUDA -4
-#define FLP_ERR_TIMEOUT -5   /* a bounded device wait gave up */
+#define FLP_ERR_TIMEOUT -5   /* a bounded host wait (flp_*synchronize_for) ran out */
 #define FLP_ERR_NONFINITE -6 /* NaN/Inf found in the state */
 #define FLP_ERR_UNSUPPORTED -7
 
@@ -102,6 +102,13 @@ FLP_API int flp_step_host(flp_propagator* h, float* state, size_t n, float* time
 /* Wait for the handle's stream; reports device-side status words
  * (FLP_ERR_NONFINITE when the bound check saw a non-finite mass). */
 FLP_API int flp_synchronize(flp_propagator* h);
+
+/* flp_synchronize with a limit: waits at most timeout_ms for the handle's
+ * stream (host-side polling, no device spin) and returns FLP_ERR_TIMEOUT when
+ * work is still pending; nothing is cancelled, so a later synchronize can
+ * still wait for it.  A caller's watchdog for a stalled or overloaded device.
+ * No counterpart in the reference (its step is synchronous). */
+FLP_API int flp_synchronize_for(flp_propagator* h, double timeout_ms);
 
 /* SimulationState::total_mass (src/compute/propagator.rs:80-82) computed on
  * the device as an FP64 compensated (Neumaier) sum over all channels. */
@@ -188,6 +195,8 @@ FLP_API int flp_batch_read_world(flp_batch* b, int world, float* out, size_t n, 
 /* CpuPropagator::run for every world at once; replays a captured CUDA graph. */
 FLP_API int flp_batch_run(flp_batch* b, uint64_t n);
 FLP_API int flp_batch_synchronize(flp_batch* b);
+/* flp_batch_synchronize with a limit, as flp_synchronize_for. */
+FLP_API int flp_batch_synchronize_for(flp_batch* b, double timeout_ms);
 /* FP64 compensated total mass of every world (n = number of worlds). */
 FLP_API int flp_batch_total_mass(flp_batch* b, double* per_world, int n);
 FLP_API int flp_batch_info(flp_batch* b, int* n_worlds, size_t* cell_channels, size_t* cells);
@@ -321,8 +330,8 @@ FLP_API void* flp_emb_stream(flp_embedded* h);
 /* Allocation-free affinity.  No counterpart in the reference: an addition for
  * callers that may not allocate device memory, such as code enqueued from
  * another framework's plugin or custom operator on that framework's stream,
- * where cudaMalloc would synchronise the device, break the caller's graph
- * capture and fragment the framework's memory pool.  Computes the same
+ * where cudaMalloc would synchronise the device and fragment the memory pool
+ * that the framework manages.  Computes the same
  * affinity as the direct path of flp_debug_affinity -- U = sum_k w_k
  * G(K_k * A_src) for a 2D config -- from the caller's device state
  * (channels*N floats) into the caller's device buffer d_affinity
@@ -335,6 +344,18 @@ FLP_API void* flp_emb_stream(flp_embedded* h);
  * capture.  Calls share the array, so calls that overlap on the GPU race and
  * must be serialised by the caller.  Calls no cudaMalloc or cudaFree. */
 FLP_API int flp_affinity_noalloc(const char* config_json, const float* d_state, float* d_affinity, void* stream);
+
+/* ---- Failure injection (tests of the error paths) ----------------------
+ * No counterpart in the reference.  Every device allocation of the library
+ * is counted; after `after` further successful allocations the next one fails
+ * as if the device were out of memory (host side: the driver is not called),
+ * so a test can make each allocation of flp_create, flp_batch_create,
+ * flp_emb_create or flp_adj_create fail in turn and check that the call
+ * returns FLP_ERR_OOM and frees what it had allocated.  after < 0 switches
+ * the injection off (the default).  Process-wide; not for production use. */
+FLP_API int flp_debug_fail_device_alloc(int64_t after);
+/* Device allocations of the library that are currently live. */
+FLP_API int flp_debug_live_device_allocs(int64_t* live);
 
 #ifdef __cplusplus
 }

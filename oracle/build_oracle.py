@@ -1,8 +1,10 @@
 """Build recipe for the CPU oracle (test infrastructure only).
 
-Compiles ``flowlenia_oracle.c`` twice into ``oracle/_build/``:
-``liboracle_f32.so`` (float arithmetic in the reference's statement order) and
-``liboracle_f64.so`` (the FP64 twin).  ``-ffp-contract=off`` keeps gcc from
+Compiles ``flowlenia_oracle.c`` into ``oracle/_build/``:
+``liboracle_f32.so`` (float arithmetic in the reference's statement order),
+``liboracle_f64.so`` (the FP64 twin) and ``liboracle_f64_noskip.so`` (the FP64
+twin without the reintegration's |m| < 1e-10 skip, used only to show where the
+reference's mass drift comes from).  ``-ffp-contract=off`` keeps gcc from
 fusing multiply-adds, matching Rust, which never contracts.
 """
 import os
@@ -12,7 +14,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "flowlenia_oracle.c")
 OUT = os.path.join(HERE, "_build")
-LIBS = {"f32": os.path.join(OUT, "liboracle_f32.so"), "f64": os.path.join(OUT, "liboracle_f64.so")}
+LIBS = {"f32": os.path.join(OUT, "liboracle_f32.so"), "f64": os.path.join(OUT, "liboracle_f64.so"),
+        "f64_noskip": os.path.join(OUT, "liboracle_f64_noskip.so")}
+DEFINES = {"f32": [], "f64": ["-DORC_F64"], "f64_noskip": ["-DORC_F64", "-DORC_MASS_SKIP=0"]}
 
 
 def build(force: bool = False) -> dict:
@@ -22,8 +26,7 @@ def build(force: bool = False) -> dict:
             continue
         cmd = ["gcc", "-O2", "-std=c11", "-D_GNU_SOURCE", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
                "-fPIC", "-shared", "-fvisibility=hidden", SRC, "-o", path, "-lm"]
-        if tag == "f64":
-            cmd.insert(1, "-DORC_F64")
+        cmd[1:1] = DEFINES[tag]
         subprocess.run(cmd, check=True)
     return dict(LIBS)
 

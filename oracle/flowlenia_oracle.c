@@ -56,6 +56,13 @@ typedef float real;
 #define ORC_SYM(name) orc32_##name
 #endif
 
+/* Sources with |m| below this are skipped by the reintegration
+ * (reintegration.rs:74-76, reintegration3d.rs:69-71).  A test-only build sets
+ * it to 0 to show that the reference's mass drift comes from this skip. */
+#ifndef ORC_MASS_SKIP
+#define ORC_MASS_SKIP 1e-10
+#endif
+
 #define EXPORT __attribute__((visibility("default")))
 
 static inline real r_max(real a, real b) { return (a != a) ? b : ((b != b) ? a : (a > b ? a : b)); }
@@ -524,7 +531,7 @@ EXPORT void ORC_SYM(advect2d)(const real* cur, const real* fx, const real* fy, r
         for (int x = 0; x < W; ++x) {
             size_t idx = (size_t)y * W + x;
             real mass = cur[idx];
-            if (R_FABS(mass) < R_LIT(1e-10)) continue;
+            if (R_FABS(mass) < (real)ORC_MASS_SKIP) continue;
             real dest_x = (real)x + dt * fx[idx];
             real dest_y = (real)y + dt * fy[idx];
             distribute_mass_2d(next, mass, dest_x, dest_y, W, H, s);
@@ -580,7 +587,7 @@ EXPORT void ORC_SYM(advect3d)(const real* cur, const real* fx, const real* fy, c
             for (int x = 0; x < W; ++x) {
                 size_t idx = (size_t)z * S + (size_t)y * W + x;
                 real mass = cur[idx];
-                if (R_FABS(mass) < R_LIT(1e-10)) continue;
+                if (R_FABS(mass) < (real)ORC_MASS_SKIP) continue;
                 real dest_x = (real)x + dt * fx[idx];
                 real dest_y = (real)y + dt * fy[idx];
                 real dest_z = (real)z + dt * fz[idx];

@@ -24,8 +24,8 @@ from . import build_oracle
 _LIBS: dict[str, C.CDLL] = {}
 
 
-def _lib(f64: bool) -> C.CDLL:
-    tag = "f64" if f64 else "f32"
+def _lib(f64: bool, tag: str | None = None) -> C.CDLL:
+    tag = tag or ("f64" if f64 else "f32")
     if tag not in _LIBS:
         paths = build_oracle.LIBS
         if not os.path.exists(paths[tag]):
@@ -91,8 +91,8 @@ def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
 
-def _fn(f64: bool, name: str):
-    return getattr(_lib(f64), ("orc64_" if f64 else "orc32_") + name)
+def _fn(f64: bool, name: str, tag: str | None = None):
+    return getattr(_lib(f64, tag), ("orc64_" if f64 else "orc32_") + name)
 
 
 def f32(x: Any) -> float:
@@ -147,9 +147,14 @@ def _pack_kernels(cfg: dict, f64: bool, exact: bool = False):
 class OraclePropagator:
     """CpuPropagator / CpuPropagator3D restated in C (f32, or f64 twin)."""
 
-    def __init__(self, cfg: dict | str, f64: bool = False, exact_params: bool = False):
+    def __init__(self, cfg: dict | str, f64: bool = False, exact_params: bool = False, mass_skip: bool = True):
         """exact_params (f64 only): take the config's numbers as given instead of
-        rounding them to f32 first (finite differences of the FP64 twin)."""
+        rounding them to f32 first (finite differences of the FP64 twin).
+        mass_skip=False (f64 only): the FP64 twin without the reintegration's
+        |m| < 1e-10 skip, to measure the mass that the skip removes."""
+        if not mass_skip and not f64:
+            raise ValueError("the build without the mass skip is FP64 only")
+        self._tag = None if mass_skip else "f64_noskip"
         cfg = normalize_config(cfg)
         validate_config(cfg)
         self.cfg = cfg
@@ -163,14 +168,14 @@ class OraclePropagator:
         self._keep = (kp, rc, ra)
         fl = cfg["flow"]
         num = float if exact else f32
-        self._h = _fn(f64, "prop_new")(self.W, self.H, self.D, self.C, num(cfg["dt"]), cfg["kernel_radius"],
+        self._h = _fn(f64, "prop_new", self._tag)(self.W, self.H, self.D, self.C, num(cfg["dt"]), cfg["kernel_radius"],
                                       len(cfg["kernels"]), _ptr(kp), _ptr(rc), _ptr(ra), num(fl["beta_a"]),
                                       num(fl["n"]), num(fl["distribution_size"]))
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            _fn(self.f64, "prop_free")(h)
+            _fn(self.f64, "prop_free", self._tag)(h)
             self._h = None
 
     def _state(self, state: np.ndarray) -> np.ndarray:
@@ -179,25 +184,25 @@ class OraclePropagator:
 
     def run(self, state: np.ndarray, steps: int = 1, threads: int = 1) -> np.ndarray:
         s = self._state(state)
-        _fn(self.f64, "prop_run")(self._h, _ptr(s), int(steps), int(threads))
+        _fn(self.f64, "prop_run", self._tag)(self._h, _ptr(s), int(steps), int(threads))
         return s
 
     def affinity(self, state: np.ndarray) -> np.ndarray:
         s = self._state(state)
         out = np.zeros_like(s)
-        _fn(self.f64, "prop_affinity")(self._h, _ptr(s), _ptr(out))
+        _fn(self.f64, "prop_affinity", self._tag)(self._h, _ptr(s), _ptr(out))
         return out
 
     def transport(self, state: np.ndarray, aff: np.ndarray) -> np.ndarray:
         s = self._state(state)
         a = self._state(aff)
         out = np.zeros_like(s)
-        _fn(self.f64, "prop_transport")(self._h, _ptr(s), _ptr(a), _ptr(out))
+        _fn(self.f64, "prop_transport", self._tag)(self._h, _ptr(s), _ptr(a), _ptr(out))
         return out
 
     def last_flow(self) -> np.ndarray:
         out = np.zeros((self.C, self.dims, self.N), dtype=_dt(self.f64))
-        _fn(self.f64, "prop_last_flow")(self._h, _ptr(out))
+        _fn(self.f64, "prop_last_flow", self._tag)(self._h, _ptr(out))
         return out
 
 

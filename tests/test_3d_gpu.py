@@ -123,3 +123,13 @@ def test_3d_channel_limit_is_refused():
     cfg["channels"] = 21
     with pytest.raises(fl._native.FlpError, match="at most 20 channels"):
         fl.CudaPropagator(cfg)
+
+
+def test_3d_depth_outside_the_transform_sizes_is_refused():
+    """3D depths are the z-transform sizes 32, 48, 64, 96, 128, 192 and 256,
+    all multiples of 16, so the flow pass's plane blocks (4 or 2 planes) always
+    divide the depth; any other depth (54 here) is refused at creation."""
+    cfg, _ = sphere_case(32, 32, 32, steps_in=0)
+    cfg["depth"] = 54
+    with pytest.raises(fl._native.FlpError, match="D in"):
+        fl.CudaPropagator(cfg)

@@ -11,6 +11,7 @@ import math
 import numpy as np
 import pytest
 
+from autoverse_b200 import workloads as wl
 from oracle import oracle as O
 
 RING = {"amplitude": 1.0, "distance": 0.5, "width": 0.15}
@@ -414,3 +415,21 @@ def test_config_validation():
             O.validate_config(dict(base, **{field: val}))
     with pytest.raises(ValueError):
         O.validate_config(dict(base, kernels=[dict(KCFG, target_channel=3)]))
+
+
+def test_mass_drift_comes_from_rounding_and_the_skip():
+    """Where the reference's mass drift comes from, on a 96x96 blob over 1000
+    steps: the FP64 twin without the |m| < 1e-10 skip of the reintegration
+    (reintegration.rs:74-76) conserves mass to FP64 round-off; with the skip
+    it loses a little (the blob's far tail); the f32 reference loses more,
+    from the rounding of its f32 overlap areas and sums."""
+    cfg, sd = wl.single_blob(96, R=13, blob_radius=0.1)
+    st = O.seed_generate(sd, cfg)
+    m0 = st.astype(np.float64).sum()
+    drift = {}
+    for name, kw in (("noskip", dict(f64=True, mass_skip=False)), ("f64", dict(f64=True)), ("f32", {})):
+        a = O.OraclePropagator(cfg, **kw).run(st.astype(np.float64 if kw else np.float32), 1000)
+        drift[name] = abs(a.astype(np.float64).sum() - m0) / m0
+    assert drift["noskip"] < 1e-13
+    assert drift["f64"] > 1e3 * drift["noskip"]
+    assert drift["f32"] > drift["f64"]
