@@ -68,6 +68,8 @@ SIGNATURES = {
     "flp_total_mass_f32": (I, [P, C.POINTER(F)]),
     "flp_get_info": (I, [P, C.POINTER(Info)]),
     "flp_set_conv_mode": (I, [P, I]),
+    "flp_get_tuning": (I, [P, C.POINTER(C.c_int32), I]),
+    "flp_set_tuning": (I, [P, C.POINTER(C.c_int32), I]),
     "flp_stream": (P, [P]),
     "flp_device_state": (P, [P]),
     "flp_device_info": (I, [C.c_char_p, I, C.POINTER(I), C.POINTER(Z)]),

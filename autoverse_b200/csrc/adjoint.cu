@@ -103,7 +103,7 @@ struct flp_adjoint {
 
     void step(const float* a, float* an) {
         launch_fft_r2c(a, S, srcs, B * nsrc, W, H, g, dmax, B, st);
-        launch_fft_cols(S, KH, T, slot, B * K, W, H, g, 0, 1.f, st);
+        launch_fft_cols_conv(S, KH, T, slot, B * nsrc, B * K, B, W, H, g, st);
         launch_fft_c2r_growth(T, U, kd, B * K, W, H, B * C, g, st);
         launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);
         launch_gather_worlds(DX, DY, MS, an, B, C, W, H, fps, pow2, dmax, st);
@@ -115,7 +115,7 @@ struct flp_adjoint {
         // 1. recompute
         launch_fft_r2c(a, S, srcs, B * nsrc, W, H, g, dmax, B, st);
         launch_fft_cols(S, nullptr, AH, nullptr, B * nsrc, W, H, g, 1, 1.f, st);
-        launch_fft_cols(S, KH, T, slot, B * K, W, H, g, 0, 1.f, st);
+        launch_fft_cols_conv(S, KH, T, slot, B * nsrc, B * K, B, W, H, g, st);
         launch_fft_c2r_raw(T, conv, nullptr, B * K, W, H, 1.f, false, g, st);
         launch_growth_worlds(conv, U, ak, B, K, C, N, st);
         launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);

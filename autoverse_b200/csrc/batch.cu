@@ -26,6 +26,7 @@
 
 #include "device_mem.h"
 #include "fft_items.cuh"
+#include "fft_warp.cuh"
 #include "host_pool.h"
 #include "flowlenia_cuda.h"
 #include "kernels.h"
@@ -38,7 +39,7 @@ extern thread_local std::string g_last_error;
 
 namespace {
 
-constexpr int BATCH_ROW_ELEMS = 2048;  // complex values per CTA in the batched row passes
+constexpr int BATCH_WPC = 8;           // warps per CTA of the batched FFT passes
 constexpr int BATCH_GBY = 2;           // destination rows per thread in the batched gather (64x32 tiles)
 constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
 constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
@@ -57,7 +58,7 @@ int col_class(int H) {
 }
 int row_nr(int M) {
     switch (M) {
-#define X(n) case n: return RowCfg<n, BATCH_ROW_ELEMS>::NR;
+#define X(n) case n: return WRowCfg<n, BATCH_WPC>::NRC;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -65,7 +66,7 @@ int row_nr(int M) {
 }
 int col_nc(int H) {
     switch (H) {
-#define X(n) case n: return ColCfg<n>::NC;
+#define X(n) case n: return WColCfg<n, BATCH_WPC>::NCC;
         FLP_COL_SIZES(X)
 #undef X
     }
@@ -164,7 +165,8 @@ __global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
         const int c = p.srcs[w.offSrc + slot];
         const size_t N = size_t(2 * M) * w.H;
         float2* Sc = p.S + w.offS + size_t(slot) * (M + 1) * w.H;
-        r2c_rows_item<M, BATCH_ROW_ELEMS>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * RowCfg<M, BATCH_ROW_ELEMS>::NR, p.tw + w.twM, p.tw + w.twW);
+        r2c_rows_witem<M, BATCH_WPC>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * WRowCfg<M, BATCH_WPC>::NRC,
+                                     p.tw + w.twM, p.tw + w.twW);
     }
 }
 
@@ -178,13 +180,11 @@ __global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
         if (it < 0) break;
         const int2 item = p.items[base + it];
         const BWorld w = p.worlds[item.x];
-        const int k = item.y >> 16, g = item.y & 0xFFFF;
+        const int slot = item.y >> 16, g = item.y & 0xFFFF;
         const int Wc = w.W / 2 + 1;
-        const int slot = p.slots[w.offKd + k];
-        const int kx0 = g * ColCfg<H>::NC;
-        const int nl = min(ColCfg<H>::NC, Wc - kx0);
-        cols_conv_item<H, true>(fsm, p.S + w.offS + (size_t(slot) * Wc + kx0) * H, p.KH + w.offKH + (size_t(k) * Wc + kx0) * H,
-                          p.T + w.offT + (size_t(k) * Wc + kx0) * H, nl, 0, 1.f, p.tw + w.twH);
+        // one forward transform of the slot's columns for all its kernels
+        cols_witem<H, BATCH_WPC>(fsm, p.S + w.offS + size_t(slot) * Wc * H, p.KH + w.offKH, p.T + w.offT,
+                                 p.slots + w.offKd, 0, w.K, slot, Wc, g * WColCfg<H, BATCH_WPC>::NCC, p.tw + w.twH);
     }
 }
 
@@ -200,8 +200,8 @@ __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
         const BWorld w = p.worlds[item.x];
         const int c = item.y >> 16, g = item.y & 0xFFFF;
         float* Uc = p.U + w.offA + size_t(c) * (2 * M) * w.H;
-        c2r_growth_item<M, BATCH_ROW_ELEMS>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H, g * RowCfg<M, BATCH_ROW_ELEMS>::NR, p.tw + w.twM,
-                           p.tw + w.twW);
+        c2r_growth_witem<M, BATCH_WPC>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H,
+                                       g * WRowCfg<M, BATCH_WPC>::NRC, p.tw + w.twM, p.tw + w.twW);
     }
 }
 
@@ -329,7 +329,7 @@ const void* cols_fn(int cls) {
 }
 size_t r2c_smem(int cls) {
     switch (ROW_SIZES[cls]) {
-#define X(n) case n: return RowCfg<n, BATCH_ROW_ELEMS>::smem_r2c;
+#define X(n) case n: return WRowCfg<n, BATCH_WPC>::smem_r2c;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -337,7 +337,7 @@ size_t r2c_smem(int cls) {
 }
 size_t c2r_smem(int cls) {
     switch (ROW_SIZES[cls]) {
-#define X(n) case n: return RowCfg<n, BATCH_ROW_ELEMS>::smem_c2r;
+#define X(n) case n: return WRowCfg<n, BATCH_WPC>::smem_c2r;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -345,7 +345,7 @@ size_t c2r_smem(int cls) {
 }
 size_t cols_smem(int cls) {
     switch (COL_SIZES[cls]) {
-#define X(n) case n: return ColCfg<n>::smem_prefetch;
+#define X(n) case n: return WColCfg<n, BATCH_WPC>::smem;
         FLP_COL_SIZES(X)
 #undef X
     }
@@ -839,8 +839,8 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         const int nr = row_nr(d.W / 2), nc = col_nc(d.H), Wc = d.W / 2 + 1;
         for (int s2 = 0; s2 < d.nsrc; ++s2)
             for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[0 * NCLS + d.mcls].push_back(make_int2(w, (s2 << 16) | g));
-        for (int k = 0; k < d.K; ++k)
-            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (k << 16) | g));
+        for (int s2 = 0; s2 < d.nsrc; ++s2)
+            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (s2 << 16) | g));
         for (int c = 0; c < d.C; ++c)
             for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
         const int fth = d.C <= 4 ? BATCH_FR_H : FL_H;

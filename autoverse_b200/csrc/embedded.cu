@@ -521,7 +521,7 @@ struct flp_embedded {
         mark(0);
         if (use_fft) {
             launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, nullptr, 0, st);
-            launch_fft_cols(d_S, d_KH, d_T, d_kslot, K, W, H, geom, 0, 1.f, st);
+            launch_fft_cols_conv(d_S, d_KH, d_T, d_kslot, nsrc, K, 1, W, H, geom, st);
             launch_fft_c2r_raw(d_T, d_conv, nullptr, K, W, H, 1.f, false, geom, st);
             launch_dep(emb_growth, dim3(unsigned((N + 255) / 256), C), dim3(256), size_t(0), st, (const float*)d_conv,
                        U, p, (const EKern*)d_ek, K, W, H, d_slots, 1 + C);
@@ -540,7 +540,7 @@ struct flp_embedded {
                        temperature, (const int*)d_slots);
             pcur ^= 1;
         } else {
-            launch_gather_2d(DX, DY, MS, an, C, W, H, fp, d_slots, st);
+            launch_gather_2d(DX, DY, MS, an, C, W, H, fp, d_slots, 1, st);
         }
         mark(3);
         cke(cudaGetLastError(), "embedded step launch");

@@ -84,9 +84,17 @@ static void set_attributes_once() {
     });
 }
 
-// Autotune cache: (W, H, D, C, K, rmax) -> chosen conv mode.
+// Measured launch choices of one world shape, cached per (W, H, D, channels,
+// kernels, largest kernel radius, source channels) for the process.  Every
+// choice gives the same bits: only the time differs.
+struct Tuning {
+    int conv_mode = -1;                                    // FLP_CONV_DIRECT / FLP_CONV_FFT; -1 = not measured
+    int wpc_r2c = 8, wpc_cols = 8, share_cols = 1, wpc_c2r = 8;  // FFT passes (FftGeom)
+    int gather_gby = 1;                                    // destination rows per gather thread (1 or 2)
+    bool fft_tuned = false, gather_tuned = false;
+};
 static std::mutex g_tune_mu;
-static std::map<std::vector<int>, int> g_tune_cache;
+static std::map<std::vector<int>, Tuning> g_tune_cache;
 
 }  // namespace flp
 
@@ -127,6 +135,8 @@ struct flp_propagator {
     int nsrc = 0;
     int conv_mode = FLP_CONV_DIRECT;
     bool conv_pending = true;  // the autotuner runs before the first convolution unless a mode is set first
+    int gather_gby = 1;        // destination rows per gather thread
+    bool tuning_cached = false;  // the last tuning came from the process cache
     float time = 0.f;
     uint64_t step = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -172,7 +182,7 @@ struct flp_propagator {
         } else {
             launch_fft_r2c(a, d_S, d_srcs, nsrc, W, H, geom, reset_slot, 1, st);
             mark(0);
-            launch_fft_cols(d_S, d_KH, d_T, d_slot, K, W, H, geom, 0, 1.f, st);
+            launch_fft_cols_conv(d_S, d_KH, d_T, d_slot, nsrc, K, 1, W, H, geom, st);
             mark(1);
             launch_fft_c2r_growth(d_T, U, d_kd, K, W, H, C, geom, st);
             mark(2);
@@ -200,7 +210,7 @@ struct flp_propagator {
         }
         launch_flow_2d(a, U, d_DX, d_DY, d_MS, C, W, H, fp, d_dmax, d_status, st);
         mark(ns - 2);
-        launch_gather_2d(d_DX, d_DY, d_MS, an, C, W, H, fp, d_dmax, st);
+        launch_gather_2d(d_DX, d_DY, d_MS, an, C, W, H, fp, d_dmax, gather_gby, st);
         mark(ns - 1);
     }
 
@@ -401,33 +411,124 @@ static float time_conv(flp_propagator* h, int mode, int reps) {
     return ms / reps;
 }
 
+// Device time of one full step (from A[cur] into the other buffer, which is
+// scratch until the next step) averaged over reps, after two untimed steps.
+static float time_step(flp_propagator* h, int reps) {
+    const float* a = h->A[h->cur];
+    float* an = h->A[h->cur ^ 1];
+    for (int i = 0; i < 2 + reps; ++i) {
+        if (i == 2) CK(cudaEventRecord(h->ev0, h->st));
+        h->enqueue_conv(a, h->d_dmax);
+        h->enqueue_transport(a, an);
+    }
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    return ms / reps;
+}
+
+static void apply_tuning(flp_propagator* h, const Tuning& t) {
+    h->geom.wpc_r2c = t.wpc_r2c;
+    h->geom.wpc_cols = t.wpc_cols;
+    h->geom.share_cols = t.share_cols;
+    h->geom.wpc_c2r = t.wpc_c2r;
+    h->gather_gby = t.gather_gby;
+}
+
+// Each FFT pass's CTA shape (warps per CTA; for the columns also one forward
+// transform per source or per kernel), one pass at a time from the defaults,
+// each candidate timed over 20 whole convolutions.
+static void tune_fft_passes(flp_propagator* h, Tuning& t) {
+    const int reps = 20;
+    auto timed = [&](const Tuning& c) {
+        apply_tuning(h, c);
+        return time_conv(h, FLP_CONV_FFT, reps);
+    };
+    float best = timed(t);
+    for (int w : {4}) {
+        Tuning c = t;
+        c.wpc_r2c = w;
+        const float ms = timed(c);
+        if (ms < best) { best = ms; t = c; }
+    }
+    for (int share : {1, 0})
+        for (int w : {8, 4}) {
+            if (share == t.share_cols && w == t.wpc_cols) continue;
+            Tuning c = t;
+            c.share_cols = share;
+            c.wpc_cols = w;
+            const float ms = timed(c);
+            if (ms < best) { best = ms; t = c; }
+        }
+    {
+        Tuning c = t;
+        c.wpc_c2r = 4;
+        const float ms = timed(c);
+        if (ms < best) { best = ms; t = c; }
+    }
+    apply_tuning(h, t);
+}
+
+// Destination rows per gather thread, timed over whole steps.
+static void tune_gather(flp_propagator* h, Tuning& t) {
+    float best = 0.f;
+    int pick = 1;
+    for (int gby : {1, 2}) {
+        h->gather_gby = gby;
+        const float ms = time_step(h, 10);
+        if (gby == 1 || ms < best) { best = ms; pick = gby; }
+    }
+    t.gather_gby = pick;
+    h->gather_gby = pick;
+}
+
 static void resolve_conv_mode(flp_propagator* h, int requested) {
     if (h->K == 0) { h->conv_mode = FLP_CONV_DIRECT; return; }
-    if (requested == FLP_CONV_DIRECT) {
-        if (!h->direct_ok) throw FlpError(FLP_ERR_UNSUPPORTED, "direct convolution supports radius <= 24");
-        h->conv_mode = FLP_CONV_DIRECT;
-        return;
-    }
-    if (requested == FLP_CONV_FFT) {
-        if (!h->fft_ok) throw FlpError(FLP_ERR_UNSUPPORTED, "FFT path needs an even width and sides of factors 2,3,5");
-        h->conv_mode = FLP_CONV_FFT;
-        return;
-    }
+    if (requested == FLP_CONV_DIRECT && !h->direct_ok)
+        throw FlpError(FLP_ERR_UNSUPPORTED, "direct convolution supports radius <= 24");
+    if (requested == FLP_CONV_FFT && !h->fft_ok)
+        throw FlpError(FLP_ERR_UNSUPPORTED, "FFT path needs an even width and sides of factors 2,3,5");
     if (!h->fft_ok && !h->direct_ok)
         throw FlpError(FLP_ERR_UNSUPPORTED, "no convolution path for this grid/radius");
-    if (!h->fft_ok) { h->conv_mode = FLP_CONV_DIRECT; return; }
-    if (!h->direct_ok) { h->conv_mode = FLP_CONV_FFT; return; }
-    std::vector<int> key = {h->W, h->H, h->D, h->C, h->K, h->rmax, h->nsrc};
+    const std::vector<int> key = {h->W, h->H, h->D, h->C, h->K, h->rmax, h->nsrc};
+    Tuning t;
+    bool cached = false;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
-        if (it != g_tune_cache.end()) { h->conv_mode = it->second; return; }
+        if (it != g_tune_cache.end()) {
+            t = it->second;
+            cached = true;
+        }
     }
-    float t_direct = time_conv(h, FLP_CONV_DIRECT, 5);
-    float t_fft = time_conv(h, FLP_CONV_FFT, 5);
-    h->conv_mode = t_fft < t_direct ? FLP_CONV_FFT : FLP_CONV_DIRECT;
+    bool measured = false;
+    int mode;
+    if (requested == FLP_CONV_DIRECT || requested == FLP_CONV_FFT) mode = requested;
+    else if (!h->fft_ok) mode = FLP_CONV_DIRECT;
+    else if (!h->direct_ok) mode = FLP_CONV_FFT;
+    else if (t.conv_mode >= 0) mode = t.conv_mode;
+    else {
+        apply_tuning(h, t);
+        const float t_direct = time_conv(h, FLP_CONV_DIRECT, 5);
+        const float t_fft = time_conv(h, FLP_CONV_FFT, 5);
+        mode = t.conv_mode = t_fft < t_direct ? FLP_CONV_FFT : FLP_CONV_DIRECT;
+        measured = true;
+    }
+    h->conv_mode = mode;
+    apply_tuning(h, t);
+    if (h->dims == 2 && mode == FLP_CONV_FFT && !t.fft_tuned && fft_row_templated(h->W / 2) &&
+        fft_col_templated(h->H)) {
+        tune_fft_passes(h, t);
+        t.fft_tuned = measured = true;
+    }
+    if (h->dims == 2 && !t.gather_tuned) {
+        tune_gather(h, t);
+        t.gather_tuned = measured = true;
+    }
+    h->tuning_cached = cached && !measured;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = h->conv_mode;
+    g_tune_cache[key] = t;
 }
 
 PropView prop_view(flp_propagator* h) {
@@ -697,9 +798,9 @@ static void check_status(flp_propagator* h) {
 }  // namespace flp
 
 // ------------------------------------------------------------------ C ABI ---
-#define FLP_TRY(body)                                                     \
+#define FLP_TRY(...)                                                      \
     try {                                                                 \
-        body;                                                             \
+        __VA_ARGS__;                                                      \
         return FLP_OK;                                                    \
     } catch (const flp::FlpError& e) {                                    \
         flp::g_last_error = e.what();                                     \
@@ -880,6 +981,47 @@ int flp_get_info(flp_propagator* h, flp_info* out) {
     })
 }
 
+int flp_get_tuning(flp_propagator* h, int32_t* out, int n) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!out || n < FLP_TUNING_FIELDS) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "tuning needs 7 ints");
+        ensure_conv_mode(h);
+        const int32_t v[FLP_TUNING_FIELDS] = {h->conv_mode,         h->geom.wpc_r2c, h->geom.wpc_cols,
+                                              h->geom.share_cols,   h->geom.wpc_c2r, h->gather_gby,
+                                              h->tuning_cached ? 1 : 0};
+        std::memcpy(out, v, sizeof(v));
+    })
+}
+
+int flp_set_tuning(flp_propagator* h, const int32_t* in, int n) {
+    FLP_CHECK_HANDLE(h);
+    FLP_TRY({
+        if (!in || n < FLP_TUNING_FIELDS - 1) throw FlpError(FLP_ERR_INVALID_ARGUMENT, "tuning needs 6 ints");
+        auto one_of = [](int v, int a, int b) { return v == a || v == b; };
+        if (!one_of(in[0], FLP_CONV_DIRECT, FLP_CONV_FFT) || !one_of(in[1], 4, 8) || !one_of(in[2], 4, 8) ||
+            !one_of(in[3], 0, 1) || !one_of(in[4], 4, 8) || !one_of(in[5], 1, 2))
+            throw FlpError(FLP_ERR_INVALID_ARGUMENT, "tuning choice out of range");
+        CK(cudaStreamSynchronize(h->st));
+        ensure_conv_mode(h);
+        if (h->K > 0) {
+            if (in[0] == FLP_CONV_DIRECT && !h->direct_ok)
+                throw FlpError(FLP_ERR_UNSUPPORTED, "direct convolution supports radius <= 24");
+            if (in[0] == FLP_CONV_FFT && !h->fft_ok)
+                throw FlpError(FLP_ERR_UNSUPPORTED, "FFT path needs an even width and sides of factors 2,3,5");
+            h->conv_mode = in[0];
+        }
+        Tuning t;
+        t.wpc_r2c = in[1];
+        t.wpc_cols = in[2];
+        t.share_cols = in[3];
+        t.wpc_c2r = in[4];
+        t.gather_gby = in[5];
+        apply_tuning(h, t);
+        h->tuning_cached = false;
+        invalidate_graphs(h);
+    })
+}
+
 int flp_set_conv_mode(flp_propagator* h, int mode) {
     FLP_CHECK_HANDLE(h);
     FLP_TRY({
@@ -967,7 +1109,6 @@ int flp_debug_transport(flp_propagator* h, const float* state, const float* aff,
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out, o, CN * sizeof(float), cudaMemcpyDeviceToHost, h->st));
         CK(cudaStreamSynchronize(h->st));
-        flp::dfree(a); flp::dfree(o);
     })
 }
 

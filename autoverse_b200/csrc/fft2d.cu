@@ -15,6 +15,7 @@
 // reference, which transforms full complex grids.
 #include "common.cuh"
 #include "fft_items.cuh"
+#include "fft_warp.cuh"
 #include "kernels.h"
 
 #include <math.h>
@@ -331,6 +332,74 @@ __global__ void __launch_bounds__(256) k_c2r_raw_t(const float2* __restrict__ T,
                     scale, accumulate != 0, twM, twW);
 }
 
+// ---- warp-synchronous single-world kernels (fft_warp.cuh)
+template <int M, int WPC>
+__global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_r2c_w(const float* __restrict__ A, float2* __restrict__ S,
+                                                               const int* __restrict__ srcs, int H,
+                                                               const float2* __restrict__ twM,
+                                                               const float2* __restrict__ twW, int* reset_slot,
+                                                               int nreset) {
+    dep_enter();
+    extern __shared__ __align__(16) float2 fsm[];
+    if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        for (int i = 0; i < nreset; ++i) reset_slot[i] = 0;
+    const int slot = blockIdx.y;
+    const int c = srcs ? srcs[slot] : slot;
+    constexpr int W = 2 * M, Wc = M + 1;
+    r2c_rows_witem<M, WPC>(fsm, A + size_t(c) * W * H, S + size_t(slot) * Wc * H, H,
+                           blockIdx.x * WRowCfg<M, WPC>::NRC, twM, twW);
+}
+
+// blockIdx.y: a source slot (share) or a kernel (one transform per kernel).
+template <int H, int WPC>
+__global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_cols_w(const float2* __restrict__ S,
+                                                                const float2* __restrict__ KH, float2* __restrict__ T,
+                                                                const int* __restrict__ slot_of_kernel, int Wc,
+                                                                int slots_per_group, int kernels_per_group, int share,
+                                                                const float2* __restrict__ twH) {
+    dep_enter();
+    extern __shared__ __align__(16) float2 fsm[];
+    int slot, kb, ke;
+    if (share) {
+        slot = blockIdx.y;
+        kb = (slot / slots_per_group) * kernels_per_group;
+        ke = kb + kernels_per_group;
+    } else {
+        kb = blockIdx.y;
+        ke = kb + 1;
+        slot = slot_of_kernel[kb];
+    }
+    cols_witem<H, WPC>(fsm, S + size_t(slot) * Wc * H, KH, T, slot_of_kernel, kb, ke, slot, Wc,
+                       blockIdx.x * WColCfg<H, WPC>::NCC, twH);
+}
+
+template <int M, int WPC>
+__global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_c2r_w(const float2* __restrict__ T, float* __restrict__ U,
+                                                               const KDesc* __restrict__ kd, int K, int H,
+                                                               const float2* __restrict__ twM,
+                                                               const float2* __restrict__ twW) {
+    dep_enter();
+    extern __shared__ __align__(16) float2 fsm[];
+    const int c = blockIdx.y;
+    constexpr int W = 2 * M;
+    c2r_growth_witem<M, WPC>(fsm, T, kd, K, c, U + size_t(c) * W * H, H, blockIdx.x * WRowCfg<M, WPC>::NRC, twM,
+                             twW);
+}
+
+template <int M, int WPC>
+__global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_c2r_raw_w(const float2* __restrict__ T, float* __restrict__ out,
+                                                                   const int* __restrict__ planes, int H, float scale,
+                                                                   int accumulate, const float2* __restrict__ twM,
+                                                                   const float2* __restrict__ twW) {
+    dep_enter();
+    extern __shared__ __align__(16) float2 fsm[];
+    const int slot = blockIdx.y;
+    const int plane = planes ? planes[slot] : slot;
+    constexpr int W = 2 * M, Wc = M + 1;
+    c2r_raw_witem<M, WPC>(fsm, T + size_t(slot) * Wc * H, out + size_t(plane) * W * H, H,
+                          blockIdx.x * WRowCfg<M, WPC>::NRC, scale, accumulate != 0, twM, twW);
+}
+
 bool fft_row_templated(int M) {
 #define X(n) if (M == n) return true;
     FLP_ROW_SIZES(X)
@@ -361,16 +430,39 @@ void fft2d_set_attributes(size_t max_bytes) {
     set((const void*)fft_rows_r2c);
     set((const void*)fft_cols_conv);
     set((const void*)fft_rows_c2r_growth);
-#define X(n) set((const void*)k_r2c_t<n>); set((const void*)k_c2r_t<n>); set((const void*)k_c2r_raw_t<n>);
+#define X(n) set((const void*)k_r2c_t<n>); set((const void*)k_c2r_t<n>); set((const void*)k_c2r_raw_t<n>);     \
+    set((const void*)k_r2c_w<n, 4>); set((const void*)k_r2c_w<n, 8>); set((const void*)k_c2r_w<n, 4>);            \
+    set((const void*)k_c2r_w<n, 8>); set((const void*)k_c2r_raw_w<n, 8>);
     FLP_ROW_SIZES(X)
 #undef X
-#define X(n) set((const void*)k_cols_t<n>);
+#define X(n) set((const void*)k_cols_t<n>); set((const void*)k_cols_w<n, 4>); set((const void*)k_cols_w<n, 8>);
     FLP_COL_SIZES(X)
 #undef X
 }
 
 void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
                     int* reset_slot, int nreset, cudaStream_t st) {
+    const int M = W / 2;
+#define X(n)                                                                                                 \
+    if (M == n) {                                                                                            \
+        if (g.wpc_r2c == 4) {                                                                                \
+            dim3 grid((H + WRowCfg<n, 4>::NRC - 1) / WRowCfg<n, 4>::NRC, nsrc);                              \
+            launch_dep(k_r2c_w<n, 4>, grid, 128, WRowCfg<n, 4>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW,     \
+                       reset_slot, nreset);                                                                  \
+        } else {                                                                                             \
+            dim3 grid((H + WRowCfg<n, 8>::NRC - 1) / WRowCfg<n, 8>::NRC, nsrc);                              \
+            launch_dep(k_r2c_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW,     \
+                       reset_slot, nreset);                                                                  \
+        }                                                                                                    \
+        return;                                                                                              \
+    }
+    FLP_ROW_SIZES(X)
+#undef X
+    launch_fft_r2c_legacy(A, S, srcs, nsrc, W, H, g, reset_slot, nreset, st);
+}
+
+void launch_fft_r2c_legacy(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
+                           int* reset_slot, int nreset, cudaStream_t st) {
     const int M = W / 2;
 #define X(n)                                                                                        \
     if (M == n) {                                                                                   \
@@ -406,8 +498,50 @@ void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* sl
     launch_fft_lines(S, KH, T, slot_of_kernel, K, W / 2 + 1, H, g, mode, scale, st);
 }
 
+void launch_fft_cols_conv(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int nslots, int K,
+                          int groups, int W, int H, const FftGeom& g, cudaStream_t st) {
+    const int Wc = W / 2 + 1;
+    const int share = g.share_cols ? 1 : 0;
+    const int spg = nslots / groups, kpg = K / groups;
+#define X(n)                                                                                                   \
+    if (H == n) {                                                                                              \
+        if (g.wpc_cols == 4) {                                                                                 \
+            dim3 grid((Wc + WColCfg<n, 4>::NCC - 1) / WColCfg<n, 4>::NCC, share ? nslots : K);                 \
+            launch_dep(k_cols_w<n, 4>, grid, 128, WColCfg<n, 4>::smem, st, S, KH, T, slot_of_kernel, Wc, spg,   \
+                       kpg, share, g.twH);                                                                     \
+        } else {                                                                                               \
+            dim3 grid((Wc + WColCfg<n, 8>::NCC - 1) / WColCfg<n, 8>::NCC, share ? nslots : K);                 \
+            launch_dep(k_cols_w<n, 8>, grid, 256, WColCfg<n, 8>::smem, st, S, KH, T, slot_of_kernel, Wc, spg,   \
+                       kpg, share, g.twH);                                                                     \
+        }                                                                                                      \
+        return;                                                                                                \
+    }
+    FLP_COL_SIZES(X)
+#undef X
+    launch_fft_lines(S, KH, T, slot_of_kernel, K, Wc, H, g, 0, 1.f, st);
+}
+
 void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,
                            cudaStream_t st) {
+    const int M = W / 2;
+#define X(n)                                                                                                  \
+    if (M == n) {                                                                                             \
+        if (g.wpc_c2r == 4) {                                                                                 \
+            dim3 grid((H + WRowCfg<n, 4>::NRC - 1) / WRowCfg<n, 4>::NRC, C);                                  \
+            launch_dep(k_c2r_w<n, 4>, grid, 128, WRowCfg<n, 4>::smem_c2r, st, T, U, kd, K, H, g.twM, g.twW);    \
+        } else {                                                                                              \
+            dim3 grid((H + WRowCfg<n, 8>::NRC - 1) / WRowCfg<n, 8>::NRC, C);                                  \
+            launch_dep(k_c2r_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_c2r, st, T, U, kd, K, H, g.twM, g.twW);    \
+        }                                                                                                     \
+        return;                                                                                               \
+    }
+    FLP_ROW_SIZES(X)
+#undef X
+    launch_fft_c2r_growth_legacy(T, U, kd, K, W, H, C, g, st);
+}
+
+void launch_fft_c2r_growth_legacy(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C,
+                                  const FftGeom& g, cudaStream_t st) {
     const int M = W / 2;
 #define X(n)                                                                                     \
     if (M == n) {                                                                                \
@@ -427,9 +561,9 @@ void launch_fft_c2r_raw(const float2* T, float* out, const int* planes, int nslo
     const int M = W / 2;
 #define X(n)                                                                                                  \
     if (M == n) {                                                                                             \
-        dim3 grid((H + RowCfg<n>::NR - 1) / RowCfg<n>::NR, nslots);                                           \
-        launch_dep(k_c2r_raw_t<n>, grid, 256, RowCfg<n>::smem_r2c, st, T, out, planes, H, scale, accumulate ? 1 : 0, \
-                                                                g.twM, g.twW);                                \
+        dim3 grid((H + WRowCfg<n, 8>::NRC - 1) / WRowCfg<n, 8>::NRC, nslots);                                 \
+        launch_dep(k_c2r_raw_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, T, out, planes, H, scale,         \
+                   accumulate ? 1 : 0, g.twM, g.twW);                                                         \
         return;                                                                                               \
     }
     FLP_ROW_SIZES(X)

@@ -27,6 +27,13 @@ struct FftGeom {
     const float2* twW = nullptr;  // exp(-2 pi i t / W),     t <= W/2
     const float2* twH = nullptr;  // exp(-2 pi i t / H),     t < H
     const float2* twD = nullptr;  // exp(-2 pi i t / D),     t < D (3D only)
+    // Warp-synchronous passes (sizes with a compiled plan): warps per CTA of
+    // the row R2C, column and row C2R passes (4 or 8), and whether a column
+    // CTA transforms a source once for all the kernels that read it (share)
+    // or each kernel's column CTA transforms its own source (more CTAs).
+    // Every choice computes the same bits.
+    int wpc_r2c = 8, wpc_cols = 8, wpc_c2r = 8;
+    int share_cols = 1;
 };
 
 bool make_plan(int L, FftPlan& p);
@@ -65,8 +72,9 @@ size_t gather_smem_bytes();
 void transport_2d_set_attributes();
 void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float* MS, int C, int W, int H,
                     const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st);
+// gby: destination rows per thread (1 or 2); both give the same bits.
 void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
-                      const FlowParams& fp, const int* dmax_slot, cudaStream_t st);
+                      const FlowParams& fp, const int* dmax_slot, int gby, cudaStream_t st);
 void launch_zero_ints(int* p, int n, cudaStream_t st);
 
 // FP64 compensated mass
@@ -80,10 +88,20 @@ void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W,
                     int* reset_slot, int nreset, cudaStream_t st);
 void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
                      const FftGeom& g, int mode, float scale, cudaStream_t st);
+void launch_fft_r2c_legacy(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
+                           int* reset_slot, int nreset, cudaStream_t st);
+void launch_fft_c2r_growth_legacy(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C,
+                                  const FftGeom& g, cudaStream_t st);
 void launch_fft_lines(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int nlines,
                       int H, const FftGeom& g, int mode, float scale, cudaStream_t st);
 void launch_fft_c2r_growth(const float2* T, float* U, const KDesc* kd, int K, int W, int H, int C, const FftGeom& g,
                            cudaStream_t st);
+// Column convolution T[k] = IFFT_col(FFT_col(S[slot_of_kernel[k]]) * KH[k])
+// for K kernels over nslots source spectra, in `groups` equal groups (worlds
+// of a batch: group i holds slots [i*nslots/groups, ...) and kernels
+// [i*K/groups, ...)); g.share_cols selects one forward transform per slot.
+void launch_fft_cols_conv(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int nslots, int K,
+                          int groups, int W, int H, const FftGeom& g, cudaStream_t st);
 // Inverse row pass without growth: slot j -> plane planes[j] (or j), times
 // scale, written or accumulated.  Templated row lengths only.
 void launch_fft_c2r_raw(const float2* T, float* out, const int* planes, int nslots, int W, int H, float scale,

@@ -144,17 +144,17 @@ __device__ __forceinline__ void gather_tile_of(int b, int ntx, int nty, int C, i
     ty = (k == 0 || k == 2) ? (row == 0 ? 0 : nty - 1) : 1 + row;
 }
 
-template <bool POW2>
+template <bool POW2, int GBY>
 __global__ void __launch_bounds__(256, 3) gather_2d(const float* __restrict__ DX, const float* __restrict__ DY,
                                                     const float* __restrict__ MS, float* __restrict__ Anext, int W,
                                                     int H, int C, FlowParams fp, const int* __restrict__ dmax_slot) {
     dep_enter();
     extern __shared__ __align__(16) float sm[];
     int tx, ty, c;
-    gather_tile_of(blockIdx.x, (W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), C, tx, ty, c);
+    gather_tile_of(blockIdx.x, (W + GT_W - 1) / GT_W, (H + gt_h(GBY) - 1) / gt_h(GBY), C, tx, ty, c);
     const size_t N = size_t(W) * H;
-    gather_item<POW2, 1>(sm, DX + size_t(c) * N, DY + size_t(c) * N, MS + size_t(c) * N, Anext + size_t(c) * N, W, H,
-                      fp, *dmax_slot, tx * GT_W, ty * gt_h(1));
+    gather_item<POW2, GBY>(sm, DX + size_t(c) * N, DY + size_t(c) * N, MS + size_t(c) * N, Anext + size_t(c) * N, W,
+                           H, fp, *dmax_slot, tx * GT_W, ty * gt_h(GBY));
 }
 
 template <int C, bool POW2>
@@ -189,12 +189,21 @@ void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float*
 }
 
 void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
-                      const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
+                      const FlowParams& fp, const int* dmax_slot, int gby, cudaStream_t st) {
+    if (gby == 2) {
+        const int tiles = ((W + GT_W - 1) / GT_W) * ((H + gt_h(2) - 1) / gt_h(2)) * C;
+        const size_t smem = gather_smem_bytes_inl(2);
+        if (fp.area_pow2)
+            launch_dep(gather_2d<true, 2>, dim3(tiles), 256, smem, st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+        else
+            launch_dep(gather_2d<false, 2>, dim3(tiles), 256, smem, st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+        return;
+    }
     const int tiles = ((W + GT_W - 1) / GT_W) * ((H + gt_h(1) - 1) / gt_h(1)) * C;
     if (fp.area_pow2)
-        launch_dep(gather_2d<true>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+        launch_dep(gather_2d<true, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
     else
-        launch_dep(gather_2d<false>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+        launch_dep(gather_2d<false, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
 }
 
 void transport_2d_set_attributes() {
@@ -204,8 +213,10 @@ void transport_2d_set_attributes() {
     };
     set((const void*)flow_2d<true>, flow_smem_bytes(64));
     set((const void*)flow_2d<false>, flow_smem_bytes(64));
-    set((const void*)gather_2d<true>, gather_smem_bytes());
-    set((const void*)gather_2d<false>, gather_smem_bytes());
+    set((const void*)gather_2d<true, 1>, gather_smem_bytes());
+    set((const void*)gather_2d<false, 1>, gather_smem_bytes());
+    set((const void*)gather_2d<true, 2>, gather_smem_bytes_inl(2));
+    set((const void*)gather_2d<false, 2>, gather_smem_bytes_inl(2));
     cudaFuncSetAttribute(conv_direct_growth_2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(conv_direct_smem_bytes(MAX_DIRECT_RADIUS)));
 }

@@ -259,6 +259,26 @@ class CudaPropagator:
         nat.check(nat.lib().flp_get_info(self._h, C.byref(i)))
         return i
 
+    TUNING_FIELDS = ("conv_mode", "wpc_r2c", "wpc_cols", "share_cols", "wpc_c2r", "gather_gby")
+
+    def tuning(self) -> dict:
+        """The autotuner's launch choices for this world's shape (run on first
+        use, cached per shape for the process); ``cached`` is True when they
+        came from an earlier handle of the same shape."""
+        buf = (C.c_int32 * 7)()
+        nat.check(nat.lib().flp_get_tuning(self._h, buf, 7))
+        out = dict(zip(self.TUNING_FIELDS, list(buf)[:6]))
+        out["cached"] = bool(buf[6])
+        return out
+
+    def set_tuning(self, **choice) -> None:
+        """Force launch choices (any of TUNING_FIELDS; the others keep their
+        current values).  No choice changes the results."""
+        cur = self.tuning()
+        cur.update(choice)
+        buf = (C.c_int32 * 6)(*[int(cur[k]) for k in self.TUNING_FIELDS])
+        nat.check(nat.lib().flp_set_tuning(self._h, buf, 6))
+
     def set_conv_mode(self, mode: int) -> None:
         nat.check(nat.lib().flp_set_conv_mode(self._h, int(mode)))
 

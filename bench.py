@@ -282,7 +282,8 @@ def measure_batched(args, dist):
     # per-stage algorithmic bytes: the single-world figures summed over the worlds
     names = {"r2c": "fft_rows_r2c", "cols": "fft_cols_conv", "c2r": "fft_rows_c2r_growth", "flow": "flow_2d",
              "gather": "gather_2d"}
-    sbytes = {k: sum(stage_bytes(c, names[k]) for c, _ in worlds) for k in stage_ms if k in names}
+    sbytes = {k: sum(stage_bytes(c, names[k.replace("batch_", "")]) for c, _ in worlds)
+              for k in stage_ms if k.replace("batch_", "") in names}
     dom = max(stage_ms, key=stage_ms.get)
     peak, peak_kind = hbm_peak()
     step_min = sum(4 * c["width"] * c["height"] * (len({k["source_channel"] for k in c["kernels"]}) +
@@ -291,7 +292,7 @@ def measure_batched(args, dist):
             "unit": "GB/s", "algorithmic_bytes_per_launch": sbytes[dom],
             "per_stage_gbs": {k: sbytes[k] / (stage_ms[k] * 1e-3) / 1e9 for k in sbytes},
             "step_minimum_bytes": step_min,
-            "step_minimum_frac": step_min / (1e-3 * t / args.batch_steps) / 1e9 / peak,
+            "step_minimum_frac": step_min / (t / args.batch_steps) / 1e9 / peak,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6.65 TB/s"}
     roof["frac"] = roof["achieved"] / peak

@@ -123,6 +123,23 @@ FLP_API int flp_get_info(flp_propagator* h, flp_info* out);
 /* Force a convolution strategy (FLP_CONV_*); FLP_CONV_AUTO re-runs the tuner. */
 FLP_API int flp_set_conv_mode(flp_propagator* h, int mode);
 
+/* Measured launch choices (the autotuner; none of them changes a result bit):
+ *   0 convolution path (FLP_CONV_DIRECT / FLP_CONV_FFT)
+ *   1 warps per CTA of the FFT row R2C pass (4 or 8)
+ *   2 warps per CTA of the FFT column pass (4 or 8)
+ *   3 column pass: 1 = one forward transform per source channel shared by
+ *     the kernels that read it, 0 = one per kernel (more CTAs)
+ *   4 warps per CTA of the FFT row C2R + growth pass (4 or 8)
+ *   5 destination rows per thread of the 2D gather (1 or 2)
+ *   6 (get only) 1 when the choices came from the process-wide cache of an
+ *     earlier handle with the same shape (grid, channels, kernels, radius,
+ *     source channels), 0 when this handle measured them.
+ * The tuner runs on a handle's first step (or flp_set_conv_mode); the choices
+ * are cached per shape for the process.  flp_set_tuning forces fields 0-5. */
+#define FLP_TUNING_FIELDS 7
+FLP_API int flp_get_tuning(flp_propagator* h, int32_t* out, int n);
+FLP_API int flp_set_tuning(flp_propagator* h, const int32_t* in, int n);
+
 /* The handle's cudaStream_t, for callers that time or order work around it. */
 FLP_API void* flp_stream(flp_propagator* h);
 

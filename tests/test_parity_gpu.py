@@ -226,10 +226,49 @@ def sum_channels_f32(st):
     return float(tot)
 
 
-def test_autotuner_picks_a_mode():
-    cfg, st = species_case(seed=12)
+def test_autotuner_picks_a_mode_and_caches_per_shape():
+    """The first handle of a shape measures (convolution path, FFT pass CTA
+    shapes, gather rows per thread); a second handle of the same shape takes
+    the cached choices."""
+    cfg, st = species_case(W=160, H=96, C=2, seed=12)  # a shape no other test uses
     with fl.CudaPropagator(cfg) as p:
+        p.write_state(st)
+        t1 = p.tuning()
         assert p.conv_mode in (fl.CONV_DIRECT, fl.CONV_FFT)
+        assert not t1["cached"]
+    with fl.CudaPropagator(cfg) as q:
+        q.write_state(st)
+        t2 = q.tuning()
+        assert t2["cached"]
+        assert {k: v for k, v in t2.items() if k != "cached"} == {k: v for k, v in t1.items() if k != "cached"}
+
+
+TUNING_VARIANTS = [
+    {},
+    {"wpc_r2c": 4}, {"wpc_cols": 4}, {"share_cols": 0}, {"share_cols": 0, "wpc_cols": 4}, {"wpc_c2r": 4},
+    {"gather_gby": 2},
+    {"wpc_r2c": 4, "wpc_cols": 4, "share_cols": 0, "wpc_c2r": 4, "gather_gby": 2},
+]
+
+
+@pytest.mark.parametrize("shape", [(512, 512, 3), (96, 64, 2), (384, 192, 1)])
+def test_every_tuning_choice_gives_the_same_bits(shape):
+    """Every launch choice the tuner can make computes the same bits (the
+    FFT passes transform each line the same way whatever the CTA shape; the
+    gather sums each destination in the same order)."""
+    W, H, C = shape
+    cfg, st = species_case(W=W, H=H, C=C, R=9, seed=15)
+    base = dict(conv_mode=fl.CONV_FFT, wpc_r2c=8, wpc_cols=8, share_cols=1, wpc_c2r=8, gather_gby=1)
+    ref = None
+    with fl.CudaPropagator(cfg) as p:
+        for v in TUNING_VARIANTS:
+            p.set_tuning(**dict(base, **v))
+            p.write_state(st)
+            p.run_device(4)
+            got = p.read_state()
+            if ref is None:
+                ref = got
+            assert np.array_equal(got, ref), v
 
 
 def test_profile_run_reports_stages():
