@@ -39,7 +39,8 @@ extern thread_local std::string g_last_error;
 
 namespace {
 
-constexpr int BATCH_WPC = 8;           // warps per CTA of the batched FFT passes
+constexpr int BATCH_WPC = 8;           // warps per CTA of the batched row R2C and column passes
+constexpr int BATCH_WPC_C2R = 4;       // warps per CTA of the batched row C2R + growth pass
 constexpr int BATCH_GBY = 2;           // destination rows per thread in the batched gather (64x32 tiles)
 constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
 constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
@@ -56,9 +57,9 @@ int col_class(int H) {
         if (COL_SIZES[i] == H) return i;
     return -1;
 }
-int row_nr(int M) {
+int row_nr(int M, int wpc) {
     switch (M) {
-#define X(n) case n: return WRowCfg<n, BATCH_WPC>::NRC;
+#define X(n) case n: return wpc == 4 ? WRowCfg<n, 4>::NRC : WRowCfg<n, 8>::NRC;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -152,7 +153,7 @@ __global__ void k_batch_reset(Pools p) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
+__global__ void __launch_bounds__(256, 3) k_batch_r2c(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(256) k_batch_r2c(Pools p, int q) {
 }
 
 template <int H>
-__global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
+__global__ void __launch_bounds__(256, 2) k_batch_cols(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(256) k_batch_cols(Pools p, int q) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
+__global__ void __launch_bounds__(32 * BATCH_WPC_C2R, 20 / BATCH_WPC_C2R) k_batch_c2r(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -200,8 +201,8 @@ __global__ void __launch_bounds__(256) k_batch_c2r(Pools p, int q) {
         const BWorld w = p.worlds[item.x];
         const int c = item.y >> 16, g = item.y & 0xFFFF;
         float* Uc = p.U + w.offA + size_t(c) * (2 * M) * w.H;
-        c2r_growth_witem<M, BATCH_WPC>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H,
-                                       g * WRowCfg<M, BATCH_WPC>::NRC, p.tw + w.twM, p.tw + w.twW);
+        c2r_growth_witem<M, BATCH_WPC_C2R>(fsm, p.T + w.offT, p.kd + w.offKd, w.K, c, Uc, w.H,
+                                           g * WRowCfg<M, BATCH_WPC_C2R>::NRC, p.tw + w.twM, p.tw + w.twW);
     }
 }
 
@@ -337,7 +338,7 @@ size_t r2c_smem(int cls) {
 }
 size_t c2r_smem(int cls) {
     switch (ROW_SIZES[cls]) {
-#define X(n) case n: return WRowCfg<n, BATCH_WPC>::smem_c2r;
+#define X(n) case n: return WRowCfg<n, BATCH_WPC_C2R>::smem_c2r;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -510,6 +511,7 @@ struct flp_batch {
     int cur = 0;
     const void* q_fn[NQUEUE] = {nullptr};
     int q_grid[NQUEUE] = {0};
+    int q_block[NQUEUE] = {0};
     size_t q_smem[NQUEUE] = {0};
     std::vector<float> time;
     std::vector<uint64_t> steps;
@@ -552,7 +554,7 @@ struct flp_batch {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(q_grid[q]);
-        cfg.blockDim = dim3(256);
+        cfg.blockDim = dim3(q_block[q]);
         cfg.dynamicSmemBytes = q_smem[q];
         cfg.stream = qs;
         cfg.attrs = attr;
@@ -836,13 +838,14 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     std::vector<int2> items[NQUEUE];
     for (int w : order) {
         const BWorld& d = b->hw[w];
-        const int nr = row_nr(d.W / 2), nc = col_nc(d.H), Wc = d.W / 2 + 1;
+        const int nr = row_nr(d.W / 2, BATCH_WPC), nr2 = row_nr(d.W / 2, BATCH_WPC_C2R), nc = col_nc(d.H),
+                  Wc = d.W / 2 + 1;
         for (int s2 = 0; s2 < d.nsrc; ++s2)
             for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[0 * NCLS + d.mcls].push_back(make_int2(w, (s2 << 16) | g));
         for (int s2 = 0; s2 < d.nsrc; ++s2)
             for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (s2 << 16) | g));
         for (int c = 0; c < d.C; ++c)
-            for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
+            for (int g = 0; g < (d.H + nr2 - 1) / nr2; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
         const int fth = d.C <= 4 ? BATCH_FR_H : FL_H;
         const int ftiles = ((d.W + FL_W - 1) / FL_W) * ((d.H + fth - 1) / fth);
         for (int t = 0; t < ftiles; ++t) items[flow_queue(d.C)].push_back(make_int2(w, t));
@@ -885,7 +888,9 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         }
         if (!b->n_q[q]) continue;
         int per_sm = 0;
-        ckb(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->q_fn[q], 256, b->q_smem[q]), "occupancy");
+        b->q_block[q] = (q / NCLS == 2 && q < 3 * NCLS) ? 32 * BATCH_WPC_C2R : 256;
+        ckb(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->q_fn[q], b->q_block[q], b->q_smem[q]),
+            "occupancy");
         b->q_grid[q] = std::max(1, std::min(per_sm * sms, b->n_q[q]));
     }
     ckb(cudaStreamSynchronize(b->st), "sync");

@@ -712,6 +712,10 @@ void emb_create(flp_embedded* h, const char* json) {
             g.twW = h->d_tw + M;
             g.twH = h->d_tw + M + Wc;
             h->geom = g;
+            // the convolution's own passes: 4-warp CTAs, one column transform
+            // per kernel (measured faster for a few kernels per world)
+            h->geom.wpc_r2c = h->geom.wpc_cols = h->geom.wpc_c2r = 4;
+            h->geom.share_cols = 0;
             std::vector<int> srcs, kslot(h->K);
             for (int k = 0; k < h->K; ++k) {
                 auto it = std::find(srcs.begin(), srcs.end(), ek[k].src);

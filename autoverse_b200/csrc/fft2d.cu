@@ -373,8 +373,19 @@ __global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_cols_w(const float2* __r
                        blockIdx.x * WColCfg<H, WPC>::NCC, twH);
 }
 
+// blockIdx.y: slot (nlines lines of H each); INV: inverse, else forward times scale.
+template <int H, int WPC, bool INV>
+__global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_lines_w(const float2* __restrict__ src, float2* __restrict__ dst,
+                                                                int nlines, float scale,
+                                                                const float2* __restrict__ twH) {
+    dep_enter();
+    extern __shared__ __align__(16) float2 fsm[];
+    const size_t off = size_t(blockIdx.y) * nlines * H;
+    cols_plain_witem<H, WPC, INV>(fsm, src + off, dst + off, nlines, blockIdx.x * WColCfg<H, WPC>::NCC, scale, twH);
+}
+
 template <int M, int WPC>
-__global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_c2r_w(const float2* __restrict__ T, float* __restrict__ U,
+__global__ void __launch_bounds__(32 * WPC, 24 / WPC) k_c2r_w(const float2* __restrict__ T, float* __restrict__ U,
                                                                const KDesc* __restrict__ kd, int K, int H,
                                                                const float2* __restrict__ twM,
                                                                const float2* __restrict__ twW) {
@@ -432,10 +443,11 @@ void fft2d_set_attributes(size_t max_bytes) {
     set((const void*)fft_rows_c2r_growth);
 #define X(n) set((const void*)k_r2c_t<n>); set((const void*)k_c2r_t<n>); set((const void*)k_c2r_raw_t<n>);     \
     set((const void*)k_r2c_w<n, 4>); set((const void*)k_r2c_w<n, 8>); set((const void*)k_c2r_w<n, 4>);            \
-    set((const void*)k_c2r_w<n, 8>); set((const void*)k_c2r_raw_w<n, 8>);
+    set((const void*)k_c2r_w<n, 8>); set((const void*)k_c2r_raw_w<n, 8>); set((const void*)k_c2r_raw_w<n, 4>);
     FLP_ROW_SIZES(X)
 #undef X
-#define X(n) set((const void*)k_cols_t<n>); set((const void*)k_cols_w<n, 4>); set((const void*)k_cols_w<n, 8>);
+#define X(n) set((const void*)k_cols_t<n>); set((const void*)k_cols_w<n, 4>); set((const void*)k_cols_w<n, 8>);     \
+    set((const void*)k_lines_w<n, 4, false>); set((const void*)k_lines_w<n, 4, true>);
     FLP_COL_SIZES(X)
 #undef X
 }
@@ -480,6 +492,20 @@ void launch_fft_r2c_legacy(const float* A, float2* S, const int* srcs, int nsrc,
 
 void launch_fft_lines(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int nlines,
                       int H, const FftGeom& g, int mode, float scale, cudaStream_t st) {
+    if (mode != 0) {
+        // plain forward (mode 1, scaled) or inverse (mode 2) transforms of K slots
+#define X(n)                                                                                                    \
+        if (H == n) {                                                                                           \
+            dim3 grid((nlines + WColCfg<n, 4>::NCC - 1) / WColCfg<n, 4>::NCC, K);                              \
+            if (mode == 1)                                                                                      \
+                launch_dep(k_lines_w<n, 4, false>, grid, 128, WColCfg<n, 4>::smem, st, S, T, nlines, scale, g.twH); \
+            else                                                                                                \
+                launch_dep(k_lines_w<n, 4, true>, grid, 128, WColCfg<n, 4>::smem, st, S, T, nlines, scale, g.twH);  \
+            return;                                                                                             \
+        }
+        FLP_COL_SIZES(X)
+#undef X
+    }
 #define X(n)                                                                                                   \
     if (H == n) {                                                                                              \
         dim3 grid((nlines + ColCfg<n>::NC - 1) / ColCfg<n>::NC, K);                                            \
@@ -561,9 +587,15 @@ void launch_fft_c2r_raw(const float2* T, float* out, const int* planes, int nslo
     const int M = W / 2;
 #define X(n)                                                                                                  \
     if (M == n) {                                                                                             \
-        dim3 grid((H + WRowCfg<n, 8>::NRC - 1) / WRowCfg<n, 8>::NRC, nslots);                                 \
-        launch_dep(k_c2r_raw_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, T, out, planes, H, scale,         \
-                   accumulate ? 1 : 0, g.twM, g.twW);                                                         \
+        if (g.wpc_c2r == 4) {                                                                                 \
+            dim3 grid((H + WRowCfg<n, 4>::NRC - 1) / WRowCfg<n, 4>::NRC, nslots);                             \
+            launch_dep(k_c2r_raw_w<n, 4>, grid, 128, WRowCfg<n, 4>::smem_r2c, st, T, out, planes, H, scale,     \
+                       accumulate ? 1 : 0, g.twM, g.twW);                                                     \
+        } else {                                                                                              \
+            dim3 grid((H + WRowCfg<n, 8>::NRC - 1) / WRowCfg<n, 8>::NRC, nslots);                             \
+            launch_dep(k_c2r_raw_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, T, out, planes, H, scale,     \
+                       accumulate ? 1 : 0, g.twM, g.twW);                                                     \
+        }                                                                                                     \
         return;                                                                                               \
     }
     FLP_ROW_SIZES(X)
