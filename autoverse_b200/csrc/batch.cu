@@ -39,8 +39,25 @@ extern thread_local std::string g_last_error;
 
 namespace {
 
-constexpr int BATCH_WPC = 8;           // warps per CTA of the batched row R2C and column passes
-constexpr int BATCH_WPC_C2R = 4;       // warps per CTA of the batched row C2R + growth pass
+// Warps per CTA of the batched FFT passes and whether a column item serves
+// every kernel of its source (one forward column transform per source) or a
+// single kernel; compile-time choices, none of which changes a result bit.
+#ifndef FLP_BATCH_WPC_R2C
+#define FLP_BATCH_WPC_R2C 4
+#endif
+#ifndef FLP_BATCH_WPC_COLS
+#define FLP_BATCH_WPC_COLS 4
+#endif
+#ifndef FLP_BATCH_WPC_C2R
+#define FLP_BATCH_WPC_C2R 4
+#endif
+#ifndef FLP_BATCH_SHARE_COLS
+#define FLP_BATCH_SHARE_COLS 1
+#endif
+constexpr int BATCH_WPC_R2C = FLP_BATCH_WPC_R2C;
+constexpr int BATCH_WPC_COLS = FLP_BATCH_WPC_COLS;
+constexpr int BATCH_WPC_C2R = FLP_BATCH_WPC_C2R;
+constexpr bool BATCH_SHARE_COLS = FLP_BATCH_SHARE_COLS != 0;
 constexpr int BATCH_GBY = 2;           // destination rows per thread in the batched gather (64x32 tiles)
 constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
 constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
@@ -67,7 +84,7 @@ int row_nr(int M, int wpc) {
 }
 int col_nc(int H) {
     switch (H) {
-#define X(n) case n: return WColCfg<n, BATCH_WPC>::NCC;
+#define X(n) case n: return WColCfg<n, BATCH_WPC_COLS>::NCC;
         FLP_COL_SIZES(X)
 #undef X
     }
@@ -153,7 +170,7 @@ __global__ void k_batch_reset(Pools p) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(256, 3) k_batch_r2c(Pools p, int q) {
+__global__ void __launch_bounds__(32 * BATCH_WPC_R2C, 24 / BATCH_WPC_R2C) k_batch_r2c(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -166,13 +183,13 @@ __global__ void __launch_bounds__(256, 3) k_batch_r2c(Pools p, int q) {
         const int c = p.srcs[w.offSrc + slot];
         const size_t N = size_t(2 * M) * w.H;
         float2* Sc = p.S + w.offS + size_t(slot) * (M + 1) * w.H;
-        r2c_rows_witem<M, BATCH_WPC>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * WRowCfg<M, BATCH_WPC>::NRC,
+        r2c_rows_witem<M, BATCH_WPC_R2C>(fsm, p.A + w.offA + size_t(c) * N, Sc, w.H, g * WRowCfg<M, BATCH_WPC_R2C>::NRC,
                                      p.tw + w.twM, p.tw + w.twW);
     }
 }
 
 template <int H>
-__global__ void __launch_bounds__(256, 2) k_batch_cols(Pools p, int q) {
+__global__ void __launch_bounds__(32 * BATCH_WPC_COLS, 16 / BATCH_WPC_COLS) k_batch_cols(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -181,11 +198,13 @@ __global__ void __launch_bounds__(256, 2) k_batch_cols(Pools p, int q) {
         if (it < 0) break;
         const int2 item = p.items[base + it];
         const BWorld w = p.worlds[item.x];
-        const int slot = item.y >> 16, g = item.y & 0xFFFF;
+        const int u = item.y >> 16, g = item.y & 0xFFFF;  // u: source slot (shared) or kernel
         const int Wc = w.W / 2 + 1;
-        // one forward transform of the slot's columns for all its kernels
-        cols_witem<H, BATCH_WPC>(fsm, p.S + w.offS + size_t(slot) * Wc * H, p.KH + w.offKH, p.T + w.offT,
-                                 p.slots + w.offKd, 0, w.K, slot, Wc, g * WColCfg<H, BATCH_WPC>::NCC, p.tw + w.twH);
+        const int slot = BATCH_SHARE_COLS ? u : p.slots[w.offKd + u];
+        const int kb = BATCH_SHARE_COLS ? 0 : u, ke = BATCH_SHARE_COLS ? w.K : u + 1;
+        cols_witem<H, BATCH_WPC_COLS>(fsm, p.S + w.offS + size_t(slot) * Wc * H, p.KH + w.offKH, p.T + w.offT,
+                                      p.slots + w.offKd, kb, ke, slot, Wc, g * WColCfg<H, BATCH_WPC_COLS>::NCC,
+                                      p.tw + w.twH);
     }
 }
 
@@ -330,7 +349,7 @@ const void* cols_fn(int cls) {
 }
 size_t r2c_smem(int cls) {
     switch (ROW_SIZES[cls]) {
-#define X(n) case n: return WRowCfg<n, BATCH_WPC>::smem_r2c;
+#define X(n) case n: return WRowCfg<n, BATCH_WPC_R2C>::smem_r2c;
         FLP_ROW_SIZES(X)
 #undef X
     }
@@ -346,7 +365,7 @@ size_t c2r_smem(int cls) {
 }
 size_t cols_smem(int cls) {
     switch (COL_SIZES[cls]) {
-#define X(n) case n: return WColCfg<n, BATCH_WPC>::smem;
+#define X(n) case n: return WColCfg<n, BATCH_WPC_COLS>::smem;
         FLP_COL_SIZES(X)
 #undef X
     }
@@ -838,12 +857,12 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     std::vector<int2> items[NQUEUE];
     for (int w : order) {
         const BWorld& d = b->hw[w];
-        const int nr = row_nr(d.W / 2, BATCH_WPC), nr2 = row_nr(d.W / 2, BATCH_WPC_C2R), nc = col_nc(d.H),
+        const int nr = row_nr(d.W / 2, BATCH_WPC_R2C), nr2 = row_nr(d.W / 2, BATCH_WPC_C2R), nc = col_nc(d.H),
                   Wc = d.W / 2 + 1;
         for (int s2 = 0; s2 < d.nsrc; ++s2)
             for (int g = 0; g < (d.H + nr - 1) / nr; ++g) items[0 * NCLS + d.mcls].push_back(make_int2(w, (s2 << 16) | g));
-        for (int s2 = 0; s2 < d.nsrc; ++s2)
-            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (s2 << 16) | g));
+        for (int u = 0; u < (BATCH_SHARE_COLS ? d.nsrc : d.K); ++u)
+            for (int g = 0; g < (Wc + nc - 1) / nc; ++g) items[1 * NCLS + d.hcls].push_back(make_int2(w, (u << 16) | g));
         for (int c = 0; c < d.C; ++c)
             for (int g = 0; g < (d.H + nr2 - 1) / nr2; ++g) items[2 * NCLS + d.mcls].push_back(make_int2(w, (c << 16) | g));
         const int fth = d.C <= 4 ? BATCH_FR_H : FL_H;
@@ -888,7 +907,9 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
         }
         if (!b->n_q[q]) continue;
         int per_sm = 0;
-        b->q_block[q] = (q / NCLS == 2 && q < 3 * NCLS) ? 32 * BATCH_WPC_C2R : 256;
+        const int pass = q < 3 * NCLS ? q / NCLS : 3;
+        b->q_block[q] = pass == 0 ? 32 * BATCH_WPC_R2C : pass == 1 ? 32 * BATCH_WPC_COLS
+                      : pass == 2 ? 32 * BATCH_WPC_C2R : 256;
         ckb(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->q_fn[q], b->q_block[q], b->q_smem[q]),
             "occupancy");
         b->q_grid[q] = std::max(1, std::min(per_sm * sms, b->n_q[q]));
