@@ -8,8 +8,9 @@
 // bit the one CudaPropagator computes.  A_0, A_k, A_2k, ... are kept.
 //
 // Backward: segment by segment from the last checkpoint, the segment's states
-// are recomputed and then each step t is reversed:
-//   1. recompute conv_k, U, the flow destinations and masses from A_t;
+// are recomputed, recording each step's convolution fields conv_k and the
+// sources' column spectra, and then each step t is reversed:
+//   1. U (growth of the recorded conv_k), the flow destinations and masses;
 //   2. reintegration adjoint (per source) -> m^, F^;
 //   3. flow adjoint -> gU^, gS^, S^_local, beta^;
 //   4. Sobel transpose -> U^ and A^ = m^ + S^;
@@ -84,7 +85,7 @@ struct flp_adjoint {
     AdjKern* ak = nullptr;
     KDesc* kd = nullptr;
     int *srcs = nullptr, *slot = nullptr, *dmax = nullptr, *status = nullptr;
-    float2 *KH = nullptr, *S = nullptr, *T = nullptr, *AH = nullptr, *CBH = nullptr, *SB = nullptr, *KS = nullptr;
+    float2 *KH = nullptr, *S = nullptr, *T = nullptr, *CBH = nullptr, *SB = nullptr, *KS = nullptr;
     float *U = nullptr, *DX = nullptr, *DY = nullptr, *MS = nullptr, *conv = nullptr, *CB = nullptr;
     float *MBAR = nullptr, *FXB = nullptr, *FYB = nullptr, *GUX = nullptr, *GUY = nullptr, *UBAR = nullptr;
     float *GSX = nullptr, *GSY = nullptr, *SBL = nullptr;
@@ -93,6 +94,11 @@ struct flp_adjoint {
     float* fin = nullptr;
     float* work[2] = {nullptr, nullptr};
     std::vector<float*> ckpt, seg;
+    // per step of the segment being reversed: the convolution fields conv_k
+    // (B x K x N) and the column spectra of the sources (B x nsrc x spec),
+    // recorded while the segment is recomputed from its checkpoint
+    std::vector<float*> convseg;
+    std::vector<float2*> ahseg;
     double* pg = nullptr;
     int steps = 0, every = 0;
     bool have_forward = false;
@@ -109,40 +115,58 @@ struct flp_adjoint {
         launch_gather_worlds(DX, DY, MS, an, B, C, W, H, fps, pow2, dmax, st);
     }
 
-    // Reverse of step t: a = A_t, gin = dL/dA_{t+1} -> gout = dL/dA_t.
-    void step_adjoint(const float* a, const float* gin, float* gout) {
-        const int nb = int(spec());
-        // 1. recompute
+    // Step i of the segment being reversed, from a = A_t: records conv_k and
+    // the sources' column spectra for its adjoint and, with an, advances to
+    // A_t+1 (the same bits as step(): the growth of the recorded conv fields
+    // is the fused growth's arithmetic).
+    void record_step(const float* a, float* an, int i) {
         launch_fft_r2c(a, S, srcs, B * nsrc, W, H, g, dmax, B, st);
-        launch_fft_cols(S, nullptr, AH, nullptr, B * nsrc, W, H, g, 1, 1.f, st);
+        launch_fft_cols(S, nullptr, ahseg[i], nullptr, B * nsrc, W, H, g, 1, 1.f, st);
         launch_fft_cols_conv(S, KH, T, slot, B * nsrc, B * K, B, W, H, g, st);
-        launch_fft_c2r_raw(T, conv, nullptr, B * K, W, H, 1.f, false, g, st);
-        launch_growth_worlds(conv, U, ak, B, K, C, N, st);
+        launch_fft_c2r_raw(T, convseg[i], nullptr, B * K, W, H, 1.f, false, g, st);
+        if (!an) return;
+        launch_growth_worlds(convseg[i], U, ak, B, K, C, N, st);
+        launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);
+        launch_gather_worlds(DX, DY, MS, an, B, C, W, H, fps, pow2, dmax, st);
+    }
+
+    // Reverse of step t (step i of its segment, recorded): a = A_t, gin =
+    // dL/dA_{t+1} -> gout = dL/dA_t.
+    void step_adjoint(const float* a, const float* gin, float* gout, int i) {
+        const int nb = int(spec());
+        const float* cv = convseg[i];
+        // 1. U and the destinations from the recorded convolution fields
+        launch_zero_ints(dmax, B, st);
+        launch_growth_worlds(cv, U, ak, B, K, C, N, st);
         launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);
         // 2-4. transport adjoints
         launch_adj_reint(DX, DY, MS, gin, MBAR, FXB, FYB, B, C, W, H, fps, pow2, st);
         launch_adj_flow(a, U, FXB, FYB, GUX, GUY, GSX, GSY, SBL, pg, P, B, C, W, H, fps, st);
         launch_adj_sobel_t(GUX, GUY, GSX, GSY, SBL, MBAR, UBAR, gout, B, C, W, H, st);
         // 5. growth adjoint
-        launch_adj_growth(conv, UBAR, CB, ak, pg, P, B, K, C, N, st);
+        launch_adj_growth(cv, UBAR, CB, ak, pg, P, B, K, C, N, st);
         // 6. convolution adjoint
         launch_fft_r2c(CB, T, nullptr, B * K, W, H, g, nullptr, 0, st);
         launch_fft_cols(T, nullptr, CBH, nullptr, B * K, W, H, g, 1, 1.f, st);
-        launch_adj_spectral(KH, CBH, AH, SB, KS, ak, B, K, nsrc, nb, st);
+        launch_adj_spectral(KH, CBH, ahseg[i], SB, KS, ak, B, K, nsrc, nb, st);
         launch_fft_cols(SB, nullptr, SB, nullptr, B * nsrc, W, H, g, 2, 1.f, st);
         launch_fft_c2r_raw(SB, gout, srcs, B * nsrc, W, H, 1.f, true, g, st);
     }
 
     void free_all() {
-        void* ptrs[] = {tw, fps, ak, kd, srcs, slot, dmax, status, KH, S, T, AH, CBH, SB, KS, U, DX, DY, MS, conv,
+        void* ptrs[] = {tw, fps, ak, kd, srcs, slot, dmax, status, KH, S, T, CBH, SB, KS, U, DX, DY, MS, conv,
                         CB, MBAR, FXB, FYB, GUX, GUY, UBAR, GSX, GSY, SBL, G[0], G[1], state0, fin, work[0], work[1],
                         pg};
         for (void* p : ptrs)
             if (p) flp::dfree(p);
         for (float* p : ckpt) flp::dfree(p);
         for (float* p : seg) flp::dfree(p);
+        for (float* p : convseg) flp::dfree(p);
+        for (float2* p : ahseg) flp::dfree(p);
         ckpt.clear();
         seg.clear();
+        convseg.clear();
+        ahseg.clear();
         for (cudaEvent_t e : {e0, e1, e2, e3})
             if (e) cudaEventDestroy(e);
         if (st) cudaStreamDestroy(st);
@@ -217,6 +241,10 @@ void adj_create(flp_adjoint* h, const char* const* jsons, int n) {
     h->g.twM = h->tw;
     h->g.twW = h->tw + M;
     h->g.twH = h->tw + M + Wc;
+    // 4-warp CTAs for the FFT passes of the whole batch (throughput-bound, as
+    // in the batched engine); the column pass transforms each source once
+    h->g.wpc_r2c = h->g.wpc_cols = h->g.wpc_c2r = 4;
+    h->g.share_cols = 1;
     // per-world tables
     std::vector<FlowParams> fps;
     std::vector<AdjKern> ak;
@@ -272,7 +300,6 @@ void adj_create(flp_adjoint* h, const char* const* jsons, int n) {
     h->KH = dalloc_a<float2>(sp * BK);
     h->S = dalloc_a<float2>(sp * nsl);
     h->T = dalloc_a<float2>(sp * BK);
-    h->AH = dalloc_a<float2>(sp * nsl);
     h->CBH = dalloc_a<float2>(sp * BK);
     h->SB = dalloc_a<float2>(sp * nsl);
     h->KS = dalloc_a<float2>(sp * BK);
@@ -310,6 +337,8 @@ void adj_forward(flp_adjoint* h, int steps, int every) {
     const int nck = (steps + every - 1) / every;
     while (int(h->ckpt.size()) < nck) h->ckpt.push_back(dalloc_a<float>(CN));
     while (int(h->seg.size()) < every) h->seg.push_back(dalloc_a<float>(CN));
+    while (int(h->convseg.size()) < every) h->convseg.push_back(dalloc_a<float>(size_t(h->B) * h->K * h->N));
+    while (int(h->ahseg.size()) < every) h->ahseg.push_back(dalloc_a<float2>(size_t(h->B) * h->nsrc * h->spec()));
     CKA(cudaEventRecord(h->e0, h->st));
     CKA(cudaMemcpyAsync(h->ckpt[0], h->state0, CN * sizeof(float), cudaMemcpyDeviceToDevice, h->st));
     const float* a = h->ckpt[0];
@@ -390,12 +419,15 @@ void adj_backward(flp_adjoint* h, const float* dl_dfinal, float* dl_dinit, doubl
     const int nck = (h->steps + h->every - 1) / h->every;
     for (int j = nck - 1; j >= 0; --j) {
         const int t0 = j * h->every, t1 = std::min(t0 + h->every, h->steps);
-        // segment states: seg[i] = A_{t0+i} for 0 < i < t1 - t0 (A_{t0} is the checkpoint)
+        // segment states: seg[i] = A_{t0+i} for 0 < i < t1 - t0 (A_{t0} is the
+        // checkpoint), recomputed with every step's convolution recorded
         const float* base = h->ckpt[j];
-        for (int i = 1; i < t1 - t0; ++i) h->step(i == 1 ? base : h->seg[i - 1], h->seg[i]);
+        const int n = t1 - t0;
+        for (int i = 0; i < n; ++i)
+            h->record_step(i == 0 ? base : h->seg[i], i + 1 < n ? h->seg[i + 1] : nullptr, i);
         for (int t = t1 - 1; t >= t0; --t) {
             const float* a = t == t0 ? base : h->seg[t - t0];
-            h->step_adjoint(a, h->G[cur], h->G[cur ^ 1]);
+            h->step_adjoint(a, h->G[cur], h->G[cur ^ 1], t - t0);
             cur ^= 1;
         }
     }

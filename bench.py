@@ -55,6 +55,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline (profiling runs)")
+    ap.add_argument("--tuning", default=None,
+                    help="force the FFT launch choices wpc_r2c,wpc_cols,share_cols,wpc_c2r,gather_gby (profiling runs, "
+                         "where the tuner's timings are distorted by the profiler); default: the tuner's own")
     ap.add_argument("--conv", choices=["auto", "direct", "fft"], default="auto",
                     help="convolution path (auto = the engine's measured choice)")
     ap.add_argument("--batch-worlds", type=int, default=4096, help="worlds in the batched measurement (0 = skip)")
@@ -589,7 +592,11 @@ def main():
     dev = nat.device_info()
     p = fl.CudaPropagator(cfg, conv_mode={"auto": fl.CONV_AUTO, "direct": fl.CONV_DIRECT,
                                           "fft": fl.CONV_FFT}[args.conv])
+    if args.tuning:
+        v = [int(x) for x in args.tuning.split(",")]
+        p.set_tuning(conv_mode=p.conv_mode, wpc_r2c=v[0], wpc_cols=v[1], share_cols=v[2], wpc_c2r=v[3], gather_gby=v[4])
     mode = {fl.CONV_DIRECT: "direct", fl.CONV_FFT: "fft"}[p.conv_mode]
+    tuning = p.tuning()
     p.write_state(state)
     flush = not args.no_flush
     # warm-up (untimed)
@@ -671,7 +678,7 @@ def main():
         "metric": metric, "value": value, "unit": "cell-steps/s", "n_gpus": WORLD, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, 0x5EED)",
-        "config": dict(desc, conv_path=mode, parallelism=("replicas x%d" % WORLD) if WORLD > 1 else "single GPU",
+        "config": dict(desc, conv_path=mode, launch_choices={k: tuning[k] for k in p.TUNING_FIELDS[1:]}, parallelism=("replicas x%d" % WORLD) if WORLD > 1 else "single GPU",
                        l2="flushed before every timed step" if flush else "warm"),
         "cell_channel_steps_per_s": value * C,
         "stage_ms_per_step": {k: v / stage_steps for k, v in stages.items()},
