@@ -58,7 +58,10 @@ constexpr int BATCH_WPC_R2C = FLP_BATCH_WPC_R2C;
 constexpr int BATCH_WPC_COLS = FLP_BATCH_WPC_COLS;
 constexpr int BATCH_WPC_C2R = FLP_BATCH_WPC_C2R;
 constexpr bool BATCH_SHARE_COLS = FLP_BATCH_SHARE_COLS != 0;
-constexpr int BATCH_GBY = 2;           // destination rows per thread in the batched gather (64x32 tiles)
+#ifndef FLP_BATCH_GBY
+#define FLP_BATCH_GBY 2
+#endif
+constexpr int BATCH_GBY = FLP_BATCH_GBY;  // destination rows per thread in the batched gather (64x32 tiles)
 constexpr int ROW_SIZES[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
 constexpr int COL_SIZES[] = {32, 48, 64, 96, 128, 192, 256, 384, 512};
 constexpr int NSTAGE = 5;
@@ -228,7 +231,10 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_C2R, 20 / BATCH_WPC_C2R) k_batc
 // Rows per thread of the batched row-walking flow (tile height 8 * that): the
 // persistent kernel is throughput-bound, so a taller walk that reloads fewer
 // halo rows pays, where the single-world kernel wants more, shorter tiles.
-constexpr int BATCH_FR_RPT = 4;
+#ifndef FLP_BATCH_FR_RPT
+#define FLP_BATCH_FR_RPT 4
+#endif
+constexpr int BATCH_FR_RPT = FLP_BATCH_FR_RPT;
 constexpr int BATCH_FR_H = 8 * BATCH_FR_RPT;
 
 template <int CV>
