@@ -86,7 +86,7 @@ struct flp_adjoint {
     KDesc* kd = nullptr;
     int *srcs = nullptr, *slot = nullptr, *dmax = nullptr, *status = nullptr;
     float2 *KH = nullptr, *S = nullptr, *T = nullptr, *CBH = nullptr, *SB = nullptr, *KS = nullptr;
-    float *U = nullptr, *DX = nullptr, *DY = nullptr, *MS = nullptr, *conv = nullptr, *CB = nullptr;
+    float *U = nullptr, *DX = nullptr, *DY = nullptr, *conv = nullptr, *CB = nullptr;
     float *MBAR = nullptr, *FXB = nullptr, *FYB = nullptr, *GUX = nullptr, *GUY = nullptr, *UBAR = nullptr;
     float *GSX = nullptr, *GSY = nullptr, *SBL = nullptr;
     float* G[2] = {nullptr, nullptr};
@@ -111,8 +111,8 @@ struct flp_adjoint {
         launch_fft_r2c(a, S, srcs, B * nsrc, W, H, g, dmax, B, st);
         launch_fft_cols_conv(S, KH, T, slot, B * nsrc, B * K, B, W, H, g, st);
         launch_fft_c2r_growth(T, U, kd, B * K, W, H, B * C, g, st);
-        launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);
-        launch_gather_worlds(DX, DY, MS, an, B, C, W, H, fps, pow2, dmax, st);
+        launch_flow_worlds(a, U, DX, DY, B, C, W, H, fps, dmax, status, st);
+        launch_gather_worlds(DX, DY, a, an, B, C, W, H, fps, pow2, dmax, st);
     }
 
     // Step i of the segment being reversed, from a = A_t: records conv_k and
@@ -126,8 +126,8 @@ struct flp_adjoint {
         launch_fft_c2r_raw(T, convseg[i], nullptr, B * K, W, H, 1.f, false, g, st);
         if (!an) return;
         launch_growth_worlds(convseg[i], U, ak, B, K, C, N, st);
-        launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);
-        launch_gather_worlds(DX, DY, MS, an, B, C, W, H, fps, pow2, dmax, st);
+        launch_flow_worlds(a, U, DX, DY, B, C, W, H, fps, dmax, status, st);
+        launch_gather_worlds(DX, DY, a, an, B, C, W, H, fps, pow2, dmax, st);
     }
 
     // Reverse of step t (step i of its segment, recorded): a = A_t, gin =
@@ -138,9 +138,9 @@ struct flp_adjoint {
         // 1. U and the destinations from the recorded convolution fields
         launch_zero_ints(dmax, B, st);
         launch_growth_worlds(cv, U, ak, B, K, C, N, st);
-        launch_flow_worlds(a, U, DX, DY, MS, B, C, W, H, fps, pow2, dmax, status, st);
+        launch_flow_worlds(a, U, DX, DY, B, C, W, H, fps, dmax, status, st);
         // 2-4. transport adjoints
-        launch_adj_reint(DX, DY, MS, gin, MBAR, FXB, FYB, B, C, W, H, fps, pow2, st);
+        launch_adj_reint(DX, DY, a, gin, MBAR, FXB, FYB, B, C, W, H, fps, pow2, st);
         launch_adj_flow(a, U, FXB, FYB, GUX, GUY, GSX, GSY, SBL, pg, P, B, C, W, H, fps, st);
         launch_adj_sobel_t(GUX, GUY, GSX, GSY, SBL, MBAR, UBAR, gout, B, C, W, H, st);
         // 5. growth adjoint
@@ -154,7 +154,7 @@ struct flp_adjoint {
     }
 
     void free_all() {
-        void* ptrs[] = {tw, fps, ak, kd, srcs, slot, dmax, status, KH, S, T, CBH, SB, KS, U, DX, DY, MS, conv,
+        void* ptrs[] = {tw, fps, ak, kd, srcs, slot, dmax, status, KH, S, T, CBH, SB, KS, U, DX, DY, conv,
                         CB, MBAR, FXB, FYB, GUX, GUY, UBAR, GSX, GSY, SBL, G[0], G[1], state0, fin, work[0], work[1],
                         pg};
         for (void* p : ptrs)
@@ -303,7 +303,7 @@ void adj_create(flp_adjoint* h, const char* const* jsons, int n) {
     h->CBH = dalloc_a<float2>(sp * BK);
     h->SB = dalloc_a<float2>(sp * nsl);
     h->KS = dalloc_a<float2>(sp * BK);
-    for (float** p : {&h->U, &h->DX, &h->DY, &h->MS, &h->MBAR, &h->FXB, &h->FYB, &h->GUX, &h->GUY, &h->UBAR,
+    for (float** p : {&h->U, &h->DX, &h->DY, &h->MBAR, &h->FXB, &h->FYB, &h->GUX, &h->GUY, &h->UBAR,
                       &h->G[0], &h->G[1], &h->state0, &h->fin, &h->work[0], &h->work[1]})
         *p = dalloc_a<float>(CN);
     h->conv = dalloc_a<float>(BK * h->N);

@@ -17,13 +17,14 @@ struct AdjKern {
     int pad;
 };
 
-void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, float* MS, int B, int C, int W, int H,
-                        const FlowParams* fps, bool pow2, int* dmax, int* status, cudaStream_t st);
-void launch_gather_worlds(const float* DX, const float* DY, const float* MS, float* An, int B, int C, int W, int H,
+void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, int B, int C, int W, int H,
+                        const FlowParams* fps, int* dmax, int* status, cudaStream_t st);
+// A: the state the flow pass read (the sources' masses)
+void launch_gather_worlds(const float* DX, const float* DY, const float* A, float* An, int B, int C, int W, int H,
                           const FlowParams* fps, bool pow2, const int* dmax, cudaStream_t st);
 void launch_growth_worlds(const float* conv, float* U, const AdjKern* ak, int B, int K, int C, int N,
                           cudaStream_t st);
-void launch_adj_reint(const float* DX, const float* DY, const float* MS, const float* G, float* MBAR, float* FXB,
+void launch_adj_reint(const float* DX, const float* DY, const float* A, const float* G, float* MBAR, float* FXB,
                       float* FYB, int B, int C, int W, int H, const FlowParams* fps, bool pow2, cudaStream_t st);
 void launch_adj_flow(const float* A, const float* U, const float* FXB, const float* FYB, float* GUX, float* GUY,
                      float* GSX, float* GSY, float* SBL, double* pgrad, int P, int B, int C, int W, int H,

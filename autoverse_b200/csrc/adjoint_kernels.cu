@@ -22,59 +22,58 @@
 namespace flp {
 
 // ------------------------------------------------------ forward, batched ----
-template <int CV, bool POW2>
+template <int CV>
 __global__ void __launch_bounds__(256) k_flow_worlds(const float* __restrict__ A, const float* __restrict__ U,
-                                                     float* __restrict__ DX, float* __restrict__ DY,
-                                                     float* __restrict__ MS, int C, int W, int H,
-                                                     const FlowParams* __restrict__ fps, int* dmax, int* status) {
+                                                     float* __restrict__ DX, float* __restrict__ DY, int C, int W,
+                                                     int H, const FlowParams* __restrict__ fps, int* dmax,
+                                                     int* status) {
     extern __shared__ __align__(16) float sm[];
     const int w = blockIdx.z;
     const size_t off = size_t(w) * C * W * H;
     const FlowParams fp = fps[w];
     if constexpr (CV == 0)
-        flow_item<POW2>(sm, A + off, U + off, DX + off, DY + off, MS + off, C, W, H, fp, blockIdx.x * FL_W,
-                        blockIdx.y * FL_H, dmax + w, status);
+        flow_item(sm, A + off, U + off, DX + off, DY + off, C, W, H, fp, blockIdx.x * FL_W, blockIdx.y * FL_H,
+                  dmax + w, status);
     else
-        flow_rows_item<CV, POW2>(A + off, U + off, DX + off, DY + off, MS + off, W, H, fp, blockIdx.x * 32,
-                                 blockIdx.y * FR_H, dmax + w, status);
+        flow_rows_item<CV>(A + off, U + off, DX + off, DY + off, W, H, fp, blockIdx.x * 32, blockIdx.y * FR_H,
+                           dmax + w, status);
 }
 
 template <bool POW2>
 __global__ void __launch_bounds__(256, 3) k_gather_worlds(const float* __restrict__ DX, const float* __restrict__ DY,
-                                                          const float* __restrict__ MS, float* __restrict__ An, int C,
+                                                          const float* __restrict__ A, float* __restrict__ An, int C,
                                                           int W, int H, const FlowParams* __restrict__ fps,
                                                           const int* __restrict__ dmax) {
     extern __shared__ __align__(16) float sm[];
     const int p = blockIdx.z, w = p / C;
     const size_t off = size_t(p) * W * H;
     const FlowParams fp = fps[w];
-    gather_item<POW2, 1>(sm, DX + off, DY + off, MS + off, An + off, W, H, fp, dmax[w], blockIdx.x * GT_W,
+    gather_item<POW2, 1>(sm, DX + off, DY + off, A + off, An + off, W, H, fp, dmax[w], blockIdx.x * GT_W,
                       blockIdx.y * gt_h(1));
 }
 
-void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, float* MS, int B, int C, int W, int H,
-                        const FlowParams* fps, bool pow2, int* dmax, int* status, cudaStream_t st) {
+void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, int B, int C, int W, int H,
+                        const FlowParams* fps, int* dmax, int* status, cudaStream_t st) {
     const int cv = C <= 4 ? C : 0;
     const int th = cv ? FR_H : FL_H;
     const dim3 grid((W + FL_W - 1) / FL_W, (H + th - 1) / th, B);
     const size_t smem = cv ? 0 : flow_smem_bytes(C);
-#define FW_CASE(v)                                                                                             \
-    if (cv == v) {                                                                                             \
-        if (pow2) k_flow_worlds<v, true><<<grid, 256, smem, st>>>(A, U, DX, DY, MS, C, W, H, fps, dmax, status);  \
-        else k_flow_worlds<v, false><<<grid, 256, smem, st>>>(A, U, DX, DY, MS, C, W, H, fps, dmax, status);      \
-        return;                                                                                                \
+    switch (cv) {
+        case 1: k_flow_worlds<1><<<grid, 256, smem, st>>>(A, U, DX, DY, C, W, H, fps, dmax, status); break;
+        case 2: k_flow_worlds<2><<<grid, 256, smem, st>>>(A, U, DX, DY, C, W, H, fps, dmax, status); break;
+        case 3: k_flow_worlds<3><<<grid, 256, smem, st>>>(A, U, DX, DY, C, W, H, fps, dmax, status); break;
+        case 4: k_flow_worlds<4><<<grid, 256, smem, st>>>(A, U, DX, DY, C, W, H, fps, dmax, status); break;
+        default: k_flow_worlds<0><<<grid, 256, smem, st>>>(A, U, DX, DY, C, W, H, fps, dmax, status); break;
     }
-    FW_CASE(0) FW_CASE(1) FW_CASE(2) FW_CASE(3) FW_CASE(4)
-#undef FW_CASE
 }
 
-void launch_gather_worlds(const float* DX, const float* DY, const float* MS, float* An, int B, int C, int W, int H,
+void launch_gather_worlds(const float* DX, const float* DY, const float* A, float* An, int B, int C, int W, int H,
                           const FlowParams* fps, bool pow2, const int* dmax, cudaStream_t st) {
     dim3 grid((W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), B * C);
     if (pow2)
-        k_gather_worlds<true><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, An, C, W, H, fps, dmax);
+        k_gather_worlds<true><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, A, An, C, W, H, fps, dmax);
     else
-        k_gather_worlds<false><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, MS, An, C, W, H, fps, dmax);
+        k_gather_worlds<false><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, A, An, C, W, H, fps, dmax);
 }
 
 // U_t = sum over kernels targeting t (kernel order) of w G(conv_k), with the
@@ -125,7 +124,7 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
 // mass and get zero gradients.
 template <bool POW2>
 __global__ void __launch_bounds__(256) k_adj_reint(const float* __restrict__ DX, const float* __restrict__ DY,
-                                                   const float* __restrict__ MS, const float* __restrict__ G,
+                                                   const float* __restrict__ A, const float* __restrict__ G,
                                                    float* __restrict__ MBAR, float* __restrict__ FXB,
                                                    float* __restrict__ FYB, int C, int W, int H,
                                                    const FlowParams* __restrict__ fps) {
@@ -135,7 +134,7 @@ __global__ void __launch_bounds__(256) k_adj_reint(const float* __restrict__ DX,
     const FlowParams fp = fps[w];
     const size_t N = size_t(W) * H;
     const size_t idx = size_t(p) * N + size_t(Y) * W + X;
-    const float m = MS[idx];
+    const float m = source_mass<POW2>(A[idx], fp);
     if (m == 0.f) {
         MBAR[idx] = 0.f;
         FXB[idx] = 0.f;
@@ -180,11 +179,11 @@ __global__ void __launch_bounds__(256) k_adj_reint(const float* __restrict__ DX,
     FYB[idx] = fp.dt * mprime * gy;
 }
 
-void launch_adj_reint(const float* DX, const float* DY, const float* MS, const float* G, float* MBAR, float* FXB,
+void launch_adj_reint(const float* DX, const float* DY, const float* A, const float* G, float* MBAR, float* FXB,
                       float* FYB, int B, int C, int W, int H, const FlowParams* fps, bool pow2, cudaStream_t st) {
     dim3 grid((W + 31) / 32, (H + 7) / 8, B * C);
-    if (pow2) k_adj_reint<true><<<grid, 256, 0, st>>>(DX, DY, MS, G, MBAR, FXB, FYB, C, W, H, fps);
-    else k_adj_reint<false><<<grid, 256, 0, st>>>(DX, DY, MS, G, MBAR, FXB, FYB, C, W, H, fps);
+    if (pow2) k_adj_reint<true><<<grid, 256, 0, st>>>(DX, DY, A, G, MBAR, FXB, FYB, C, W, H, fps);
+    else k_adj_reint<false><<<grid, 256, 0, st>>>(DX, DY, A, G, MBAR, FXB, FYB, C, W, H, fps);
 }
 
 // Stage C planes of a field family over a 34x10 region (1-cell torus halo).
@@ -428,8 +427,7 @@ void adjoint_set_attributes() {
     auto set = [](const void* f, size_t bytes) {
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     };
-    set((const void*)k_flow_worlds<0, true>, flow_smem_bytes(ADJ_MAX_CHANNELS));
-    set((const void*)k_flow_worlds<0, false>, flow_smem_bytes(ADJ_MAX_CHANNELS));
+    set((const void*)k_flow_worlds<0>, flow_smem_bytes(ADJ_MAX_CHANNELS));
     set((const void*)k_gather_worlds<true>, gather_smem_bytes());
     set((const void*)k_gather_worlds<false>, gather_smem_bytes());
     set((const void*)k_adj_flow, sizeof(float) * (2 * ADJ_MAX_CHANNELS + 1) * FL_RC);

@@ -58,6 +58,17 @@ constexpr int BATCH_WPC_R2C = FLP_BATCH_WPC_R2C;
 constexpr int BATCH_WPC_COLS = FLP_BATCH_WPC_COLS;
 constexpr int BATCH_WPC_C2R = FLP_BATCH_WPC_C2R;
 constexpr bool BATCH_SHARE_COLS = FLP_BATCH_SHARE_COLS != 0;
+// Resident warps per SM that each FFT pass's launch bounds ask the register
+// allocator for (the passes are latency-bound single waves of persistent CTAs).
+#ifndef FLP_BATCH_WARPS_R2C
+#define FLP_BATCH_WARPS_R2C 24
+#endif
+#ifndef FLP_BATCH_WARPS_COLS
+#define FLP_BATCH_WARPS_COLS 16
+#endif
+#ifndef FLP_BATCH_WARPS_C2R
+#define FLP_BATCH_WARPS_C2R 20
+#endif
 #ifndef FLP_BATCH_GBY
 #define FLP_BATCH_GBY 2
 #endif
@@ -96,7 +107,7 @@ int col_nc(int H) {
 
 struct BWorld {
     int W, H, C, K, nsrc, mcls, hcls, pad;
-    long long offA;  // float offset of channel 0 in the state / U / DX / DY / MS pools
+    long long offA;  // float offset of channel 0 in the state / U / DX / DY pools
     long long offS;  // float2 offset in the source-spectrum pool
     long long offT;  // float2 offset in the product pool
     long long offKH; // float2 offset in the kernel-spectrum pool, shared by worlds with the same grid and stencils
@@ -130,7 +141,6 @@ struct Pools {
     float* U;
     float* DX;
     float* DY;
-    float* MS;
     float2* S;
     float2* T;
     const float2* KH;
@@ -173,7 +183,7 @@ __global__ void k_batch_reset(Pools p) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(32 * BATCH_WPC_R2C, 24 / BATCH_WPC_R2C) k_batch_r2c(Pools p, int q) {
+__global__ void __launch_bounds__(32 * BATCH_WPC_R2C, FLP_BATCH_WARPS_R2C / BATCH_WPC_R2C) k_batch_r2c(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -192,7 +202,7 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_R2C, 24 / BATCH_WPC_R2C) k_batc
 }
 
 template <int H>
-__global__ void __launch_bounds__(32 * BATCH_WPC_COLS, 16 / BATCH_WPC_COLS) k_batch_cols(Pools p, int q) {
+__global__ void __launch_bounds__(32 * BATCH_WPC_COLS, FLP_BATCH_WARPS_COLS / BATCH_WPC_COLS) k_batch_cols(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -212,7 +222,7 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_COLS, 16 / BATCH_WPC_COLS) k_ba
 }
 
 template <int M>
-__global__ void __launch_bounds__(32 * BATCH_WPC_C2R, 20 / BATCH_WPC_C2R) k_batch_c2r(Pools p, int q) {
+__global__ void __launch_bounds__(32 * BATCH_WPC_C2R, FLP_BATCH_WARPS_C2R / BATCH_WPC_C2R) k_batch_c2r(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
@@ -251,16 +261,11 @@ __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
         const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * (CV ? BATCH_FR_H : FL_H);
         const float* A = p.A + w.offA;
         const float* U = p.U + w.offA;
-        float *DX = p.DX + w.offA, *DY = p.DY + w.offA, *MS = p.MS + w.offA;
-        if constexpr (CV == 0) {
-            if (w.fp.area_pow2) flow_item<true>(sm, A, U, DX, DY, MS, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
-            else flow_item<false>(sm, A, U, DX, DY, MS, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
-        } else {
-            if (w.fp.area_pow2)
-                flow_rows_item<CV, true, BATCH_FR_RPT>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
-            else
-                flow_rows_item<CV, false, BATCH_FR_RPT>(A, U, DX, DY, MS, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
-        }
+        float *DX = p.DX + w.offA, *DY = p.DY + w.offA;
+        if constexpr (CV == 0)
+            flow_item(sm, A, U, DX, DY, w.C, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
+        else
+            flow_rows_item<CV, BATCH_FR_RPT>(A, U, DX, DY, w.W, w.H, w.fp, x0, y0, p.dmax + item.x, p.status);
     }
 }
 
@@ -280,9 +285,9 @@ __global__ void __launch_bounds__(256, 3) k_batch_gather(Pools p) {
         const size_t off = size_t(w.offA) + size_t(c) * w.W * w.H;
         const int bits = p.dmax[item.x];
         if (w.fp.area_pow2)
-            gather_item<true, BATCH_GBY>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
+            gather_item<true, BATCH_GBY>(sm, p.DX + off, p.DY + off, p.A + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
         else
-            gather_item<false, BATCH_GBY>(sm, p.DX + off, p.DY + off, p.MS + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
+            gather_item<false, BATCH_GBY>(sm, p.DX + off, p.DY + off, p.A + off, p.Anext + off, w.W, w.H, w.fp, bits, x0, y0);
     }
 }
 
@@ -523,7 +528,7 @@ struct flp_batch {
     int* d_dmax = nullptr;
     int* d_status = nullptr;
     float* A[2] = {nullptr, nullptr};
-    float *U = nullptr, *DX = nullptr, *DY = nullptr, *MS = nullptr;
+    float *U = nullptr, *DX = nullptr, *DY = nullptr;
     float2 *S = nullptr, *T = nullptr, *KH = nullptr, *tw = nullptr;
     KDesc* d_kd = nullptr;
     int *d_srcs = nullptr, *d_slots = nullptr;
@@ -563,7 +568,7 @@ struct flp_batch {
         p.n_worlds = n;
         p.A = A[cur];
         p.Anext = A[cur ^ 1];
-        p.U = U; p.DX = DX; p.DY = DY; p.MS = MS;
+        p.U = U; p.DX = DX; p.DY = DY;
         p.S = S; p.T = T; p.KH = KH;
         p.kd = d_kd; p.srcs = d_srcs; p.slots = d_slots; p.tw = tw;
         return p;
@@ -648,7 +653,7 @@ struct flp_batch {
         if (ev_fork) cudaEventDestroy(ev_fork);
         for (cudaStream_t q : side)
             if (q) cudaStreamDestroy(q);
-        void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, MS, S, T,
+        void* ptrs[] = {d_worlds, d_items, d_qoff, d_counters, d_dmax, d_status, A[0], A[1], U, DX, DY, S, T,
                         KH, tw, d_kd, d_srcs, d_slots, d_mass, flush_buf, d_stats, d_celloff, d_snaps};
         for (void* q : ptrs)
             if (q) flp::dfree(q);
@@ -815,7 +820,6 @@ void batch_create(flp_batch* b, const char* const* jsons, int n) {
     b->U = dalloc_b<float>(CN);
     b->DX = dalloc_b<float>(CN);
     b->DY = dalloc_b<float>(CN);
-    b->MS = dalloc_b<float>(CN);
     ckb(cudaMemsetAsync(b->A[0], 0, CN * sizeof(float), b->st), "memset");
     ckb(cudaMemsetAsync(b->A[1], 0, CN * sizeof(float), b->st), "memset");
     ckb(cudaMemsetAsync(b->U, 0, CN * sizeof(float), b->st), "memset");

@@ -204,13 +204,12 @@ __device__ __forceinline__ float chan_sum(const float* __restrict__ A, int C, si
 }
 
 // One thread per cell (block 32x8).  Writes destinations DX/DY for every
-// channel and MS (mass zeroed below 1e-10, times 1/(2s)^2 when exact) for the
-// plain gather; slots[0] takes the largest |dest - x| of a mass-carrying
-// cell, slots[1 + c] channel c's largest flow magnitude over all cells.
+// channel; slots[0] takes the largest |dest - x| of a mass-carrying cell,
+// slots[1 + c] channel c's largest flow magnitude over all cells.
 __global__ void __launch_bounds__(256) emb_flow(const float* __restrict__ A, const float* __restrict__ U,
                                                 const float* __restrict__ P, float* __restrict__ DX,
-                                                float* __restrict__ DY, float* __restrict__ MS, int C, int W, int H,
-                                                FlowParams fp, int* slots, int* status) {
+                                                float* __restrict__ DY, int C, int W, int H, FlowParams fp,
+                                                int* slots, int* status) {
     dep_enter();
     const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
     const bool in = x < W && y < H;
@@ -243,13 +242,11 @@ __global__ void __launch_bounds__(256) emb_flow(const float* __restrict__ A, con
             const float fy = __fsub_rn(__fmul_rn(oma, guy), __fmul_rn(alpha, gay));
             const float dx = __fadd_rn(float(x), __fmul_rn(fp.dt, fx));
             const float dy = __fadd_rn(float(y), __fmul_rn(fp.dt, fy));
-            float mass = A[size_t(c) * N + idx];
+            const float mass = A[size_t(c) * N + idx];
             bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
-            if (fabsf(mass) < 1e-10f) mass = 0.f;
-            if (mass != 0.f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(x)), fabsf(dy - float(y))));
+            if (fabsf(mass) >= 1e-10f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(x)), fabsf(dy - float(y))));
             DX[size_t(c) * N + idx] = dx;
             DY[size_t(c) * N + idx] = dy;
-            MS[size_t(c) * N + idx] = fp.area_pow2 ? __fmul_rn(mass, fp.inv_area) : mass;
             fmag = sqrtf(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)));  // NaN is skipped like f32::max
         }
         for (int o = 16; o > 0; o >>= 1) fmag = fmaxf(fmag, __shfl_xor_sync(0xffffffffu, fmag, o));
@@ -488,7 +485,7 @@ struct flp_embedded {
     float* A[2] = {nullptr, nullptr};
     float* P[2] = {nullptr, nullptr};  // C x NPAR x N, field planes
     int cur = 0, pcur = 0;
-    float *U = nullptr, *DX = nullptr, *DY = nullptr, *MS = nullptr;
+    float *U = nullptr, *DX = nullptr, *DY = nullptr;
     int* d_slots = nullptr;  // [0] displacement bound, [1 + c] flow magnitude of channel c
     int* d_status = nullptr;
     EKern* d_ek = nullptr;
@@ -532,7 +529,7 @@ struct flp_embedded {
         }
         mark(1);
         launch_dep(emb_flow, dim3((W + 31) / 32, (H + 7) / 8), dim3(256), size_t(0), st, a, (const float*)U, p, DX,
-                   DY, MS, C, W, H, fp, d_slots, d_status);
+                   DY, C, W, H, fp, d_slots, d_status);
         mark(2);
         if (enabled) {
             launch_dep(emb_gather, dim3((W + EG_T - 1) / EG_T, (H + EG_T - 1) / EG_T, C), dim3(256), gather_smem(),
@@ -540,7 +537,7 @@ struct flp_embedded {
                        temperature, (const int*)d_slots);
             pcur ^= 1;
         } else {
-            launch_gather_2d(DX, DY, MS, an, C, W, H, fp, d_slots, 1, st);
+            launch_gather_2d(DX, DY, a, an, C, W, H, fp, d_slots, 1, st);
         }
         mark(3);
         cke(cudaGetLastError(), "embedded step launch");
@@ -609,7 +606,7 @@ struct flp_embedded {
         for (auto& row : graph)
             for (auto& g : row)
                 if (g) cudaGraphExecDestroy(g);
-        void* ptrs[] = {A[0], A[1], P[0], P[1], U, DX, DY, MS, d_slots, d_status, d_ek, d_taps, d_partial, d_mass,
+        void* ptrs[] = {A[0], A[1], P[0], P[1], U, DX, DY, d_slots, d_status, d_ek, d_taps, d_partial, d_mass,
                         d_tw, d_S, d_T, d_KH, d_srcs, d_kslot, d_conv};
         for (void* q : ptrs)
             if (q) flp::dfree(q);
@@ -681,7 +678,6 @@ void emb_create(flp_embedded* h, const char* json) {
     h->U = ealloc<float>(CN);
     h->DX = ealloc<float>(CN);
     h->DY = ealloc<float>(CN);
-    h->MS = ealloc<float>(CN);
     h->d_slots = ealloc<int>(1 + h->C);
     h->d_status = ealloc<int>(1);
     cke(cudaMemset(h->d_slots, 0, sizeof(int) * (1 + h->C)), "memset");

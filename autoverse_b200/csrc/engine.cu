@@ -115,9 +115,9 @@ struct flp_propagator {
     bool direct_ok = false;
     FlowParams fp{};
     int* d_dmax = nullptr;   // largest |dest - x| of the step (float bits), reset by the step's first kernel
-    float* d_DX = nullptr;   // per-channel destinations and masses (C x N each)
+    float* d_DX = nullptr;   // per-channel destinations (C x N each)
     float* d_DY = nullptr;
-    float* d_MS = nullptr;
+    float* d_MS = nullptr;   // 3D only: per-channel source masses
     float* d_DZ = nullptr;   // 3D only
     int* d_status = nullptr;
     double2* d_partial = nullptr;
@@ -208,9 +208,9 @@ struct flp_propagator {
             mark(ns - 1);
             return;
         }
-        launch_flow_2d(a, U, d_DX, d_DY, d_MS, C, W, H, fp, d_dmax, d_status, st);
+        launch_flow_2d(a, U, d_DX, d_DY, C, W, H, fp, d_dmax, d_status, st);
         mark(ns - 2);
-        launch_gather_2d(d_DX, d_DY, d_MS, an, C, W, H, fp, d_dmax, gather_gby, st);
+        launch_gather_2d(d_DX, d_DY, a, an, C, W, H, fp, d_dmax, gather_gby, st);
         mark(ns - 1);
     }
 
@@ -594,8 +594,10 @@ static void create(const std::string& json, flp_propagator* h) {
     h->d_dmax = dalloc<int>(1);
     h->d_DX = dalloc<float>(CN);
     h->d_DY = dalloc<float>(CN);
-    h->d_MS = dalloc<float>(CN);
-    if (h->dims == 3) h->d_DZ = dalloc<float>(CN);
+    if (h->dims == 3) {
+        h->d_MS = dalloc<float>(CN);
+        h->d_DZ = dalloc<float>(CN);
+    }
     h->d_status = dalloc<int>(1);
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
     h->np = 256;

@@ -70,10 +70,11 @@ void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, con
 size_t flow_smem_bytes(int C);
 size_t gather_smem_bytes();
 void transport_2d_set_attributes();
-void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float* MS, int C, int W, int H,
+void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, int C, int W, int H,
                     const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st);
-// gby: destination rows per thread (1 or 2); both give the same bits.
-void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
+// A: the state the flow pass read (the sources' masses); gby: destination rows
+// per thread (1 or 2), both give the same bits.
+void launch_gather_2d(const float* DX, const float* DY, const float* A, float* Anext, int C, int W, int H,
                       const FlowParams& fp, const int* dmax_slot, int gby, cudaStream_t st);
 void launch_zero_ints(int* p, int n, cudaStream_t st);
 

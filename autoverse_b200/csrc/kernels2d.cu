@@ -114,14 +114,12 @@ void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, con
 size_t flow_smem_bytes(int C) { return flow_smem_bytes_inl(C); }
 size_t gather_smem_bytes() { return gather_smem_bytes_inl(1); }
 
-template <bool POW2>
 __global__ void __launch_bounds__(256) flow_2d(const float* __restrict__ A, const float* __restrict__ U,
-                                               float* __restrict__ DX, float* __restrict__ DY,
-                                               float* __restrict__ MS, int C, int W, int H, FlowParams fp,
-                                               int* dmax_slot, int* status) {
+                                               float* __restrict__ DX, float* __restrict__ DY, int C, int W, int H,
+                                               FlowParams fp, int* dmax_slot, int* status) {
     dep_enter();
     extern __shared__ __align__(16) float sm[];
-    flow_item<POW2>(sm, A, U, DX, DY, MS, C, W, H, fp, blockIdx.x * FL_W, blockIdx.y * FL_H, dmax_slot, status);
+    flow_item(sm, A, U, DX, DY, C, W, H, fp, blockIdx.x * FL_W, blockIdx.y * FL_H, dmax_slot, status);
 }
 
 // Tile of a gather block: the launch is one wave and a half, and tiles on the
@@ -146,64 +144,58 @@ __device__ __forceinline__ void gather_tile_of(int b, int ntx, int nty, int C, i
 
 template <bool POW2, int GBY>
 __global__ void __launch_bounds__(256, 3) gather_2d(const float* __restrict__ DX, const float* __restrict__ DY,
-                                                    const float* __restrict__ MS, float* __restrict__ Anext, int W,
+                                                    const float* __restrict__ A, float* __restrict__ Anext, int W,
                                                     int H, int C, FlowParams fp, const int* __restrict__ dmax_slot) {
     dep_enter();
     extern __shared__ __align__(16) float sm[];
     int tx, ty, c;
     gather_tile_of(blockIdx.x, (W + GT_W - 1) / GT_W, (H + gt_h(GBY) - 1) / gt_h(GBY), C, tx, ty, c);
     const size_t N = size_t(W) * H;
-    gather_item<POW2, GBY>(sm, DX + size_t(c) * N, DY + size_t(c) * N, MS + size_t(c) * N, Anext + size_t(c) * N, W,
+    gather_item<POW2, GBY>(sm, DX + size_t(c) * N, DY + size_t(c) * N, A + size_t(c) * N, Anext + size_t(c) * N, W,
                            H, fp, *dmax_slot, tx * GT_W, ty * gt_h(GBY));
 }
 
-template <int C, bool POW2>
+template <int C>
 __global__ void __launch_bounds__(256) flow_rows_2d(const float* __restrict__ A, const float* __restrict__ U,
-                                                    float* __restrict__ DX, float* __restrict__ DY,
-                                                    float* __restrict__ MS, int W, int H, FlowParams fp,
-                                                    int* dmax_slot, int* status) {
+                                                    float* __restrict__ DX, float* __restrict__ DY, int W, int H,
+                                                    FlowParams fp, int* dmax_slot, int* status) {
     dep_enter();
-    flow_rows_item<C, POW2>(A, U, DX, DY, MS, W, H, fp, blockIdx.x * 32, blockIdx.y * FR_H, dmax_slot, status);
+    flow_rows_item<C>(A, U, DX, DY, W, H, fp, blockIdx.x * 32, blockIdx.y * FR_H, dmax_slot, status);
 }
 
 // One compiled kernel per channel count 1..4 (the register-resident row walk),
 // the staged kernel for more channels.
-void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, float* MS, int C, int W, int H,
+void launch_flow_2d(const float* A, const float* U, float* DX, float* DY, int C, int W, int H,
                     const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
     if (C >= 1 && C <= 4) {
         const dim3 g((W + 31) / 32, (H + FR_H - 1) / FR_H);
-#define FR_CASE(c)                                                                                                 \
-        if (C == c) {                                                                                              \
-            if (fp.area_pow2) launch_dep(flow_rows_2d<c, true>, g, 256, 0, st, A, U, DX, DY, MS, W, H, fp, dmax_slot, status);   \
-            else launch_dep(flow_rows_2d<c, false>, g, 256, 0, st, A, U, DX, DY, MS, W, H, fp, dmax_slot, status);              \
-            return;                                                                                                \
+        switch (C) {
+            case 1: launch_dep(flow_rows_2d<1>, g, 256, 0, st, A, U, DX, DY, W, H, fp, dmax_slot, status); return;
+            case 2: launch_dep(flow_rows_2d<2>, g, 256, 0, st, A, U, DX, DY, W, H, fp, dmax_slot, status); return;
+            case 3: launch_dep(flow_rows_2d<3>, g, 256, 0, st, A, U, DX, DY, W, H, fp, dmax_slot, status); return;
+            default: launch_dep(flow_rows_2d<4>, g, 256, 0, st, A, U, DX, DY, W, H, fp, dmax_slot, status); return;
         }
-        FR_CASE(1) FR_CASE(2) FR_CASE(3) FR_CASE(4)
-#undef FR_CASE
     }
     dim3 grid((W + FL_W - 1) / FL_W, (H + FL_H - 1) / FL_H);
-    if (fp.area_pow2)
-        launch_dep(flow_2d<true>, grid, 256, flow_smem_bytes(C), st, A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
-    else
-        launch_dep(flow_2d<false>, grid, 256, flow_smem_bytes(C), st, A, U, DX, DY, MS, C, W, H, fp, dmax_slot, status);
+    launch_dep(flow_2d, grid, 256, flow_smem_bytes(C), st, A, U, DX, DY, C, W, H, fp, dmax_slot, status);
 }
 
-void launch_gather_2d(const float* DX, const float* DY, const float* MS, float* Anext, int C, int W, int H,
+void launch_gather_2d(const float* DX, const float* DY, const float* A, float* Anext, int C, int W, int H,
                       const FlowParams& fp, const int* dmax_slot, int gby, cudaStream_t st) {
     if (gby == 2) {
         const int tiles = ((W + GT_W - 1) / GT_W) * ((H + gt_h(2) - 1) / gt_h(2)) * C;
         const size_t smem = gather_smem_bytes_inl(2);
         if (fp.area_pow2)
-            launch_dep(gather_2d<true, 2>, dim3(tiles), 256, smem, st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+            launch_dep(gather_2d<true, 2>, dim3(tiles), 256, smem, st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
         else
-            launch_dep(gather_2d<false, 2>, dim3(tiles), 256, smem, st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+            launch_dep(gather_2d<false, 2>, dim3(tiles), 256, smem, st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
         return;
     }
     const int tiles = ((W + GT_W - 1) / GT_W) * ((H + gt_h(1) - 1) / gt_h(1)) * C;
     if (fp.area_pow2)
-        launch_dep(gather_2d<true, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+        launch_dep(gather_2d<true, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
     else
-        launch_dep(gather_2d<false, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, MS, Anext, W, H, C, fp, dmax_slot);
+        launch_dep(gather_2d<false, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
 }
 
 void transport_2d_set_attributes() {
@@ -211,8 +203,7 @@ void transport_2d_set_attributes() {
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
-    set((const void*)flow_2d<true>, flow_smem_bytes(64));
-    set((const void*)flow_2d<false>, flow_smem_bytes(64));
+    set((const void*)flow_2d, flow_smem_bytes(64));
     set((const void*)gather_2d<true, 1>, gather_smem_bytes());
     set((const void*)gather_2d<false, 1>, gather_smem_bytes());
     set((const void*)gather_2d<true, 2>, gather_smem_bytes_inl(2));

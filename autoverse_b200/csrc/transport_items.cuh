@@ -15,10 +15,11 @@ namespace flp {
 // Transport in two kernels.
 //
 // flow_2d (one thread per cell, all channels): channel sum, Sobel of the sum
-// and of U_c, alpha, flow, destination dest = x + dt*F (reintegration.rs:81-82)
-// and the mass (zeroed below 1e-10, reintegration.rs:76-78), written as three
-// planes per channel; it also publishes the largest |dest - x| of any cell
-// with mass.
+// and of U_c, alpha, flow and destination dest = x + dt*F
+// (reintegration.rs:81-82), written as two planes per channel; it also
+// publishes the largest |dest - x| of any cell with mass.  The gather takes a
+// source's mass from the state itself (source_mass: zero below 1e-10,
+// reintegration.rs:76-78).
 //
 // gather_2d (one block per 64x16 or 64x32 tile and channel, 4x1 or 4x2
 // destinations per thread): with D the largest
@@ -93,6 +94,16 @@ __device__ __forceinline__ int f2i_sat(float v) {
     return int(v);
 }
 
+// The mass a source at state value a deposits: zero below the reference's
+// 1e-10 threshold (reintegration.rs:76-78), pre-scaled by 1/(2s)^2 when that
+// factor is a power of two (then m * area equals the reference's
+// mass * (area / total_area) exactly).
+template <bool POW2>
+__device__ __forceinline__ float source_mass(float a, const FlowParams& fp) {
+    const float m = fabsf(a) < 1e-10f ? 0.f : a;
+    return POW2 ? __fmul_rn(m, fp.inv_area) : m;
+}
+
 // ------------------------------------------------------------- flow_2d ----
 constexpr int FL_W = 32, FL_H = 8;
 constexpr int FL_RW = FL_W + 2, FL_RH = FL_H + 2, FL_RC = FL_RW * FL_RH;  // region with the Sobel ring
@@ -115,10 +126,9 @@ __device__ __forceinline__ void block_max_atomic(float v, bool bad, int* slot) {
 }
 
 // One 32x8 tile of flow_2d; `sm` holds flow_smem_bytes(C).
-template <bool POW2>
-__device__ void flow_item(float* sm, const float* __restrict__ A, const float* __restrict__ U,
-                          float* __restrict__ DX, float* __restrict__ DY, float* __restrict__ MS, int C, int W, int H,
-                          const FlowParams& fp, int x0, int y0, int* dmax_slot, int* status) {
+inline __device__ void flow_item(float* sm, const float* __restrict__ A, const float* __restrict__ U,
+                                 float* __restrict__ DX, float* __restrict__ DY, int C, int W, int H,
+                                 const FlowParams& fp, int x0, int y0, int* dmax_slot, int* status) {
     float* as = sm;                    // C staged A planes
     float* us = sm + C * FL_RC;        // C staged U planes
     float* asum = sm + 2 * C * FL_RC;  // channel sum
@@ -164,13 +174,11 @@ __device__ void flow_item(float* sm, const float* __restrict__ A, const float* _
             const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
             const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
             const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
-            float mass = as[c * FL_RC + o + FL_RW + 1];
+            const float mass = as[c * FL_RC + o + FL_RW + 1];
             bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
-            if (fabsf(mass) < 1e-10f) mass = 0.f;
-            if (mass != 0.f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
+            if (fabsf(mass) >= 1e-10f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
             DX[size_t(c) * N + cell] = dx;
             DY[size_t(c) * N + cell] = dy;
-            MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
         }
     }
     if (status && __syncthreads_or(bad ? 1 : 0) && tid == 0) atomicOr(status, STATUS_NONFINITE);
@@ -189,11 +197,10 @@ __device__ void flow_item(float* sm, const float* __restrict__ A, const float* _
 constexpr int FR_RPT = 2;            // rows per thread of the single-world kernels
 constexpr int FR_H = 8 * FR_RPT;     // tile height: 8 warps of 32 columns
 
-template <int C, bool POW2, int RPT = FR_RPT>
+template <int C, int RPT = FR_RPT>
 __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, const float* __restrict__ U,
-                                               float* __restrict__ DX, float* __restrict__ DY,
-                                               float* __restrict__ MS, int W, int H, const FlowParams& fp, int x0,
-                                               int y0, int* dmax_slot, int* status) {
+                                               float* __restrict__ DX, float* __restrict__ DY, int W, int H,
+                                               const FlowParams& fp, int x0, int y0, int* dmax_slot, int* status) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const size_t N = size_t(W) * H;
@@ -268,13 +275,11 @@ __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, cons
             const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
             const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
             const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
-            float mass = ac[c];
+            const float mass = ac[c];
             bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
-            if (fabsf(mass) < 1e-10f) mass = 0.f;
-            if (mass != 0.f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
+            if (fabsf(mass) >= 1e-10f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
             DX[size_t(c) * N + cell] = dx;
             DY[size_t(c) * N + cell] = dy;
-            MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
         }
     }
     if (status && __syncthreads_or(bad ? 1 : 0) && threadIdx.x == 0) atomicOr(status, STATUS_NONFINITE);
@@ -300,19 +305,19 @@ static_assert(SR_W % 4 == 0, "source rows must stay 16-byte aligned");
 
 inline size_t gather_smem_bytes_inl(int gby) { return sizeof(float) * 5 * SR_W * sr_hmax(gby); }
 
-// Stage the dx, dy and m planes of an SR_W x SRH source region (columns
+// Stage the dx, dy and state planes of an SR_W x SRH source region (columns
 // colx[], rows rowy[]) into shared memory.  When W and the three base
 // pointers allow it, whole 16-byte chunks are copied: x0 - TP and W are
 // multiples of 4, so every chunk of 4 source columns is 4 contiguous, aligned
 // columns after the wrap.
 template <int SRH, int SW>
 __device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* smass, const float* __restrict__ DX,
-                                              const float* __restrict__ DY, const float* __restrict__ MS,
+                                              const float* __restrict__ DY, const float* __restrict__ AS,
                                               const int* colx, const int* rowy, int W) {
     const int tid = threadIdx.x;
     const bool vec = (W & 3) == 0 &&
                      ((reinterpret_cast<uintptr_t>(DX) | reinterpret_cast<uintptr_t>(DY) |
-                       reinterpret_cast<uintptr_t>(MS)) & 15) == 0;
+                       reinterpret_cast<uintptr_t>(AS)) & 15) == 0;
     if (vec) {
         constexpr int CH = SW / 4;
         for (int i = tid; i < 3 * SRH * CH; i += 256) {
@@ -321,7 +326,7 @@ __device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* sma
             const size_t idx = size_t(rowy[sy]) * W + colx[4 * c4];
             const int cell = sy * SW + 4 * c4;
             float* dst = k == 0 ? sdx + cell : (k == 1 ? sdy + cell : smass + cell);
-            cp_async16(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
+            cp_async16(dst, (k == 0 ? DX : (k == 1 ? DY : AS)) + idx);
         }
     } else {
         constexpr int NS = SW * SRH;
@@ -330,7 +335,7 @@ __device__ __forceinline__ void stage_sources(float* sdx, float* sdy, float* sma
             const int sy = cell / SW, sx = cell - sy * SW;
             const size_t idx = size_t(rowy[sy]) * W + colx[sx];
             float* dst = k == 0 ? sdx + cell : (k == 1 ? sdy + cell : smass + cell);
-            cp_async4(dst, (k == 0 ? DX : (k == 1 ? DY : MS)) + idx);
+            cp_async4(dst, (k == 0 ? DX : (k == 1 ? DY : AS)) + idx);
         }
     }
 }
@@ -543,7 +548,7 @@ __device__ __forceinline__ void gather_thread(bool cm, int& tx, int& ty) {
 // (inlined together, the batched gather spilled in its common RN = 1 path).
 template <int RN, bool POW2, int GBY>
 __device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
-                            const float* __restrict__ MS, float* __restrict__ out, int W, int H, const FlowParams& fp,
+                            const float* __restrict__ A, float* __restrict__ out, int W, int H, const FlowParams& fp,
                             int x0, int y0) {
     constexpr int SRH = gt_h(GBY) + 2 * RN + 1;
     const int tid = threadIdx.x;
@@ -561,14 +566,18 @@ __device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX
     if (tid < SR_W) colx[tid] = wrap_near(x0 - TP + tid, W);
     else if (tid < SR_W + SRH) rowy[tid - SR_W] = wrap_near(y0 - RN + (tid - SR_W), H);
     __syncthreads();
-    // stage destinations and masses (dx -> xmin in place, dy -> ymin in place)
-    if (cm) stage_sources<SRH, SR_W>(sxmin, symin, smass, DX, DY, MS, colx, rowy, W);
-    else stage_sources<SRH, SR_W - 4>(sxmin, symin, smass, DX, DY, MS, colx, rowy, W);
+    // stage destinations and states (dx -> xmin in place, dy -> ymin in place,
+    // state -> source mass in place)
+    if (cm) stage_sources<SRH, SR_W>(sxmin, symin, smass, DX, DY, A, colx, rowy, W);
+    else stage_sources<SRH, SR_W - 4>(sxmin, symin, smass, DX, DY, A, colx, rowy, W);
     cp_async_wait_all();
     __syncthreads();
     for (int i = 4 * tid; i < sw * SRH; i += 1024) {
         const float4 dx = *reinterpret_cast<const float4*>(sxmin + i);
         const float4 dy = *reinterpret_cast<const float4*>(symin + i);
+        const float4 a = *reinterpret_cast<const float4*>(smass + i);
+        *reinterpret_cast<float4*>(smass + i) = make_float4(source_mass<POW2>(a.x, fp), source_mass<POW2>(a.y, fp),
+                                                            source_mass<POW2>(a.z, fp), source_mass<POW2>(a.w, fp));
         *reinterpret_cast<float4*>(sxmin + i) =
             make_float4(__fsub_rn(dx.x, s), __fsub_rn(dx.y, s), __fsub_rn(dx.z, s), __fsub_rn(dx.w, s));
         *reinterpret_cast<float4*>(sxmax + i) =
@@ -585,11 +594,12 @@ __device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX
 }
 
 // Reintegrated mass at destination (X, Y) for any window, sources read from
-// the destination planes in global memory.  Handles the nearest-cell mode,
-// the reference's [-W, 2W] cell clamp, and windows wider than the grid.
+// the destination and state planes in global memory.  Handles the
+// nearest-cell mode, the reference's [-W, 2W] cell clamp, and windows wider
+// than the grid.
 template <bool POW2>
 __device__ float gather_generic_2d(const float* __restrict__ DX, const float* __restrict__ DY,
-                                   const float* __restrict__ MS, int W, int H, int X, int Y, int R,
+                                   const float* __restrict__ A, int W, int H, int X, int Y, int R,
                                    const FlowParams& fp) {
     float acc = 0.f;
     for (int jy = 0; jy <= 2 * R; ++jy) {
@@ -601,7 +611,7 @@ __device__ float gather_generic_2d(const float* __restrict__ DX, const float* __
             const int xw = wrap_coord(X + kx, W);
             const int ix = xw - kx;
             const size_t src = size_t(yw) * W + xw;
-            const float m = MS[src];
+            const float m = source_mass<POW2>(A[src], fp);
             if (m == 0.f) continue;
             const float dx = DX[src], dy = DY[src];
             if (fp.point_mode) {
@@ -626,19 +636,20 @@ __device__ float gather_generic_2d(const float* __restrict__ DX, const float* __
 }
 
 // One 64 x (16 * GBY) tile of one channel of gather_2d; `sm` holds
-// gather_smem_bytes_inl(GBY).  dxc/dyc/msc/out are that channel's planes.
+// gather_smem_bytes_inl(GBY).  dxc/dyc are that channel's destination planes,
+// ac its state plane (the sources' masses), out its next-state plane.
 template <bool POW2, int GBY>
 __device__ void gather_item(float* sm, const float* __restrict__ dxc, const float* __restrict__ dyc,
-                            const float* __restrict__ msc, float* __restrict__ out, int W, int H,
+                            const float* __restrict__ ac, float* __restrict__ out, int W, int H,
                             const FlowParams& fp, int dmax_bits, int x0, int y0) {
     const int RN = window_from_dmax(dmax_bits, fp, max(W, H));
     const bool fast = RN <= RN_MAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && !fp.point_mode;
     if (fast) {
         switch (RN) {
-            case 0: gather_body<0, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
-            case 1: gather_body<1, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
-            case 2: gather_body<2, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
-            default: gather_body<3, POW2, GBY>(sm, dxc, dyc, msc, out, W, H, fp, x0, y0); break;
+            case 0: gather_body<0, POW2, GBY>(sm, dxc, dyc, ac, out, W, H, fp, x0, y0); break;
+            case 1: gather_body<1, POW2, GBY>(sm, dxc, dyc, ac, out, W, H, fp, x0, y0); break;
+            case 2: gather_body<2, POW2, GBY>(sm, dxc, dyc, ac, out, W, H, fp, x0, y0); break;
+            default: gather_body<3, POW2, GBY>(sm, dxc, dyc, ac, out, W, H, fp, x0, y0); break;
         }
         return;
     }
@@ -650,7 +661,7 @@ __device__ void gather_item(float* sm, const float* __restrict__ dxc, const floa
         for (int i = 0; i < 4; ++i) {
             const int X = x0 + 4 * tx + i;
             if (X < W && Y < H)
-                out[size_t(Y) * W + X] = gather_generic_2d<POW2>(dxc, dyc, msc, W, H, X, Y, RN + 1, fp);
+                out[size_t(Y) * W + X] = gather_generic_2d<POW2>(dxc, dyc, ac, W, H, X, Y, RN + 1, fp);
         }
     }
 }
