@@ -333,12 +333,13 @@ __global__ void __launch_bounds__(256) k_c2r_raw_t(const float2* __restrict__ T,
 }
 
 // ---- warp-synchronous single-world kernels (fft_warp.cuh)
-template <int M, int WPC>
+// COPY: the planes read (A may be mapped host memory) are also written to Acopy.
+template <int M, int WPC, bool COPY = false>
 __global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_r2c_w(const float* __restrict__ A, float2* __restrict__ S,
                                                                const int* __restrict__ srcs, int H,
                                                                const float2* __restrict__ twM,
                                                                const float2* __restrict__ twW, int* reset_slot,
-                                                               int nreset) {
+                                                               int nreset, float* __restrict__ Acopy) {
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
@@ -346,8 +347,9 @@ __global__ void __launch_bounds__(32 * WPC, 16 / WPC) k_r2c_w(const float* __res
     const int slot = blockIdx.y;
     const int c = srcs ? srcs[slot] : slot;
     constexpr int W = 2 * M, Wc = M + 1;
-    r2c_rows_witem<M, WPC>(fsm, A + size_t(c) * W * H, S + size_t(slot) * Wc * H, H,
-                           blockIdx.x * WRowCfg<M, WPC>::NRC, twM, twW);
+    const size_t off = size_t(c) * W * H;
+    r2c_rows_witem<M, WPC, COPY>(fsm, A + off, S + size_t(slot) * Wc * H, H, blockIdx.x * WRowCfg<M, WPC>::NRC, twM,
+                                 twW, COPY ? Acopy + off : nullptr);
 }
 
 // blockIdx.y: a source slot (share) or a kernel (one transform per kernel).
@@ -443,6 +445,7 @@ void fft2d_set_attributes(size_t max_bytes) {
     set((const void*)fft_rows_c2r_growth);
 #define X(n) set((const void*)k_r2c_t<n>); set((const void*)k_c2r_t<n>); set((const void*)k_c2r_raw_t<n>);     \
     set((const void*)k_r2c_w<n, 4>); set((const void*)k_r2c_w<n, 8>); set((const void*)k_c2r_w<n, 4>);            \
+    set((const void*)k_r2c_w<n, 4, true>); set((const void*)k_r2c_w<n, 8, true>);                                  \
     set((const void*)k_c2r_w<n, 8>); set((const void*)k_c2r_raw_w<n, 8>); set((const void*)k_c2r_raw_w<n, 4>);
     FLP_ROW_SIZES(X)
 #undef X
@@ -452,24 +455,41 @@ void fft2d_set_attributes(size_t max_bytes) {
 #undef X
 }
 
+bool fft_rows_copy_width(int W) {
+    const int M = W / 2;
+#define X(n) if (W % 2 == 0 && M == n) return true;
+    FLP_ROW_SIZES(X)
+#undef X
+    return false;
+}
+
 void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
-                    int* reset_slot, int nreset, cudaStream_t st) {
+                    int* reset_slot, int nreset, cudaStream_t st, float* Acopy) {
     const int M = W / 2;
 #define X(n)                                                                                                 \
     if (M == n) {                                                                                            \
         if (g.wpc_r2c == 4) {                                                                                \
             dim3 grid((H + WRowCfg<n, 4>::NRC - 1) / WRowCfg<n, 4>::NRC, nsrc);                              \
-            launch_dep(k_r2c_w<n, 4>, grid, 128, WRowCfg<n, 4>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW,     \
-                       reset_slot, nreset);                                                                  \
+            if (Acopy)                                                                                       \
+                launch_dep(k_r2c_w<n, 4, true>, grid, 128, WRowCfg<n, 4>::smem_r2c, st, A, S, srcs, H, g.twM,  \
+                           g.twW, reset_slot, nreset, Acopy);                                                \
+            else                                                                                             \
+                launch_dep(k_r2c_w<n, 4>, grid, 128, WRowCfg<n, 4>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW, \
+                           reset_slot, nreset, Acopy);                                                       \
         } else {                                                                                             \
             dim3 grid((H + WRowCfg<n, 8>::NRC - 1) / WRowCfg<n, 8>::NRC, nsrc);                              \
-            launch_dep(k_r2c_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW,     \
-                       reset_slot, nreset);                                                                  \
+            if (Acopy)                                                                                       \
+                launch_dep(k_r2c_w<n, 8, true>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, A, S, srcs, H, g.twM,  \
+                           g.twW, reset_slot, nreset, Acopy);                                                \
+            else                                                                                             \
+                launch_dep(k_r2c_w<n, 8>, grid, 256, WRowCfg<n, 8>::smem_r2c, st, A, S, srcs, H, g.twM, g.twW, \
+                           reset_slot, nreset, Acopy);                                                       \
         }                                                                                                    \
         return;                                                                                              \
     }
     FLP_ROW_SIZES(X)
 #undef X
+    if (Acopy) throw std::runtime_error("row transform with a plane copy: no warp-synchronous kernel for this width");
     launch_fft_r2c_legacy(A, S, srcs, nsrc, W, H, g, reset_slot, nreset, st);
 }
 

@@ -239,9 +239,13 @@ struct WColCfg {
 // NRC rows of one real plane x (width 2M) -> half spectra written transposed,
 // Sc[kx][y] for kx <= M.  z[n] = x[2n] + i x[2n+1]; X[k] = (Z[k] + conj
 // Z[M-k]) / 2 + e^{-2 pi i k / 2M} (Z[k] - conj Z[M-k]) / 2i.
-template <int M, int WPC>
+// With COPY, every row value read is also written to xcopy at the same
+// offset (the first stage reads each value of a row exactly once): a plane
+// read from mapped host memory leaves its device copy behind.
+template <int M, int WPC, bool COPY = false>
 __device__ void r2c_rows_witem(float2* sm, const float* __restrict__ x, float2* __restrict__ Sc, int H, int y0,
-                               const float2* __restrict__ twM, const float2* __restrict__ twW) {
+                               const float2* __restrict__ twM, const float2* __restrict__ twW,
+                               float* __restrict__ xcopy = nullptr) {
     using P = WPlan<M>;
     constexpr int NLW = P::NLW, LS = P::LS, Wc = M + 1, W = 2 * M, NRC = WRowCfg<M, WPC>::NRC;
     constexpr int XS = WRowCfg<M, WPC>::XS;
@@ -252,7 +256,11 @@ __device__ void r2c_rows_witem(float2* sm, const float* __restrict__ x, float2* 
     const int row0 = warp * NLW;
     auto ld0 = [&](int, int, int line, int n) -> float2 {
         const int y = y0 + row0 + line;
-        return y < H ? *reinterpret_cast<const float2*>(x + size_t(y) * W + 2 * n) : make_float2(0.f, 0.f);
+        if (y >= H) return make_float2(0.f, 0.f);
+        const size_t o = size_t(y) * W + 2 * n;
+        const float2 v = *reinterpret_cast<const float2*>(x + o);
+        if constexpr (COPY) *reinterpret_cast<float2*>(xcopy + o) = v;
+        return v;
     };
     float2* z = ((P::nst() - 1) % 2 == 0) ? a : b;  // the buffer the last stage writes
     auto stz = [z](int, int, int line, int n, float2 v) { z[line * LS + pad8(n)] = v; };

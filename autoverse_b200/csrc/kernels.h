@@ -85,8 +85,12 @@ void launch_mass_fp64(const float* A, size_t n, double2* partial, int np, double
 size_t fft_rows_smem(int W, int NR, bool with_u);
 size_t fft_cols_smem(int H, int NC);
 void fft2d_set_attributes(size_t max_bytes);
+// Acopy (optional, widths with a warp-synchronous kernel only): the source
+// planes read are also written there, at the same offsets (A may then be
+// mapped host memory and Acopy its device copy).
 void launch_fft_r2c(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
-                    int* reset_slot, int nreset, cudaStream_t st);
+                    int* reset_slot, int nreset, cudaStream_t st, float* Acopy = nullptr);
+bool fft_rows_copy_width(int W);  // whether launch_fft_r2c takes Acopy for this width
 void launch_fft_cols(const float2* S, const float2* KH, float2* T, const int* slot_of_kernel, int K, int W, int H,
                      const FftGeom& g, int mode, float scale, cudaStream_t st);
 void launch_fft_r2c_legacy(const float* A, float2* S, const int* srcs, int nsrc, int W, int H, const FftGeom& g,
@@ -121,9 +125,10 @@ size_t flow3d_smem_bytes(int C, int nz);
 int flow3d_max_channels();
 size_t gather3d_smem_bytes();
 void transport_3d_set_attributes();
-void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
+void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, int C, int W, int H,
                     int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st);
-void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
+// A: the state the flow pass read (the sources' masses)
+void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* A, float* Anext, int C, int W,
                       int H, int D, const FlowParams& fp, const int* dmax_slot, cudaStream_t st);
 
 }  // namespace flp

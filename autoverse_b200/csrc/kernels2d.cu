@@ -192,10 +192,11 @@ void launch_gather_2d(const float* DX, const float* DY, const float* A, float* A
         return;
     }
     const int tiles = ((W + GT_W - 1) / GT_W) * ((H + gt_h(1) - 1) / gt_h(1)) * C;
+    const size_t smem = gather_smem_bytes();
     if (fp.area_pow2)
-        launch_dep(gather_2d<true, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
+        launch_dep(gather_2d<true, 1>, dim3(tiles), 256, smem, st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
     else
-        launch_dep(gather_2d<false, 1>, dim3(tiles), 256, gather_smem_bytes(), st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
+        launch_dep(gather_2d<false, 1>, dim3(tiles), 256, smem, st, DX, DY, A, Anext, W, H, C, fp, dmax_slot);
 }
 
 void transport_2d_set_attributes() {

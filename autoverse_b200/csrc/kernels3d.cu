@@ -70,11 +70,11 @@ __device__ __forceinline__ void sobel3_run(const Win3& w, float (&gx)[NZ], float
     }
 }
 
-template <bool POW2, int F3_NZ>
+template <int F3_NZ>
 __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, const float* __restrict__ U,
                                                float* __restrict__ DX, float* __restrict__ DY,
-                                               float* __restrict__ DZ, float* __restrict__ MS, int C, int W, int H,
-                                               int D, FlowParams fp, int* dmax_slot, int* status) {
+                                               float* __restrict__ DZ, int C, int W, int H, int D, FlowParams fp,
+                                               int* dmax_slot, int* status) {
     dep_enter();
     constexpr int F3_NP = F3_NZ + 2, F3_RC = f3_rc(F3_NZ);
     extern __shared__ __align__(16) float sm[];
@@ -145,15 +145,13 @@ __global__ void __launch_bounds__(256) flow_3d(const float* __restrict__ A, cons
                 const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
                 const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
                 const float dz = __fadd_rn(float(z), __fmul_rn(fp.dt, fz));
-                float mass = as[c * F3_RC + (k + 1) * F3_PL + o + F3_RW + 1];
+                const float mass = as[c * F3_RC + (k + 1) * F3_PL + o + F3_RW + 1];
                 bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy) && isfinite(dz));
-                if (fabsf(mass) < 1e-10f) mass = 0.f;
-                if (mass != 0.f)
+                if (fabsf(mass) >= 1e-10f)
                     dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fmaxf(fabsf(dy - float(Y)), fabsf(dz - float(z)))));
                 DX[size_t(c) * N + cell] = dx;
                 DY[size_t(c) * N + cell] = dy;
                 DZ[size_t(c) * N + cell] = dz;
-                MS[size_t(c) * N + cell] = POW2 ? __fmul_rn(mass, fp.inv_area) : mass;
             }
         }
     }
@@ -224,7 +222,7 @@ __device__ __forceinline__ void rotate_left(float (&t)[NW], int r) {
 // One 32x8 block of destinations in plane Z of one channel.
 template <int RN, bool POW2>
 __device__ void gather3d_plane(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
-                               const float* __restrict__ DZ, const float* __restrict__ MS, float* __restrict__ out,
+                               const float* __restrict__ DZ, const float* __restrict__ A, float* __restrict__ out,
                                int W, int H, int D, int Z, const FlowParams& fp) {
     constexpr int SW = G3_W + 2 * RN + 1, SH = G3_H + 2 * RN + 1, SD = 2 * RN + 2, PL = SW * SH, NC = PL * SD;
     float* sx = sm;
@@ -243,10 +241,12 @@ __device__ void gather3d_plane(float* sm, const float* __restrict__ DX, const fl
         const int pz = cell / PL, r = cell - pz * PL;
         const int ly = r / SW, lx = r - ly * SW;
         const size_t idx = (size_t(plz[pz]) * H + rowy[ly]) * W + colx[lx];
-        const float* src = k == 0 ? DX : (k == 1 ? DY : (k == 2 ? DZ : MS));
+        const float* src = k == 0 ? DX : (k == 1 ? DY : (k == 2 ? DZ : A));
         cp_async4(sm + i, src + idx);
     }
     cp_async_wait_all();
+    __syncthreads();
+    for (int i = tid; i < NC; i += 256) smm[i] = source_mass<POW2>(smm[i], fp);  // state -> source mass
     __syncthreads();
     const int lx = tid & (G3_W - 1), ly = tid / G3_W;
     const int X = x0 + lx, Y = y0 + ly;
@@ -283,7 +283,7 @@ __device__ void gather3d_plane(float* sm, const float* __restrict__ DX, const fl
 // nearest-cell mode and the reference's [-W, 2W] cell clamps.
 template <bool POW2>
 __device__ float gather3d_generic(const float* __restrict__ DX, const float* __restrict__ DY,
-                                  const float* __restrict__ DZ, const float* __restrict__ MS, int W, int H, int D,
+                                  const float* __restrict__ DZ, const float* __restrict__ A, int W, int H, int D,
                                   int X, int Y, int Z, int R, const FlowParams& fp) {
     float acc = 0.f;
     for (int jz = 0; jz <= 2 * R; ++jz) {
@@ -296,7 +296,7 @@ __device__ float gather3d_generic(const float* __restrict__ DX, const float* __r
                 const int kx = rotated_offset(jx, X, R, W);
                 const int xw = wrap_coord(X + kx, W), ix = xw - kx;
                 const size_t src = (size_t(zw) * H + yw) * W + xw;
-                const float m = MS[src];
+                const float m = source_mass<POW2>(A[src], fp);
                 if (m == 0.f) continue;
                 const float dx = DX[src], dy = DY[src], dz = DZ[src];
                 if (fp.point_mode) {
@@ -340,7 +340,7 @@ struct March3 {
 
 template <int RN, bool POW2>
 __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const float* __restrict__ DY,
-                               const float* __restrict__ DZ, const float* __restrict__ MS, float* __restrict__ out,
+                               const float* __restrict__ DZ, const float* __restrict__ A, float* __restrict__ out,
                                int W, int H, int D, int z0, int nz, const FlowParams& fp) {
     using M = March3<RN>;
     constexpr int SW = M::SW, SH = M::SH, NS = M::NS, NW = M::NW, SD = M::SD;
@@ -366,7 +366,7 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
                 r[0][p] = DX[idx];
                 r[1][p] = DY[idx];
                 r[2][p] = DZ[idx];
-                r[3][p] = MS[idx];
+                r[3][p] = A[idx];
             }
         }
     };
@@ -383,7 +383,7 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
             if (i < NS) {
                 const int ly = i / SW, lx = i - ly * SW;
                 const int xw = colx[lx], yw = rowy[ly];
-                Mm[i] = r[3][p];
+                Mm[i] = source_mass<POW2>(r[3][p], fp);
                 const float xa = __fsub_rn(r[0][p], s), xb = __fadd_rn(r[0][p], s);
                 const float ya = __fsub_rn(r[1][p], s), yb = __fadd_rn(r[1][p], s);
                 const float za = __fsub_rn(r[2][p], s), zb = __fadd_rn(r[2][p], s);
@@ -455,7 +455,7 @@ inline size_t gather3d_dyn_smem() {
 // Grid: (x tiles, y tiles, channels * z chunks of G3_NZ planes).
 template <bool POW2>
 __global__ void __launch_bounds__(256) gather_3d(const float* __restrict__ DX, const float* __restrict__ DY,
-                                                 const float* __restrict__ DZ, const float* __restrict__ MS,
+                                                 const float* __restrict__ DZ, const float* __restrict__ A,
                                                  float* __restrict__ Anext, int C, int W, int H, int D, FlowParams fp,
                                                  const int* __restrict__ dmax_slot) {
     dep_enter();
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(256) gather_3d(const float* __restrict__ DX, c
     const size_t N = size_t(W) * H * D, off = size_t(c) * N;
     const int RN = window_from_dmax(*dmax_slot, fp, max(max(W, H), D));
     const bool fast = RN <= G3_RNMAX && 2 * RN + 2 <= W && 2 * RN + 2 <= H && 2 * RN + 2 <= D && !fp.point_mode;
-    const float *dx = DX + off, *dy = DY + off, *dz = DZ + off, *ms = MS + off;
+    const float *dx = DX + off, *dy = DY + off, *dz = DZ + off, *ms = A + off;  // ms: the state (source masses)
     float* o = Anext + off;
     if (fast && RN == 0) {
         gather3d_march<0, POW2>(sm, dx, dy, dz, ms, o, W, H, D, z0, nz, fp);
@@ -491,27 +491,22 @@ __global__ void __launch_bounds__(256) gather_3d(const float* __restrict__ DX, c
 
 size_t gather3d_smem_bytes() { return gather3d_dyn_smem(); }
 
-void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, float* MS, int C, int W, int H,
-                    int D, const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
+void launch_flow_3d(const float* A, const float* U, float* DX, float* DY, float* DZ, int C, int W, int H, int D,
+                    const FlowParams& fp, int* dmax_slot, int* status, cudaStream_t st) {
     const int nz = flow3d_nz(C);
     dim3 grid((W + F3_W - 1) / F3_W, (H + F3_H - 1) / F3_H, (D + nz - 1) / nz);
     const size_t smem = flow3d_smem_bytes(C, nz);
-    if (nz == 4) {
-        if (fp.area_pow2) launch_dep(flow_3d<true, 4>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
-        else launch_dep(flow_3d<false, 4>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
-    } else {
-        if (fp.area_pow2) launch_dep(flow_3d<true, 2>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
-        else launch_dep(flow_3d<false, 2>, grid, 256, smem, st, A, U, DX, DY, DZ, MS, C, W, H, D, fp, dmax_slot, status);
-    }
+    if (nz == 4) launch_dep(flow_3d<4>, grid, 256, smem, st, A, U, DX, DY, DZ, C, W, H, D, fp, dmax_slot, status);
+    else launch_dep(flow_3d<2>, grid, 256, smem, st, A, U, DX, DY, DZ, C, W, H, D, fp, dmax_slot, status);
 }
 
-void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* MS, float* Anext, int C, int W,
+void launch_gather_3d(const float* DX, const float* DY, const float* DZ, const float* A, float* Anext, int C, int W,
                       int H, int D, const FlowParams& fp, const int* dmax_slot, cudaStream_t st) {
     dim3 grid((W + G3_W - 1) / G3_W, (H + G3_H - 1) / G3_H, C * ((D + G3_NZ - 1) / G3_NZ));
     if (fp.area_pow2)
-        launch_dep(gather_3d<true>, grid, 256, gather3d_smem_bytes(), st, DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
+        launch_dep(gather_3d<true>, grid, 256, gather3d_smem_bytes(), st, DX, DY, DZ, A, Anext, C, W, H, D, fp, dmax_slot);
     else
-        launch_dep(gather_3d<false>, grid, 256, gather3d_smem_bytes(), st, DX, DY, DZ, MS, Anext, C, W, H, D, fp, dmax_slot);
+        launch_dep(gather_3d<false>, grid, 256, gather3d_smem_bytes(), st, DX, DY, DZ, A, Anext, C, W, H, D, fp, dmax_slot);
 }
 
 void transport_3d_set_attributes() {
@@ -520,10 +515,8 @@ void transport_3d_set_attributes() {
         cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
     const int c4 = int((F3_SMEM_MAX / (sizeof(float) * f3_rc(4)) - 1) / 2);  // most channels with four planes
-    set((const void*)flow_3d<true, 4>, flow3d_smem_bytes(c4, 4));
-    set((const void*)flow_3d<false, 4>, flow3d_smem_bytes(c4, 4));
-    set((const void*)flow_3d<true, 2>, flow3d_smem_bytes(flow3d_max_channels(), 2));
-    set((const void*)flow_3d<false, 2>, flow3d_smem_bytes(flow3d_max_channels(), 2));
+    set((const void*)flow_3d<4>, flow3d_smem_bytes(c4, 4));
+    set((const void*)flow_3d<2>, flow3d_smem_bytes(flow3d_max_channels(), 2));
     set((const void*)gather_3d<true>, gather3d_smem_bytes());
     set((const void*)gather_3d<false>, gather3d_smem_bytes());
 }

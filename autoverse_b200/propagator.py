@@ -219,14 +219,20 @@ class CudaPropagator:
 
     def step_host(self, channels: np.ndarray, steps: int = 1, time: float | None = None,
                   step: int | None = None) -> tuple[float, int]:
-        """Advance a state held in host memory in place (flp_step_host): copy in,
+        """Advance a state held in host memory in place (flp_step_host): in,
         `steps` steps, copy back, one synchronisation.  `channels` must be a
-        C-contiguous float32 array of channels*cells values (a PinnedBuffer's
-        array makes both copies DMA transfers).  Returns the advanced (time, step)."""
+        C-contiguous float32 array of channels*cells values; with a
+        PinnedBuffer's array the copy back is a DMA transfer and, on the 2D FFT
+        path, the first step's row transforms read the state straight from the
+        pinned buffer (pageable memory is copied in).  Returns the advanced
+        (time, step)."""
         if channels.dtype != np.float32 or not channels.flags["C_CONTIGUOUS"] or not channels.flags["WRITEABLE"]:
             raise ValueError("channels must be a writeable C-contiguous float32 array")
-        t = C.c_float(self.info().time if time is None else time)
-        s = C.c_uint64(self.info().step if step is None else step)
+        if time is None or step is None:
+            i = self.info()
+            time = i.time if time is None else time
+            step = i.step if step is None else step
+        t, s = C.c_float(time), C.c_uint64(step)
         nat.check(nat.lib().flp_step_host(self._h, channels.ctypes.data, channels.size, C.byref(t), C.byref(s),
                                           C.c_uint64(int(steps))))
         self._bound_state = None

@@ -96,7 +96,10 @@ FLP_API int flp_run(flp_propagator* h, uint64_t n);
  * copies state[channels*depth*height*width] in (with *time and *step when
  * given), advances `steps` steps, and copies the state and the advanced clock
  * back into the same buffers; one stream synchronisation.  With `state` in
- * pinned memory (flp_host_alloc) both copies are DMA transfers. */
+ * pinned memory (flp_host_alloc or any device-addressable page-locked buffer)
+ * the copy back is a DMA transfer and, on the 2D FFT path, the first step's
+ * row transforms read the source channels straight from the buffer instead of
+ * a copy in; the results are the same bits either way. */
 FLP_API int flp_step_host(flp_propagator* h, float* state, size_t n, float* time, uint64_t* step, uint64_t steps);
 
 /* Wait for the handle's stream; reports device-side status words

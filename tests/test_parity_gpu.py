@@ -192,6 +192,50 @@ def test_step_host_matches_device_steps():
             p2.step_host(host.astype(np.float64))
 
 
+def _one_source_case():
+    """C=2 with every kernel reading channel 0: channel 1 is no source."""
+    rng = np.random.default_rng(15)
+    ks = [wl.kernel(0, t, wl.random_rings(rng, 1, 2), weight=0.7, mu=0.18, sigma=0.03) for t in (0, 1)]
+    cfg = wl.config(128, 64, 2, ks, kernel_radius=9)
+    st = np.zeros((2, 128 * 64), np.float32)
+    st[:, 20 * 128 + 30: 20 * 128 + 60] = rng.random((2, 30), dtype=np.float32)
+    st[:, 40 * 128 + 70: 40 * 128 + 100] = rng.random((2, 30), dtype=np.float32)
+    return cfg, st
+
+
+@pytest.mark.parametrize("case", ["species96x64", "one_source", "width80"])
+@pytest.mark.parametrize("steps", [1, 2, 3, 11])
+def test_step_host_pinned_matches_pageable_and_device(case, steps):
+    """On the FFT path a pinned host state is read by the first step's row
+    transforms directly (widths with a warp-synchronous row transform; channels
+    that no kernel reads are copied); pageable memory, and widths without that
+    transform, are copied in.  Every form gives the device-resident run's bits
+    and the same clock."""
+    if case == "species96x64":
+        cfg, st = species_case(seed=16)
+    elif case == "one_source":
+        cfg, st = _one_source_case()
+    else:
+        cfg, st = species_case(W=80, H=48, C=2, seed=17)
+    with fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT) as p1, fl.CudaPropagator(cfg, conv_mode=fl.CONV_FFT) as p2:
+        p1.write_state(st)
+        p1.run_device(steps)
+        ref = p1.read_state()
+        pin = fl.propagator.PinnedBuffer(st.shape)
+        pin.array[...] = st
+        t, n = p2.step_host(pin.array, steps=steps, time=0.0, step=0)
+        assert np.array_equal(pin.array, ref)
+        assert n == steps and t == pytest.approx(p1.info().time, rel=0, abs=0)
+        assert np.array_equal(p2.read_state(), ref)  # the device state follows the host one
+        host = st.copy()
+        p2.step_host(host, steps=steps, time=0.0, step=0)
+        assert np.array_equal(host, ref)
+        # a further call continues from the host buffer, not from the device state
+        pin.array[...] = st
+        p2.step_host(pin.array, steps=steps, time=0.0, step=0)
+        assert np.array_equal(pin.array, ref)
+
+
 def nat_step(p):
     from autoverse_b200 import _native as nat
     nat.check(nat.lib().flp_step(p._h))
