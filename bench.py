@@ -128,12 +128,12 @@ def stage_bytes(cfg, stage):
         "fft_z_conv": (nsrc + 2 * K) * spec,
         "fft_y_inv": 2 * K * spec,
         "fft_x_c2r_growth": K * spec + C * N * 4,
-        "flow_3d": 2 * C * N * 4 + 4 * C * N * 4,
+        "flow_3d": 2 * C * N * 4 + 3 * C * N * 4,
         "gather_3d": 4 * C * N * 4 + C * N * 4,
         "fft_rows_r2c": nsrc * N * 4 + nsrc * spec,
         "fft_cols_conv": (nsrc + 2 * K) * spec,
         "fft_rows_c2r_growth": K * spec + C * N * 4,
-        "flow_2d": 2 * C * N * 4 + 3 * C * N * 4,
+        "flow_2d": 2 * C * N * 4 + 2 * C * N * 4,
         "gather_2d": 3 * C * N * 4 + C * N * 4,
         "conv_direct_growth_2d": nsrc * N * 4 + C * N * 4,
     }.get(stage)
