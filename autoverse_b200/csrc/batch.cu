@@ -150,15 +150,41 @@ struct Pools {
     const float2* tw;
 };
 
-// Claim the next item of a queue; -1 when the queue is drained.
-__device__ __forceinline__ int next_item(int* counter, int n) {
-    __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
-    __syncthreads();
-    const int it = s_item;
-    __syncthreads();
-    return it < n ? it : -1;
-}
+// A persistent CTA's cursor on a work queue.  Item k's index sits in
+// slot[k & 1]; thread 0 claims the following item (atomicAdd on the queue's
+// counter) while item k is processed and publishes it at the item's end, so
+// the atomic's round trip is hidden behind the item and one barrier per item
+// suffices: a slot is rewritten only after every thread has passed the
+// barrier that followed its last read.  Each CTA claims up to two indices past
+// the end; the counters are rearmed every step.
+struct QueueCursor {
+    int* counter;
+    int n, k, ahead;
+    int* slot;  // two shared ints
+    __device__ __forceinline__ QueueCursor(int* c, int n_, int* s) : counter(c), n(n_), k(0), ahead(0), slot(s) {
+        if (threadIdx.x == 0) {
+            slot[0] = atomicAdd(counter, 1);
+            ahead = atomicAdd(counter, 1);
+        }
+        __syncthreads();
+    }
+    // The current item, -1 when the queue is drained (uniform over the CTA).
+    __device__ __forceinline__ int item() const {
+        const int it = slot[k & 1];
+        return it < n ? it : -1;
+    }
+    // Publish the claimed item and claim the one after it; call at the end of
+    // an item by every thread.
+    __device__ __forceinline__ void advance() {
+        if (threadIdx.x == 0) {
+            slot[(k + 1) & 1] = ahead;
+            ahead = atomicAdd(counter, 1);
+        }
+        ++k;
+        __syncthreads();
+    }
+};
+
 
 // Wrap-padding of kernel stencils onto W x H planes (Kernel::pad_to_size,
 // kernel.rs:98-117), one block per plane: desc[p] = (tap offset, side, plane).
@@ -187,10 +213,9 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_R2C, FLP_BATCH_WARPS_R2C / BATC
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
-    for (;;) {
-        const int it = next_item(p.counters + q, n);
-        if (it < 0) break;
-        const int2 item = p.items[base + it];
+    __shared__ int qslot[2];
+    for (QueueCursor cur(p.counters + q, n, qslot); cur.item() >= 0; cur.advance()) {
+        const int2 item = p.items[base + cur.item()];
         const BWorld w = p.worlds[item.x];
         const int slot = item.y >> 16, g = item.y & 0xFFFF;
         const int c = p.srcs[w.offSrc + slot];
@@ -206,10 +231,9 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_COLS, FLP_BATCH_WARPS_COLS / BA
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
-    for (;;) {
-        const int it = next_item(p.counters + q, n);
-        if (it < 0) break;
-        const int2 item = p.items[base + it];
+    __shared__ int qslot[2];
+    for (QueueCursor cur(p.counters + q, n, qslot); cur.item() >= 0; cur.advance()) {
+        const int2 item = p.items[base + cur.item()];
         const BWorld w = p.worlds[item.x];
         const int u = item.y >> 16, g = item.y & 0xFFFF;  // u: source slot (shared) or kernel
         const int Wc = w.W / 2 + 1;
@@ -226,10 +250,9 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_C2R, FLP_BATCH_WARPS_C2R / BATC
     dep_enter();
     extern __shared__ __align__(16) float2 fsm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
-    for (;;) {
-        const int it = next_item(p.counters + q, n);
-        if (it < 0) break;
-        const int2 item = p.items[base + it];
+    __shared__ int qslot[2];
+    for (QueueCursor cur(p.counters + q, n, qslot); cur.item() >= 0; cur.advance()) {
+        const int2 item = p.items[base + cur.item()];
         const BWorld w = p.worlds[item.x];
         const int c = item.y >> 16, g = item.y & 0xFFFF;
         float* Uc = p.U + w.offA + size_t(c) * (2 * M) * w.H;
@@ -252,10 +275,9 @@ __global__ void __launch_bounds__(256) k_batch_flow(Pools p, int q) {
     dep_enter();
     extern __shared__ __align__(16) float sm[];
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
-    for (;;) {
-        const int it = next_item(p.counters + q, n);
-        if (it < 0) break;
-        const int2 item = p.items[base + it];
+    __shared__ int qslot[2];
+    for (QueueCursor cur(p.counters + q, n, qslot); cur.item() >= 0; cur.advance()) {
+        const int2 item = p.items[base + cur.item()];
         const BWorld w = p.worlds[item.x];
         const int tiles_x = (w.W + FL_W - 1) / FL_W;
         const int x0 = (item.y % tiles_x) * FL_W, y0 = (item.y / tiles_x) * (CV ? BATCH_FR_H : FL_H);
@@ -274,10 +296,9 @@ __global__ void __launch_bounds__(256, 3) k_batch_gather(Pools p) {
     extern __shared__ __align__(16) float sm[];
     constexpr int q = QG;
     const int base = p.q_off[q], n = p.q_off[q + 1] - base;
-    for (;;) {
-        const int it = next_item(p.counters + q, n);
-        if (it < 0) break;
-        const int2 item = p.items[base + it];
+    __shared__ int qslot[2];
+    for (QueueCursor cur(p.counters + q, n, qslot); cur.item() >= 0; cur.advance()) {
+        const int2 item = p.items[base + cur.item()];
         const BWorld w = p.worlds[item.x];
         const int c = item.y >> 16, t = item.y & 0xFFFF;
         const int tiles_x = (w.W + GT_W - 1) / GT_W;
