@@ -34,6 +34,7 @@ struct FlowParams {
     int beta_pow2;
     int area_pow2;      // 1 when the division by total_area is a multiplication
     int point_mode;     // total_area < 1e-10: nearest-cell deposit
+    int wide_square;    // area_pow2 and s >= 0.75: a square is wider than a cell plus any rounding of its ends
 };
 
 // Programmatic dependent launch.  The step's kernels are launched with

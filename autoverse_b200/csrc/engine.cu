@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -408,35 +409,76 @@ static void setup_fft3d(flp_propagator* h, const std::vector<KernelStencil>& ks)
     h->fft_ok = true;
 }
 
-static float time_conv(flp_propagator* h, int mode, int reps) {
+// The tuner's stopwatch: every timed repetition starts with the L2 cache
+// flushed (a memset of twice its size, outside the timed interval), so the
+// candidates are ranked as they run when a step's inputs come from HBM: every
+// world or batch larger than L2, and every step measured after a flush.  (For
+// a world small enough to stay in L2 across back-to-back steps, the warm
+// ranking differs by about 1 us at 512x512: the flushed step there favours one
+// destination row per gather thread and 4-warp column CTAs, the warm one two
+// rows and 8 warps.)
+struct ColdTimer {
+    static constexpr int MAX_REPS = 20;
+    flp_propagator* h;
+    DevScratch scratch;
+    void* flush = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t ev[2 * MAX_REPS] = {};
+    explicit ColdTimer(flp_propagator* hh) : h(hh) {
+        int dev = 0, l2 = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+        bytes = std::max<size_t>(size_t(2) * size_t(l2), size_t(64) << 20);
+        flush = scratch.add(dalloc<char>(bytes));
+        for (auto& e : ev) CK(cudaEventCreate(&e));
+    }
+    ~ColdTimer() {
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    ColdTimer(const ColdTimer&) = delete;
+    ColdTimer& operator=(const ColdTimer&) = delete;
+    // Mean device time of enqueue() over reps flushed repetitions, after two
+    // untimed ones.
+    template <class F>
+    float time(F&& enqueue, int reps) {
+        reps = std::min(reps, MAX_REPS);
+        enqueue();
+        enqueue();
+        for (int i = 0; i < reps; ++i) {
+            CK(cudaMemsetAsync(flush, i & 0xFF, bytes, h->st));
+            CK(cudaEventRecord(ev[2 * i], h->st));
+            enqueue();
+            CK(cudaEventRecord(ev[2 * i + 1], h->st));
+        }
+        CK(cudaEventSynchronize(ev[2 * reps - 1]));
+        float total = 0.f;
+        for (int i = 0; i < reps; ++i) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
+            total += ms;
+        }
+        return total / reps;
+    }
+};
+
+static float time_conv(flp_propagator* h, ColdTimer& tm, int mode, int reps) {
     int saved = h->conv_mode;
     h->conv_mode = mode;
-    for (int i = 0; i < 2; ++i) h->enqueue_conv(h->A[h->cur], nullptr);
-    CK(cudaEventRecord(h->ev0, h->st));
-    for (int i = 0; i < reps; ++i) h->enqueue_conv(h->A[h->cur], nullptr);
-    CK(cudaEventRecord(h->ev1, h->st));
-    CK(cudaEventSynchronize(h->ev1));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    const float ms = tm.time([&] { h->enqueue_conv(h->A[h->cur], nullptr); }, reps);
     h->conv_mode = saved;
-    return ms / reps;
+    return ms;
 }
 
 // Device time of one full step (from A[cur] into the other buffer, which is
-// scratch until the next step) averaged over reps, after two untimed steps.
-static float time_step(flp_propagator* h, int reps) {
+// scratch until the next step).
+static float time_step(flp_propagator* h, ColdTimer& tm, int reps) {
     const float* a = h->A[h->cur];
     float* an = h->A[h->cur ^ 1];
-    for (int i = 0; i < 2 + reps; ++i) {
-        if (i == 2) CK(cudaEventRecord(h->ev0, h->st));
+    return tm.time([&] {
         h->enqueue_conv(a, h->d_dmax);
         h->enqueue_transport(a, an);
-    }
-    CK(cudaEventRecord(h->ev1, h->st));
-    CK(cudaEventSynchronize(h->ev1));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-    return ms / reps;
+    }, reps);
 }
 
 static void apply_tuning(flp_propagator* h, const Tuning& t) {
@@ -450,11 +492,11 @@ static void apply_tuning(flp_propagator* h, const Tuning& t) {
 // Each FFT pass's CTA shape (warps per CTA; for the columns also one forward
 // transform per source or per kernel), one pass at a time from the defaults,
 // each candidate timed over 20 whole convolutions.
-static void tune_fft_passes(flp_propagator* h, Tuning& t) {
+static void tune_fft_passes(flp_propagator* h, ColdTimer& tm, Tuning& t) {
     const int reps = 20;
     auto timed = [&](const Tuning& c) {
         apply_tuning(h, c);
-        return time_conv(h, FLP_CONV_FFT, reps);
+        return time_conv(h, tm, FLP_CONV_FFT, reps);
     };
     float best = timed(t);
     for (int w : {4}) {
@@ -482,12 +524,12 @@ static void tune_fft_passes(flp_propagator* h, Tuning& t) {
 }
 
 // Destination rows per gather thread, timed over whole steps.
-static void tune_gather(flp_propagator* h, Tuning& t) {
+static void tune_gather(flp_propagator* h, ColdTimer& tm, Tuning& t) {
     float best = 0.f;
     int pick = 1;
     for (int gby : {1, 2}) {
         h->gather_gby = gby;
-        const float ms = time_step(h, 10);
+        const float ms = time_step(h, tm, 10);
         if (gby == 1 || ms < best) { best = ms; pick = gby; }
     }
     t.gather_gby = pick;
@@ -514,6 +556,11 @@ static void resolve_conv_mode(flp_propagator* h, int requested) {
         }
     }
     bool measured = false;
+    std::unique_ptr<ColdTimer> tm;
+    auto timer = [&]() -> ColdTimer& {
+        if (!tm) tm.reset(new ColdTimer(h));
+        return *tm;
+    };
     int mode;
     if (requested == FLP_CONV_DIRECT || requested == FLP_CONV_FFT) mode = requested;
     else if (!h->fft_ok) mode = FLP_CONV_DIRECT;
@@ -521,8 +568,8 @@ static void resolve_conv_mode(flp_propagator* h, int requested) {
     else if (t.conv_mode >= 0) mode = t.conv_mode;
     else {
         apply_tuning(h, t);
-        const float t_direct = time_conv(h, FLP_CONV_DIRECT, 5);
-        const float t_fft = time_conv(h, FLP_CONV_FFT, 5);
+        const float t_direct = time_conv(h, timer(), FLP_CONV_DIRECT, 5);
+        const float t_fft = time_conv(h, timer(), FLP_CONV_FFT, 5);
         mode = t.conv_mode = t_fft < t_direct ? FLP_CONV_FFT : FLP_CONV_DIRECT;
         measured = true;
     }
@@ -530,11 +577,11 @@ static void resolve_conv_mode(flp_propagator* h, int requested) {
     apply_tuning(h, t);
     if (h->dims == 2 && mode == FLP_CONV_FFT && !t.fft_tuned && fft_row_templated(h->W / 2) &&
         fft_col_templated(h->H)) {
-        tune_fft_passes(h, t);
+        tune_fft_passes(h, timer(), t);
         t.fft_tuned = measured = true;
     }
     if (h->dims == 2 && !t.gather_tuned) {
-        tune_gather(h, t);
+        tune_gather(h, timer(), t);
         t.gather_tuned = measured = true;
     }
     h->tuning_cached = cached && !measured;
@@ -578,6 +625,9 @@ FlowParams flow_params_of(const SimulationConfig& cfg) {
     fp.nexp = cfg.flow.n;
     fp.point_mode = fp.total_area < 1e-10f ? 1 : 0;
     if (fp.point_mode) fp.area_pow2 = 0;  // nearest-cell deposits carry the raw mass
+    // With 2s >= 1.5 no rounded square [dest - s, dest + s] fits inside one cell,
+    // which the 2D gather's saturating overlap form relies on.
+    fp.wide_square = fp.area_pow2 && fp.s >= 0.75f ? 1 : 0;
     // dest = x + dt*F and x_min/x_max are rounded at the scale of the largest
     // coordinate; allow a few ulps of it plus a fixed slack.
     const float maxside = float(std::max(std::max(cfg.width, cfg.height), cfg.depth));
