@@ -12,6 +12,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -42,7 +43,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     os.makedirs(os.path.dirname(lib), exist_ok=True)
     os.makedirs(objdir, exist_ok=True)
     hdr = _newest_header()
-    objs = []
+    objs, jobs = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -53,9 +54,18 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd += ["-Xptxas", "-v"] if ptxas_verbose else []
         else:
             cmd = [NVCC, *COMMON, "-x", "c++", "-c", src, "-o", obj]
+        jobs.append(cmd)
+    # translation units are independent: compile them concurrently
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for f in [ex.submit(run, c) for c in jobs]:
+            f.result()
     if force or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
         cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs]
         if verbose:
