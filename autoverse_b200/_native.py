@@ -107,6 +107,7 @@ SIGNATURES = {
     "flp_batch_kernel_spectra": (I, [P, C.POINTER(I), C.POINTER(Z)]),
     "flp_batch_profile_run": (I, [P, I, I, C.POINTER(F), C.POINTER(F)]),
     "flp_debug_transport": (I, [P, P, P, P, Z]),
+    "flp_twin64_step": (I, [S, P, P, P]),
     "flp_emb_create": (I, [S, PP]),
     "flp_emb_destroy": (I, [P]),
     "flp_emb_state_from_seed": (I, [P, S]),

@@ -22,6 +22,14 @@ struct KDesc {
     float pad;
 };
 
+// The same descriptor with double parameters, for the FP64 twin (twin64.cu).
+struct KDesc64 {
+    int src, tgt;
+    int r;
+    int tap_off;
+    double weight, mu, inv2s2;
+};
+
 // Flow/reintegration parameters of one world.
 struct FlowParams {
     float dt;
@@ -100,36 +108,52 @@ __device__ __forceinline__ int wrap_near(int c, int size) {
     return c;
 }
 
+// Round-to-nearest arithmetic without contraction, for the f32 engine and for
+// the same functions instantiated in double (the FP64 twin, twin64.cu).
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float r_pow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ double r_pow(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ float r_exp(float a) { return expf(a); }
+__device__ __forceinline__ double r_exp(double a) { return exp(a); }
+
 // alpha = clamp((A/beta)^n, 0, 1) with the reference's integer-n fast paths
 // (src/compute/flow.rs:14-32).  Division is IEEE (nvcc default prec-div).
-__device__ __forceinline__ float flow_alpha(float mass, float beta_a, float n) {
-    float ratio = __fdiv_rn(mass, beta_a);
-    float p;
-    if (n == 1.0f) p = ratio;
-    else if (n == 2.0f) p = __fmul_rn(ratio, ratio);
-    else if (n == 3.0f) p = __fmul_rn(__fmul_rn(ratio, ratio), ratio);
-    else if (n == 4.0f) { float r2 = __fmul_rn(ratio, ratio); p = __fmul_rn(r2, r2); }
-    else p = powf(ratio, n);
-    if (p < 0.0f) p = 0.0f;
-    if (p > 1.0f) p = 1.0f;
+template <class T>
+__device__ __forceinline__ T flow_alpha(T mass, T beta_a, T n) {
+    T ratio = rn_div(mass, beta_a);
+    T p;
+    if (n == T(1)) p = ratio;
+    else if (n == T(2)) p = rn_mul(ratio, ratio);
+    else if (n == T(3)) p = rn_mul(rn_mul(ratio, ratio), ratio);
+    else if (n == T(4)) { T r2 = rn_mul(ratio, ratio); p = rn_mul(r2, r2); }
+    else p = r_pow(ratio, n);
+    if (p < T(0)) p = T(0);
+    if (p > T(1)) p = T(1);
     return p;
 }
 
 // 2D Sobel, gradient.rs:99-102, evaluated left to right without contraction.
-__device__ __forceinline__ void sobel2(float tl, float tc, float tr, float ml, float mr, float bl, float bc, float br,
-                                      float& gx, float& gy) {
-    float x = __fadd_rn(-tl, tr);
-    x = __fsub_rn(x, __fmul_rn(2.0f, ml));
-    x = __fadd_rn(x, __fmul_rn(2.0f, mr));
-    x = __fsub_rn(x, bl);
-    x = __fadd_rn(x, br);
-    gx = __fmul_rn(x, 0.125f);
-    float y = __fsub_rn(-tl, __fmul_rn(2.0f, tc));
-    y = __fsub_rn(y, tr);
-    y = __fadd_rn(y, bl);
-    y = __fadd_rn(y, __fmul_rn(2.0f, bc));
-    y = __fadd_rn(y, br);
-    gy = __fmul_rn(y, 0.125f);
+template <class T>
+__device__ __forceinline__ void sobel2(T tl, T tc, T tr, T ml, T mr, T bl, T bc, T br, T& gx, T& gy) {
+    T x = rn_add(-tl, tr);
+    x = rn_sub(x, rn_mul(T(2), ml));
+    x = rn_add(x, rn_mul(T(2), mr));
+    x = rn_sub(x, bl);
+    x = rn_add(x, br);
+    gx = rn_mul(x, T(0.125));
+    T y = rn_sub(-tl, rn_mul(T(2), tc));
+    y = rn_sub(y, tr);
+    y = rn_add(y, bl);
+    y = rn_add(y, rn_mul(T(2), bc));
+    y = rn_add(y, br);
+    gy = rn_mul(y, T(0.125));
 }
 
 }  // namespace flp

@@ -65,6 +65,8 @@ PropView prop_view(flp_propagator* h);
 size_t conv_direct_smem_bytes(int rmax);
 void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, const float* taps, int W, int H, int C,
                            int rmax, int* reset_slot, cudaStream_t st);
+cudaError_t launch_conv_direct_2d_f64(const double* A, double* U, const KDesc64* kd, int K, const double* taps, int W,
+                                      int H, int C, int rmax);
 
 // transport: flow (destinations) then gather
 size_t flow_smem_bytes(int C);

@@ -30,12 +30,19 @@ namespace flp {
 // ---------------------------------------------------------------------------
 constexpr int CD_TW = 32, CD_TH = 32;
 
-__global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __restrict__ A, float* __restrict__ U,
-                                                             const KDesc* __restrict__ kd, int K,
-                                                             const float* __restrict__ taps, int W, int H, int rmax,
+// T = float in the engine; the FP64 twin (twin64.cu) instantiates the same
+// kernel in double with a descriptor type of double parameters.
+__device__ __forceinline__ float r_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double r_fma(double a, double b, double c) { return fma(a, b, c); }
+
+template <class T, class KD>
+__global__ void __launch_bounds__(256) conv_direct_growth_2d(const T* __restrict__ A, T* __restrict__ U,
+                                                             const KD* __restrict__ kd, int K,
+                                                             const T* __restrict__ taps, int W, int H, int rmax,
                                                              int* reset_slot, int nreset) {
     dep_enter();
-    extern __shared__ float sm[];
+    extern __shared__ __align__(16) unsigned char conv_sm[];
+    T* sm = reinterpret_cast<T*>(conv_sm);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * 32 + tx;
     const int c = blockIdx.z;
@@ -44,18 +51,18 @@ __global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __rest
     if (reset_slot && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0)
         for (int i = 0; i < nreset; ++i) reset_slot[i] = 0;
     const int Pmax = CD_TW + 2 * rmax;
-    float* tile = sm;                                   // (CD_TH + 2r) x (CD_TW + 2r)
-    float* tsm = sm + size_t(CD_TH + 2 * rmax) * Pmax;  // taps
-    float accu[4] = {0.f, 0.f, 0.f, 0.f};
+    T* tile = sm;                                   // (CD_TH + 2r) x (CD_TW + 2r)
+    T* tsm = sm + size_t(CD_TH + 2 * rmax) * Pmax;  // taps
+    T accu[4] = {T(0), T(0), T(0), T(0)};
     int loaded_src = -1, loaded_r = -1;
     for (int k = 0; k < K; ++k) {
-        const KDesc d = kd[k];
+        const KD d = kd[k];
         if (d.tgt != c) continue;
         const int r = d.r, side = 2 * r + 1, P = CD_TW + 2 * r;
         __syncthreads();
         for (int i = tid; i < side * side; i += 256) tsm[i] = taps[d.tap_off + i];
         if (d.src != loaded_src || r != loaded_r) {
-            const float* a = A + size_t(d.src) * N;
+            const T* a = A + size_t(d.src) * N;
             const int rows = CD_TH + 2 * r;
             for (int i = tid; i < rows * P; i += 256) {
                 int ly = i / P, lx = i - ly * P;
@@ -69,28 +76,28 @@ __global__ void __launch_bounds__(256) conv_direct_growth_2d(const float* __rest
         // Each stencil row is summed on its own (fused multiply-adds), then the
         // row sums are added: two chains of 2r+1 roundings instead of one of
         // (2r+1)^2, which keeps the sum's rounding error near that of an f32 FFT.
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        T acc[4] = {T(0), T(0), T(0), T(0)};
         for (int dy = 0; dy < side; ++dy) {
-            const float* trow = tsm + dy * side;
-            const float* base = tile + (ty + dy) * P + tx;
-            float row[4] = {0.f, 0.f, 0.f, 0.f};
+            const T* trow = tsm + dy * side;
+            const T* base = tile + (ty + dy) * P + tx;
+            T row[4] = {T(0), T(0), T(0), T(0)};
             for (int dx = 0; dx < side; ++dx) {
-                const float t = trow[dx];
+                const T t = trow[dx];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) row[i] = fmaf(t, base[(8 * i) * P + dx], row[i]);
+                for (int i = 0; i < 4; ++i) row[i] = r_fma(t, base[(8 * i) * P + dx], row[i]);
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[i] = __fadd_rn(acc[i], row[i]);
+            for (int i = 0; i < 4; ++i) acc[i] = rn_add(acc[i], row[i]);
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            float diff = __fsub_rn(acc[i], d.mu);
-            float e = expf(__fmul_rn(__fmul_rn(-diff, diff), d.inv2s2));
-            float g = __fsub_rn(__fmul_rn(2.0f, e), 1.0f);
-            accu[i] = __fadd_rn(accu[i], __fmul_rn(d.weight, g));
+            T diff = rn_sub(acc[i], T(d.mu));
+            T e = r_exp(rn_mul(rn_mul(-diff, diff), T(d.inv2s2)));
+            T g = rn_sub(rn_mul(T(2), e), T(1));
+            accu[i] = rn_add(accu[i], rn_mul(T(d.weight), g));
         }
     }
-    float* u = U + size_t(c) * N;
+    T* u = U + size_t(c) * N;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         int y = y0 + ty + 8 * i, x = x0 + tx;
@@ -108,7 +115,22 @@ void launch_conv_direct_2d(const float* A, float* U, const KDesc* kd, int K, con
                            int rmax, int* reset_slot, cudaStream_t st) {
     dim3 grid((W + CD_TW - 1) / CD_TW, (H + CD_TH - 1) / CD_TH, C);
     size_t smem = conv_direct_smem_bytes(rmax);
-    launch_dep(conv_direct_growth_2d, grid, dim3(32, 8), smem, st, A, U, kd, K, taps, W, H, rmax, reset_slot, 1);
+    launch_dep(conv_direct_growth_2d<float, KDesc>, grid, dim3(32, 8), smem, st, A, U, kd, K, taps, W, H, rmax,
+               reset_slot, 1);
+}
+
+// The direct convolution instantiated in double (FP64 twin); its shared
+// memory exceeds the default 48 KB above r = 15.
+cudaError_t launch_conv_direct_2d_f64(const double* A, double* U, const KDesc64* kd, int K, const double* taps, int W,
+                                      int H, int C, int rmax) {
+    const int P = CD_TW + 2 * rmax, side = 2 * rmax + 1;
+    const size_t smem = sizeof(double) * (size_t(CD_TH + 2 * rmax) * P + size_t(side) * side);
+    cudaError_t e = cudaFuncSetAttribute(conv_direct_growth_2d<double, KDesc64>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    dim3 grid((W + CD_TW - 1) / CD_TW, (H + CD_TH - 1) / CD_TH, C);
+    conv_direct_growth_2d<double, KDesc64><<<grid, dim3(32, 8), smem>>>(A, U, kd, K, taps, W, H, rmax, nullptr, 0);
+    return cudaGetLastError();
 }
 
 size_t flow_smem_bytes(int C) { return flow_smem_bytes_inl(C); }
@@ -209,7 +231,7 @@ void transport_2d_set_attributes() {
     set((const void*)gather_2d<false, 1>, gather_smem_bytes());
     set((const void*)gather_2d<true, 2>, gather_smem_bytes_inl(2));
     set((const void*)gather_2d<false, 2>, gather_smem_bytes_inl(2));
-    cudaFuncSetAttribute(conv_direct_growth_2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(conv_direct_growth_2d<float, KDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(conv_direct_smem_bytes(MAX_DIRECT_RADIUS)));
 }
 

@@ -217,53 +217,64 @@ SimulationConfig parse_config(const std::string& text) {
 }
 
 // ----------------------------------------------------------------- kernel ----
-KernelStencil build_kernel(const KernelConfig& kc, int max_radius, int dims) {
-    KernelStencil k;
-    float rr = std::round(kc.radius * float(max_radius));
-    int actual_radius = rr > 0.f ? int(rr) : 0;
+// R = float is the engine's stencil (the reference's f32 arithmetic); the FP64
+// twin instantiates the same statements in double.
+template <class R>
+KernelStencilT<R> build_kernel_t(const KernelConfig& kc, int max_radius, int dims) {
+    KernelStencilT<R> k;
+    R rr = std::round(R(kc.radius) * R(max_radius));
+    int actual_radius = rr > R(0) ? int(rr) : 0;
     k.radius = actual_radius;
     k.size = actual_radius * 2 + 1;
     k.dims = dims;
     const int size = k.size;
-    const float center = float(actual_radius);
+    const R center = R(actual_radius);
     const int zs = dims == 3 ? size : 1;
-    k.data.assign(size_t(size) * size * zs, 0.f);
-    float sum = 0.f;
+    k.data.assign(size_t(size) * size * zs, R(0));
+    R sum = R(0);
     for (int z = 0; z < zs; ++z)
         for (int y = 0; y < size; ++y)
             for (int x = 0; x < size; ++x) {
-                float dx = float(x) - center, dy = float(y) - center;
-                float dist;
+                R dx = R(x) - center, dy = R(y) - center;
+                R dist;
                 if (dims == 3) {
-                    float dz = float(z) - center;
+                    R dz = R(z) - center;
                     dist = std::sqrt(dx * dx + dy * dy + dz * dz);
                 } else {
                     dist = std::sqrt(dx * dx + dy * dy);
                 }
-                float norm_dist = dist / float(actual_radius);
-                if (norm_dist > 1.0f) continue;
-                float value = 0.f;
+                R norm_dist = dist / R(actual_radius);
+                if (norm_dist > R(1)) continue;
+                R value = R(0);
                 for (const auto& ring : kc.rings) {
-                    float ring_dist = std::fabs(norm_dist - ring.distance);
-                    float bump = ring.amplitude * std::exp(-ring_dist * ring_dist / (2.0f * ring.width * ring.width));
+                    R ring_dist = std::fabs(norm_dist - R(ring.distance));
+                    R bump = R(ring.amplitude) *
+                             std::exp(-ring_dist * ring_dist / (R(2) * R(ring.width) * R(ring.width)));
                     value += bump;
                 }
                 k.data[(size_t(z) * size + y) * size + x] = value;
                 sum += value;
             }
-    if (sum > 0.f) {
-        float inv_sum = 1.0f / sum;
+    if (sum > R(0)) {
+        R inv_sum = R(1) / sum;
         for (auto& v : k.data) v *= inv_sum;
     }
     return k;
 }
+template KernelStencilT<float> build_kernel_t<float>(const KernelConfig&, int, int);
+template KernelStencilT<double> build_kernel_t<double>(const KernelConfig&, int, int);
 
-std::vector<float> pad_kernel(const KernelStencil& k, int W, int H, int D) {
+KernelStencil build_kernel(const KernelConfig& kc, int max_radius, int dims) {
+    return build_kernel_t<float>(kc, max_radius, dims);
+}
+
+template <class R>
+std::vector<R> pad_kernel_t(const KernelStencilT<R>& k, int W, int H, int D) {
     // The reference indexes with ((dx + W) % W) as usize, which panics (an
     // out-of-range index) once r exceeds a side; report it instead.
     if (k.radius > W || k.radius > H || (k.dims == 3 && k.radius > D))
         throw ConfigError("kernel radius " + std::to_string(k.radius) + " exceeds a grid side");
-    std::vector<float> out(size_t(W) * H * D, 0.f);
+    std::vector<R> out(size_t(W) * H * D, R(0));
     const int c = k.size / 2;
     const int zs = k.dims == 3 ? k.size : 1;
     for (int kz = 0; kz < zs; ++kz)
@@ -275,6 +286,10 @@ std::vector<float> pad_kernel(const KernelStencil& k, int W, int H, int D) {
             }
     return out;
 }
+template std::vector<float> pad_kernel_t<float>(const KernelStencilT<float>&, int, int, int);
+template std::vector<double> pad_kernel_t<double>(const KernelStencilT<double>&, int, int, int);
+
+std::vector<float> pad_kernel(const KernelStencil& k, int W, int H, int D) { return pad_kernel_t<float>(k, W, H, D); }
 
 // ------------------------------------------------------------------- seed ----
 namespace {

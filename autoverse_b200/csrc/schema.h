@@ -81,16 +81,23 @@ void generate_seed_into(const std::string& seed_json, const SimulationConfig& cf
 // --------------------------------------------------------------- kernel ----
 // Kernel::from_config / Kernel3D::from_config (kernel.rs:32-92,
 // kernel3d.rs:32-90): the normalised ring-sum stencil, side 2r+1.
-struct KernelStencil {
+template <class R>
+struct KernelStencilT {
     int radius = 0;  // r = round(radius * kernel_radius)
     int size = 1;    // 2r+1
     int dims = 2;
-    std::vector<float> data;  // size^dims values, row-major
+    std::vector<R> data;  // size^dims values, row-major
 };
+using KernelStencil = KernelStencilT<float>;
+// R = float (the engine) or double (the FP64 twin); instantiated in schema.cpp.
+template <class R>
+KernelStencilT<R> build_kernel_t(const KernelConfig& kc, int max_radius, int dims);
 KernelStencil build_kernel(const KernelConfig& kc, int max_radius, int dims);
 
 // Kernel::pad_to_size (kernel.rs:98-117, kernel3d.rs:103-133): wrap-padded
 // onto the torus; later taps overwrite earlier ones when 2r+1 exceeds a side.
+template <class R>
+std::vector<R> pad_kernel_t(const KernelStencilT<R>& k, int W, int H, int D);
 std::vector<float> pad_kernel(const KernelStencil& k, int W, int H, int D);
 
 }  // namespace flp

@@ -46,21 +46,49 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // alpha with the reference's division mass / beta_a; a power-of-two beta_a
-// turns it into an exact multiplication.
-__device__ __forceinline__ float alpha_fp(float mass, const FlowParams& fp) {
+// turns it into an exact multiplication.  T = float in the engine, double in
+// the FP64 twin (the parameters are the f32 values the reference uses).
+template <class T>
+__device__ __forceinline__ T alpha_fp(T mass, const FlowParams& fp) {
     if (fp.beta_pow2) {
-        const float ratio = __fmul_rn(mass, fp.inv_beta);
-        float p;
+        const T ratio = rn_mul(mass, T(fp.inv_beta));
+        T p;
         if (fp.nexp == 1.0f) p = ratio;
-        else if (fp.nexp == 2.0f) p = __fmul_rn(ratio, ratio);
-        else if (fp.nexp == 3.0f) p = __fmul_rn(__fmul_rn(ratio, ratio), ratio);
-        else if (fp.nexp == 4.0f) { const float r2 = __fmul_rn(ratio, ratio); p = __fmul_rn(r2, r2); }
-        else p = powf(ratio, fp.nexp);
-        if (p < 0.0f) p = 0.0f;  // f32::clamp(0, 1); NaN passes through
-        if (p > 1.0f) p = 1.0f;
+        else if (fp.nexp == 2.0f) p = rn_mul(ratio, ratio);
+        else if (fp.nexp == 3.0f) p = rn_mul(rn_mul(ratio, ratio), ratio);
+        else if (fp.nexp == 4.0f) { const T r2 = rn_mul(ratio, ratio); p = rn_mul(r2, r2); }
+        else p = r_pow(ratio, T(fp.nexp));
+        if (p < T(0)) p = T(0);  // f32::clamp(0, 1); NaN passes through
+        if (p > T(1)) p = T(1);
         return p;
     }
-    return flow_alpha(mass, fp.beta_a, fp.nexp);
+    return flow_alpha(mass, T(fp.beta_a), T(fp.nexp));
+}
+
+// Per-cell flow (propagator.rs:304-330, flow.rs:68-87) and destination
+// (reintegration.rs:81-82), shared by every flow kernel: flow_mix takes the
+// 3x3 window of the channel sum, flow_destination the 3x3 window of one U_c.
+template <class T>
+struct FlowMix {
+    T oma, agx, agy;  // 1 - alpha, alpha * grad(sum)
+};
+template <class T>
+__device__ __forceinline__ FlowMix<T> flow_mix(T tl, T tc, T tr, T ml, T mc, T mr, T bl, T bc, T br,
+                                               const FlowParams& fp) {
+    T gax, gay;
+    sobel2(tl, tc, tr, ml, mr, bl, bc, br, gax, gay);
+    const T alpha = alpha_fp(mc, fp);
+    return {rn_sub(T(1), alpha), rn_mul(alpha, gax), rn_mul(alpha, gay)};
+}
+template <class T>
+__device__ __forceinline__ void flow_destination(const FlowMix<T>& f, T tl, T tc, T tr, T ml, T mr, T bl, T bc,
+                                                 T br, int X, int Y, const FlowParams& fp, T& dx, T& dy) {
+    T gux, guy;
+    sobel2(tl, tc, tr, ml, mr, bl, bc, br, gux, guy);
+    const T fx = rn_sub(rn_mul(f.oma, gux), f.agx);
+    const T fy = rn_sub(rn_mul(f.oma, guy), f.agy);
+    dx = rn_add(T(X), rn_mul(T(fp.dt), fx));
+    dy = rn_add(T(Y), rn_mul(T(fp.dt), fy));
 }
 
 // Window from the largest displacement (dmax slot: float bits of a
@@ -86,11 +114,12 @@ __device__ __forceinline__ int rotated_offset(int j, int c, int R, int size) {
     return -R + (j - (2 * R + 1 - n_lo));
 }
 
-__device__ __forceinline__ int f2i_sat(float v) {
+template <class T>
+__device__ __forceinline__ int f2i_sat(T v) {
     // Rust `f32 as i32`: saturating, NaN -> 0.
     if (v != v) return 0;
-    if (v >= 2147483647.f) return 2147483647;
-    if (v <= -2147483648.f) return -2147483647 - 1;
+    if (v >= T(2147483647.f)) return 2147483647;
+    if (v <= T(-2147483648.f)) return -2147483647 - 1;
     return int(v);
 }
 
@@ -98,10 +127,10 @@ __device__ __forceinline__ int f2i_sat(float v) {
 // 1e-10 threshold (reintegration.rs:76-78), pre-scaled by 1/(2s)^2 when that
 // factor is a power of two (then m * area equals the reference's
 // mass * (area / total_area) exactly).
-template <bool POW2>
-__device__ __forceinline__ float source_mass(float a, const FlowParams& fp) {
-    const float m = fabsf(a) < 1e-10f ? 0.f : a;
-    return POW2 ? __fmul_rn(m, fp.inv_area) : m;
+template <bool POW2, class T>
+__device__ __forceinline__ T source_mass(T a, const FlowParams& fp) {
+    const T m = fabs(a) < T(1e-10f) ? T(0) : a;
+    return POW2 ? rn_mul(m, T(fp.inv_area)) : m;
 }
 
 // ------------------------------------------------------------- flow_2d ----
@@ -159,21 +188,14 @@ inline __device__ void flow_item(float* sm, const float* __restrict__ A, const f
     if (X < W && Y < H) {
         const int o = ly * FL_RW + lx;  // top-left of the 3x3 window
         const float* a = asum + o;
-        float gax, gay;
-        sobel2(a[0], a[1], a[2], a[FL_RW], a[FL_RW + 2], a[2 * FL_RW], a[2 * FL_RW + 1], a[2 * FL_RW + 2], gax, gay);
-        const float alpha = alpha_fp(a[FL_RW + 1], fp);
-        const float oma = __fsub_rn(1.0f, alpha);
-        const float agx = __fmul_rn(alpha, gax), agy = __fmul_rn(alpha, gay);
+        const FlowMix<float> f = flow_mix(a[0], a[1], a[2], a[FL_RW], a[FL_RW + 1], a[FL_RW + 2], a[2 * FL_RW],
+                                          a[2 * FL_RW + 1], a[2 * FL_RW + 2], fp);
         const size_t cell = size_t(Y) * W + X;
         for (int c = 0; c < C; ++c) {
             const float* u = us + c * FL_RC + o;
-            float gux, guy;
-            sobel2(u[0], u[1], u[2], u[FL_RW], u[FL_RW + 2], u[2 * FL_RW], u[2 * FL_RW + 1], u[2 * FL_RW + 2], gux,
-                   guy);
-            const float fx = __fsub_rn(__fmul_rn(oma, gux), agx);
-            const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
-            const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
-            const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
+            float dx, dy;
+            flow_destination(f, u[0], u[1], u[2], u[FL_RW], u[FL_RW + 2], u[2 * FL_RW], u[2 * FL_RW + 1],
+                             u[2 * FL_RW + 2], X, Y, fp, dx, dy);
             const float mass = as[c * FL_RC + o + FL_RW + 1];
             bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
             if (fabsf(mass) >= 1e-10f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
@@ -260,21 +282,14 @@ __device__ __forceinline__ void flow_rows_item(const float* __restrict__ A, cons
         if (r < 2) continue;
         const int Y = yb + r - 2;
         if (X >= W || Y >= H) continue;
-        float gax, gay;
-        sobel2(sw[0][0], sw[0][1], sw[0][2], sw[1][0], sw[1][2], sw[2][0], sw[2][1], sw[2][2], gax, gay);
-        const float alpha = alpha_fp(sw[1][1], fp);
-        const float oma = __fsub_rn(1.0f, alpha);
-        const float agx = __fmul_rn(alpha, gax), agy = __fmul_rn(alpha, gay);
+        const FlowMix<float> f = flow_mix(sw[0][0], sw[0][1], sw[0][2], sw[1][0], sw[1][1], sw[1][2], sw[2][0],
+                                          sw[2][1], sw[2][2], fp);
         const size_t cell = size_t(Y) * W + X;
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            float gux, guy;
-            sobel2(uw[c][0][0], uw[c][0][1], uw[c][0][2], uw[c][1][0], uw[c][1][2], uw[c][2][0], uw[c][2][1],
-                   uw[c][2][2], gux, guy);
-            const float fx = __fsub_rn(__fmul_rn(oma, gux), agx);
-            const float fy = __fsub_rn(__fmul_rn(oma, guy), agy);
-            const float dx = __fadd_rn(float(X), __fmul_rn(fp.dt, fx));
-            const float dy = __fadd_rn(float(Y), __fmul_rn(fp.dt, fy));
+            float dx, dy;
+            flow_destination(f, uw[c][0][0], uw[c][0][1], uw[c][0][2], uw[c][1][0], uw[c][1][2], uw[c][2][0],
+                             uw[c][2][1], uw[c][2][2], X, Y, fp, dx, dy);
             const float mass = ac[c];
             bad |= !(isfinite(mass) && isfinite(dx) && isfinite(dy));
             if (fabsf(mass) >= 1e-10f) dmax = fmaxf(dmax, fmaxf(fabsf(dx - float(X)), fabsf(dy - float(Y))));
@@ -618,11 +633,11 @@ __device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX
 // the destination and state planes in global memory.  Handles the
 // nearest-cell mode, the reference's [-W, 2W] cell clamp, and windows wider
 // than the grid.
-template <bool POW2>
-__device__ float gather_generic_2d(const float* __restrict__ DX, const float* __restrict__ DY,
-                                   const float* __restrict__ A, int W, int H, int X, int Y, int R,
-                                   const FlowParams& fp) {
-    float acc = 0.f;
+template <bool POW2, class T>
+__device__ T gather_generic_2d(const T* __restrict__ DX, const T* __restrict__ DY, const T* __restrict__ A, int W,
+                               int H, int X, int Y, int R, const FlowParams& fp) {
+    const T s = T(fp.s);
+    T acc = T(0);
     for (int jy = 0; jy <= 2 * R; ++jy) {
         const int ky = rotated_offset(jy, Y, R, H);
         const int yw = wrap_coord(Y + ky, H);
@@ -632,25 +647,25 @@ __device__ float gather_generic_2d(const float* __restrict__ DX, const float* __
             const int xw = wrap_coord(X + kx, W);
             const int ix = xw - kx;
             const size_t src = size_t(yw) * W + xw;
-            const float m = source_mass<POW2>(A[src], fp);
-            if (m == 0.f) continue;
-            const float dx = DX[src], dy = DY[src];
+            const T m = source_mass<POW2>(A[src], fp);
+            if (m == T(0)) continue;
+            const T dx = DX[src], dy = DY[src];
             if (fp.point_mode) {
-                if (f2i_sat(roundf(dx)) == ix && f2i_sat(roundf(dy)) == iy) acc = __fadd_rn(acc, m);
+                if (f2i_sat(round(dx)) == ix && f2i_sat(round(dy)) == iy) acc = rn_add(acc, m);
                 continue;
             }
-            const float xmin = __fsub_rn(dx, fp.s), xmax = __fadd_rn(dx, fp.s);
-            const float ymin = __fsub_rn(dy, fp.s), ymax = __fadd_rn(dy, fp.s);
-            const int ix_lo = max(f2i_sat(floorf(xmin)), -W), ix_hi = min(f2i_sat(ceilf(xmax)), 2 * W);
-            const int iy_lo = max(f2i_sat(floorf(ymin)), -H), iy_hi = min(f2i_sat(ceilf(ymax)), 2 * H);
+            const T xmin = rn_sub(dx, s), xmax = rn_add(dx, s);
+            const T ymin = rn_sub(dy, s), ymax = rn_add(dy, s);
+            const int ix_lo = max(f2i_sat(floor(xmin)), -W), ix_hi = min(f2i_sat(ceil(xmax)), 2 * W);
+            const int iy_lo = max(f2i_sat(floor(ymin)), -H), iy_hi = min(f2i_sat(ceil(ymax)), 2 * H);
             if (ix < ix_lo || ix > ix_hi || iy < iy_lo || iy > iy_hi) continue;
-            const float ox0 = fmaxf(float(ix), xmin), ox1 = fminf(float(ix + 1), xmax);
-            const float oy0 = fmaxf(float(iy), ymin), oy1 = fminf(float(iy + 1), ymax);
-            const float ow = fmaxf(__fsub_rn(ox1, ox0), 0.f);
-            const float oh = fmaxf(__fsub_rn(oy1, oy0), 0.f);
-            const float area = __fmul_rn(ow, oh);
-            if (!(area > 0.f)) continue;
-            acc = __fadd_rn(acc, POW2 ? __fmul_rn(m, area) : __fmul_rn(m, __fdiv_rn(area, fp.total_area)));
+            const T ox0 = fmax(T(ix), xmin), ox1 = fmin(T(ix + 1), xmax);
+            const T oy0 = fmax(T(iy), ymin), oy1 = fmin(T(iy + 1), ymax);
+            const T ow = fmax(rn_sub(ox1, ox0), T(0));
+            const T oh = fmax(rn_sub(oy1, oy0), T(0));
+            const T area = rn_mul(ow, oh);
+            if (!(area > T(0))) continue;
+            acc = rn_add(acc, POW2 ? rn_mul(m, area) : rn_mul(m, rn_div(area, T(fp.total_area))));
         }
     }
     return acc;

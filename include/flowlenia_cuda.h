@@ -181,6 +181,15 @@ FLP_API int flp_debug_affinity(flp_propagator* h, float* aff_out, size_t n);
  * mass sum, Sobel, flow, reintegration.  Writes the next state to out. */
 FLP_API int flp_debug_transport(flp_propagator* h, const float* state, const float* aff, float* out, size_t n);
 
+/* FP64 twin of one 2D step (CpuPropagator::step, propagator.rs:239-420, in
+ * double): the engine's own direct convolution + growth, flow and gather
+ * functions instantiated in double, with the config's f32 parameters widened.
+ * No counterpart in the reference: it states the f32 engine's error against
+ * an FP64 build of the same arithmetic.  Host buffers of channels*N doubles:
+ * state in, next state out, affinity out (may be NULL).  Allocates and frees
+ * its own device buffers; synchronous; diagnostic, not a product path. */
+FLP_API int flp_twin64_step(const char* config_json, const double* state, double* affinity, double* next);
+
 /* ---- Batched worlds ----------------------------------------------------
  * Many independent 2D worlds of uneven sizes, channel counts and parameters,
  * advanced together by persistent kernels that pull (world, tile) items from
