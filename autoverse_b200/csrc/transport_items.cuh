@@ -464,6 +464,73 @@ __device__ __forceinline__ void gather_row(const float* __restrict__ rxmin, cons
     }
 }
 
+// Terms of the source columns JA..JB of one source row (inside one float4
+// chunk), for an x-edge warp: each term is kept in vals and also added to acc
+// where `add` holds, so that a lane can take the columns either before or
+// after the others.  sh moves the destinations into the frame of wrapped
+// sources (a multiple of W, or 0).
+template <bool WIDE, int RN, bool POW2, int DM, int GBY, int JA, int JB>
+__device__ __forceinline__ void gather_terms(const float* __restrict__ rxmin, const float* __restrict__ rxmax,
+                                             const float* __restrict__ rymin, const float* __restrict__ rymax,
+                                             const float* __restrict__ rm, const float (&fy)[GBY + 1],
+                                             const float (&fxs)[5], float sh, bool add, float total_area,
+                                             float (&acc)[GBY][4], float (&vals)[GBY][4][JB - JA + 1]) {
+    constexpr int q = JA / 4;
+    static_assert(JB / 4 == q, "one chunk of 4 source columns");
+    const float4 vxa = *reinterpret_cast<const float4*>(rxmin + 4 * q);
+    const float4 vxb = *reinterpret_cast<const float4*>(rxmax + 4 * q);
+    const float4 vya = *reinterpret_cast<const float4*>(rymin + 4 * q);
+    const float4 vyb = *reinterpret_cast<const float4*>(rymax + 4 * q);
+    const float4 vm = *reinterpret_cast<const float4*>(rm + 4 * q);
+    const float xa[4] = {vxa.x, vxa.y, vxa.z, vxa.w}, xb[4] = {vxb.x, vxb.y, vxb.z, vxb.w};
+    const float ya[4] = {vya.x, vya.y, vya.z, vya.w}, yb[4] = {vyb.x, vyb.y, vyb.z, vyb.w};
+    const float mm[4] = {vm.x, vm.y, vm.z, vm.w};
+#pragma unroll
+    for (int j = JA; j <= JB; ++j) {
+        const int jj = j - 4 * q;
+        const float m = mm[jj];
+        float oh[GBY];
+#pragma unroll
+        for (int d = 0; d < GBY; ++d) {
+            if (!((DM >> d) & 1)) continue;
+            oh[d] = cell_overlap<WIDE>(fy[d], fy[d + 1], ya[jj], yb[jj]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (j - TP - i < -RN || j - TP - i > RN + 1) continue;
+            const float ow = cell_overlap<WIDE>(__fadd_rn(fxs[i], sh), __fadd_rn(fxs[i + 1], sh), xa[jj], xb[jj]);
+#pragma unroll
+            for (int d = 0; d < GBY; ++d) {
+                if (!((DM >> d) & 1)) continue;
+                const float area = __fmul_rn(ow, oh[d]);
+                // a term without mass or overlap is +0 or -0, which leaves acc
+                // (never -0: it starts at +0) unchanged
+                const float v = POW2 ? __fmul_rn(m, area)
+                                     : ((m != 0.f && area > 0.f) ? __fmul_rn(m, __fdiv_rn(area, total_area)) : 0.f);
+                vals[d][i][j - JA] = v;
+                if (add) acc[d][i] = __fadd_rn(acc[d][i], v);
+            }
+        }
+    }
+}
+
+// Adds the kept terms of source columns JA..JB where `add` holds, in column order.
+template <int RN, int DM, int GBY, int JA, int JB>
+__device__ __forceinline__ void gather_add_terms(bool add, float (&acc)[GBY][4],
+                                                 const float (&vals)[GBY][4][JB - JA + 1]) {
+#pragma unroll
+    for (int j = JA; j <= JB; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (j - TP - i < -RN || j - TP - i > RN + 1) continue;
+#pragma unroll
+            for (int d = 0; d < GBY; ++d) {
+                if (!((DM >> d) & 1)) continue;
+                if (add) acc[d][i] = __fadd_rn(acc[d][i], vals[d][i][j - JA]);
+            }
+        }
+}
+
 // The 4 x GBY destinations of one thread.  Each destination sums its sources
 // in the reference's deposit order: row-major over wrapped source indices,
 // i.e. rows in wrap-pass order (rows past the bottom edge wrap to the top and
@@ -489,6 +556,21 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
     static_assert(RN <= 3 && TP == 4, "edge column ranges assume RN <= 3 and 4-column chunks");
     const bool xleft = cp_hi == 2 && cp_lo == 1 && X0 == 0;
     const bool xright = cp_lo == 0 && cp_hi == 1 && X0 == W - 4 && (W & 3) == 0;
+    // Warps that hold an x-edge lane (X0 = 0 or X0 = W - 4) take one path for
+    // all their lanes when RN <= 1 and GBY = 2 (with one destination row per
+    // thread the kept terms cost more than the edge lanes' passes; measured on
+    // the 512x512 single world): the source columns left of the thread's
+    // block (j < TP) and right of it (j >= 2 TP) are computed once, kept in
+    // registers and added where each lane's wrapped order puts them (a left
+    // edge lane adds the left columns last, a right edge lane the right columns
+    // first), instead of the edge and the inside lanes running their passes
+    // one after the other.
+    bool xedge = false;
+    if constexpr (RN <= 1 && GBY == 2) {
+        const bool simple = xin || xleft || xright;
+        xedge = __any_sync(__activemask(), xleft || xright) && simple;
+    }
+    const float shL = xleft ? float(W) : 0.f, shR = xright ? -float(W) : 0.f;
     const int gx_base = x0 - TP + 4 * tx;
     float fxs[5];
 #pragma unroll
@@ -504,6 +586,33 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
 #pragma unroll
         for (int d = 0; d <= GBY; ++d) fy[d] = float(yb + d);
         const int off = (GBY * ty + r) * sw + 4 * tx;
+        if constexpr (RN <= 1 && GBY == 2) {
+            if (xedge) {
+                constexpr int RA = 2 * TP, RB = TP + 3 + RN + 1;  // right columns
+                float vr[GBY][4][RB - RA + 1];
+                gather_terms<WIDE, RN, POW2, DM, GBY, RA, RB>(sxmin + off, sxmax + off, symin + off, symax + off,
+                                                              smass + off, fy, fxs, shR, xright, fp.total_area, acc,
+                                                              vr);
+                if constexpr (RN > 0) {
+                    constexpr int LA = TP - RN, LB = TP - 1;  // left columns
+                    float vl[GBY][4][LB - LA + 1];
+                    gather_terms<WIDE, RN, POW2, DM, GBY, LA, LB>(sxmin + off, sxmax + off, symin + off,
+                                                                  symax + off, smass + off, fy, fxs, shL, !xleft,
+                                                                  fp.total_area, acc, vl);
+                    gather_row<WIDE, RN, POW2, false, DM, GBY, TP, 2 * TP - 1>(
+                        sxmin + off, sxmax + off, symin + off, symax + off, smass + off, fy, fxs, X0, gx_base, W, 1,
+                        fp.total_area, acc);
+                    gather_add_terms<RN, DM, GBY, RA, RB>(!xright, acc, vr);
+                    gather_add_terms<RN, DM, GBY, LA, LB>(xleft, acc, vl);
+                } else {
+                    gather_row<WIDE, RN, POW2, false, DM, GBY, TP, 2 * TP - 1>(
+                        sxmin + off, sxmax + off, symin + off, symax + off, smass + off, fy, fxs, X0, gx_base, W, 1,
+                        fp.total_area, acc);
+                    gather_add_terms<RN, DM, GBY, RA, RB>(!xright, acc, vr);
+                }
+                return;
+            }
+        }
         if (xin) {
             gather_row<WIDE, RN, POW2, false, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off,
                                                        smass + off, fy, fxs, X0, gx_base, W, 1, fp.total_area, acc);
@@ -564,12 +673,43 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
 // keeps the rows read by a quarter-warp in distinct bank groups of the
 // 76-float rows (GBY = 1: 8 consecutive thread rows of one column; GBY = 2:
 // 4 thread rows of two columns).
+//
+// For GBY = 2 the x-edge tiles take a lane table (tx | ty << 4 per thread):
+// warp 0 holds the two edge columns tx = 0 and 15 (it takes the x-edge path
+// of gather_strip), warp 1 the top and bottom thread rows ty = 0 and 15 of the
+// inner columns (the lanes whose source rows wrap in a tile on a y edge, so
+// that only two warps run a second row pass), the other six warps the inner
+// block.  Every quarter-warp of the table reads distinct 16-byte bank groups
+// of the 76-float rows ((6 ty + tx) mod 8 all different).
+static __device__ const unsigned char kGatherEdgeLanes2[256] = {
+      0,  15,  16,  31,  32,  47,  48,  63,  64,  79,  80,  95,  96, 111, 112, 127,
+    128, 143, 144, 159, 160, 175, 176, 191, 192, 207, 208, 223, 224, 239, 240, 255,
+     10, 251, 241,   6,   4, 254,   7,   9,  11,  20,  14,  13, 250,   8,   1, 253,
+      2, 249, 243,  26, 252,  25, 247,  12, 248,   3,  19, 246,   5, 244, 245, 242,
+    148,  57,  52,  33, 210,  58,  35, 137, 139, 220,  70, 217,  41, 204, 146, 173,
+     46, 140, 227, 116, 197, 113,  62,  37, 102,  98, 205,  30,  61, 177,  65, 190,
+    215, 130,  42,  40,  53, 213, 155, 218,  69,  38,  86, 206,  67, 201, 136, 107,
+    169,  68, 170, 110, 195,  81,  90,  83,  23,  60, 232, 221,  92, 209, 236, 219,
+    150, 124, 131,  56, 133, 172,  71, 237, 226, 120, 214, 164, 231, 171, 115, 109,
+    162, 202,  76,  72, 185, 125, 187, 193, 238, 216, 104, 100,  93, 189, 123, 129,
+    158,  78,  18,  66,  89,  77, 119,  29,  54, 188,  22, 153,  97, 156, 101, 103,
+     44, 180,  43, 184, 222,  73, 161,  75, 126, 142, 235, 122,  45, 138, 203, 141,
+     36, 117,  34,  91, 178, 166, 167, 105, 199, 228, 168, 234,  74, 183, 121, 233,
+    181, 108, 106,  50, 230, 149, 229, 179, 135, 118, 196,  88,  85, 174,  27, 225,
+    154, 212, 145,  21,  24, 114,  51, 147, 200,  84,  87,  99, 198,  49, 132, 211,
+    182, 194, 151,  17, 134, 157, 165,  94,  28, 163,  82, 152,  55,  39, 186,  59,
+};
+
 template <int GBY>
-__device__ __forceinline__ void gather_thread(bool cm, int& tx, int& ty) {
+__device__ __forceinline__ void gather_thread(bool cm, bool table, int& tx, int& ty) {
     const int tid = threadIdx.x;
     if (!cm) {
         tx = tid & 15;
         ty = tid >> 4;
+    } else if (GBY == 2 && table) {
+        const int v = kGatherEdgeLanes2[tid];
+        tx = v & 15;
+        ty = v >> 4;
     } else if (GBY == 1) {
         tx = tid >> 4;
         ty = tid & 15;
@@ -589,8 +729,10 @@ __device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX
     constexpr int SRH = gt_h(GBY) + 2 * RN + 1;
     const int tid = threadIdx.x;
     const bool cm = gather_column_major(x0, W, RN);
+    // the lane table when the tile's x-edge lanes are tx = 0 and tx = 15 only
+    const bool table = x0 + GT_W + RN < W || x0 + GT_W == W;
     int tx, ty;
-    gather_thread<GBY>(cm, tx, ty);
+    gather_thread<GBY>(cm, table, tx, ty);
     const int sw = cm ? SR_W : SR_W - 4;  // row stride: padded only for the column-major mapping
     float* sxmin = sm;                    // SRH x sw each
     float* sxmax = sxmin + sw * SRH;
