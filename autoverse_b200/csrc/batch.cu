@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(32 * BATCH_WPC_C2R, FLP_BATCH_WARPS_C2R / BATC
 // persistent kernel is throughput-bound, so a taller walk that reloads fewer
 // halo rows pays, where the single-world kernel wants more, shorter tiles.
 #ifndef FLP_BATCH_FR_RPT
-#define FLP_BATCH_FR_RPT 4
+#define FLP_BATCH_FR_RPT 8
 #endif
 constexpr int BATCH_FR_RPT = FLP_BATCH_FR_RPT;
 constexpr int BATCH_FR_H = 8 * BATCH_FR_RPT;

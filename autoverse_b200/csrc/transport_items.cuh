@@ -216,7 +216,10 @@ inline __device__ void flow_item(float* sm, const float* __restrict__ A, const f
 // (x0-1 for lane 0, x0+32 for lane 31) from one extra load per row and field.
 // Every lane loads the wrapped column of its position, so partial tiles and
 // grids narrower than a warp see the torus neighbours.
-constexpr int FR_RPT = 2;            // rows per thread of the single-world kernels
+#ifndef FLP_FR_RPT
+#define FLP_FR_RPT 2
+#endif
+constexpr int FR_RPT = FLP_FR_RPT;   // rows per thread of the single-world kernels
 constexpr int FR_H = 8 * FR_RPT;     // tile height: 8 warps of 32 columns
 
 template <int C, int RPT = FR_RPT>
