@@ -22,6 +22,19 @@
 namespace flp {
 
 // ------------------------------------------------------ forward, batched ----
+// Rows per thread of the flow's row walk and destination rows per thread of
+// the gather for the differentiable batch (worlds of one shape, whose planes
+// together exceed L2): a taller walk reloads fewer halo rows.
+#ifndef FLP_ADJ_FR_RPT
+#define FLP_ADJ_FR_RPT 8
+#endif
+#ifndef FLP_ADJ_GBY
+#define FLP_ADJ_GBY 2
+#endif
+constexpr int ADJ_FR_RPT = FLP_ADJ_FR_RPT;
+constexpr int ADJ_FR_H = 8 * ADJ_FR_RPT;
+constexpr int ADJ_GBY = FLP_ADJ_GBY;
+
 template <int CV>
 __global__ void __launch_bounds__(256) k_flow_worlds(const float* __restrict__ A, const float* __restrict__ U,
                                                      float* __restrict__ DX, float* __restrict__ DY, int C, int W,
@@ -35,8 +48,8 @@ __global__ void __launch_bounds__(256) k_flow_worlds(const float* __restrict__ A
         flow_item(sm, A + off, U + off, DX + off, DY + off, C, W, H, fp, blockIdx.x * FL_W, blockIdx.y * FL_H,
                   dmax + w, status);
     else
-        flow_rows_item<CV>(A + off, U + off, DX + off, DY + off, W, H, fp, blockIdx.x * 32, blockIdx.y * FR_H,
-                           dmax + w, status);
+        flow_rows_item<CV, ADJ_FR_RPT>(A + off, U + off, DX + off, DY + off, W, H, fp, blockIdx.x * 32,
+                                       blockIdx.y * ADJ_FR_H, dmax + w, status);
 }
 
 template <bool POW2>
@@ -48,14 +61,14 @@ __global__ void __launch_bounds__(256, 3) k_gather_worlds(const float* __restric
     const int p = blockIdx.z, w = p / C;
     const size_t off = size_t(p) * W * H;
     const FlowParams fp = fps[w];
-    gather_item<POW2, 1>(sm, DX + off, DY + off, A + off, An + off, W, H, fp, dmax[w], blockIdx.x * GT_W,
-                      blockIdx.y * gt_h(1));
+    gather_item<POW2, ADJ_GBY>(sm, DX + off, DY + off, A + off, An + off, W, H, fp, dmax[w], blockIdx.x * GT_W,
+                               blockIdx.y * gt_h(ADJ_GBY));
 }
 
 void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, int B, int C, int W, int H,
                         const FlowParams* fps, int* dmax, int* status, cudaStream_t st) {
     const int cv = C <= 4 ? C : 0;
-    const int th = cv ? FR_H : FL_H;
+    const int th = cv ? ADJ_FR_H : FL_H;
     const dim3 grid((W + FL_W - 1) / FL_W, (H + th - 1) / th, B);
     const size_t smem = cv ? 0 : flow_smem_bytes(C);
     switch (cv) {
@@ -69,11 +82,12 @@ void launch_flow_worlds(const float* A, const float* U, float* DX, float* DY, in
 
 void launch_gather_worlds(const float* DX, const float* DY, const float* A, float* An, int B, int C, int W, int H,
                           const FlowParams* fps, bool pow2, const int* dmax, cudaStream_t st) {
-    dim3 grid((W + GT_W - 1) / GT_W, (H + gt_h(1) - 1) / gt_h(1), B * C);
+    dim3 grid((W + GT_W - 1) / GT_W, (H + gt_h(ADJ_GBY) - 1) / gt_h(ADJ_GBY), B * C);
+    const size_t smem = gather_smem_bytes_inl(ADJ_GBY);
     if (pow2)
-        k_gather_worlds<true><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, A, An, C, W, H, fps, dmax);
+        k_gather_worlds<true><<<grid, 256, smem, st>>>(DX, DY, A, An, C, W, H, fps, dmax);
     else
-        k_gather_worlds<false><<<grid, 256, gather_smem_bytes(), st>>>(DX, DY, A, An, C, W, H, fps, dmax);
+        k_gather_worlds<false><<<grid, 256, smem, st>>>(DX, DY, A, An, C, W, H, fps, dmax);
 }
 
 // U_t = sum over kernels targeting t (kernel order) of w G(conv_k), with the
@@ -428,8 +442,8 @@ void adjoint_set_attributes() {
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     };
     set((const void*)k_flow_worlds<0>, flow_smem_bytes(ADJ_MAX_CHANNELS));
-    set((const void*)k_gather_worlds<true>, gather_smem_bytes());
-    set((const void*)k_gather_worlds<false>, gather_smem_bytes());
+    set((const void*)k_gather_worlds<true>, gather_smem_bytes_inl(ADJ_GBY));
+    set((const void*)k_gather_worlds<false>, gather_smem_bytes_inl(ADJ_GBY));
     set((const void*)k_adj_flow, sizeof(float) * (2 * ADJ_MAX_CHANNELS + 1) * FL_RC);
     set((const void*)k_adj_sobel_t, sizeof(float) * (2 * ADJ_MAX_CHANNELS + 2) * FL_RC);
 }

@@ -534,6 +534,11 @@ __device__ __forceinline__ void gather_add_terms(bool add, float (&acc)[GBY][4],
         }
 }
 
+// Whether one-row tiles (GBY = 1) also take the x-edge path of gather_strip.
+#ifndef FLP_GATHER_EDGE_ONE_ROW
+#define FLP_GATHER_EDGE_ONE_ROW 0
+#endif
+
 // The 4 x GBY destinations of one thread.  Each destination sums its sources
 // in the reference's deposit order: row-major over wrapped source indices,
 // i.e. rows in wrap-pass order (rows past the bottom edge wrap to the top and
@@ -569,7 +574,7 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
     // first), instead of the edge and the inside lanes running their passes
     // one after the other.
     bool xedge = false;
-    if constexpr (RN <= 1 && GBY == 2) {
+    if constexpr (RN <= 1 && (GBY == 2 || FLP_GATHER_EDGE_ONE_ROW)) {
         const bool simple = xin || xleft || xright;
         xedge = __any_sync(__activemask(), xleft || xright) && simple;
     }
@@ -589,7 +594,7 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
 #pragma unroll
         for (int d = 0; d <= GBY; ++d) fy[d] = float(yb + d);
         const int off = (GBY * ty + r) * sw + 4 * tx;
-        if constexpr (RN <= 1 && GBY == 2) {
+        if constexpr (RN <= 1 && (GBY == 2 || FLP_GATHER_EDGE_ONE_ROW)) {
             if (xedge) {
                 constexpr int RA = 2 * TP, RB = TP + 3 + RN + 1;  // right columns
                 float vr[GBY][4][RB - RA + 1];
