@@ -566,8 +566,8 @@ __device__ __forceinline__ void gather_strip(const float* sxmin, const float* sx
     const bool xright = cp_lo == 0 && cp_hi == 1 && X0 == W - 4 && (W & 3) == 0;
     // Warps that hold an x-edge lane (X0 = 0 or X0 = W - 4) take one path for
     // all their lanes when RN <= 1 and GBY = 2 (with one destination row per
-    // thread the kept terms cost more than the edge lanes' passes; measured on
-    // the 512x512 single world): the source columns left of the thread's
+    // thread it made no measurable difference on the 512x512 single world, so
+    // it is a compile-time option there): the source columns left of the thread's
     // block (j < TP) and right of it (j >= 2 TP) are computed once, kept in
     // registers and added where each lane's wrapped order puts them (a left
     // edge lane adds the left columns last, a right edge lane the right columns
