@@ -69,6 +69,8 @@ def parse_args():
     ap.add_argument("--embedded-size", type=int, default=256, help="side of the parameter-embedded world (0 = skip)")
     ap.add_argument("--record-steps", type=int, default=400, help="steps of the recording measurement (0 = skip)")
     ap.add_argument("--sweep-worlds", type=int, default=1024, help="worlds of the parameter-sweep measurement (0 = skip)")
+    ap.add_argument("--other-steps", type=int, default=1000,
+                    help="steps of the blob 256^2 and sphere 128^3 measurements beside the headline (0 = skip)")
     return ap.parse_args()
 
 
@@ -529,6 +531,41 @@ def measure_recording(args, dist, cfg, state, mode):
             "frames": stats["frame_count"], "mib_per_s_written": stats["total_bytes"] / 2**20 / t}
 
 
+def measure_other_configs(args, dist, headline: str):
+    """The other single-world configurations on the same path (blob 256^2,
+    1 channel, R=13; sphere 128^3, R=10): device step rate with the L2 flushed
+    before every step, the per-kernel split and the dominant kernel's fraction
+    of the measured HBM bandwidth."""
+    import autoverse_b200 as fl
+    peak, _ = hbm_peak()
+    out = {}
+    for name in ("blob256", "sphere128"):
+        if name == headline:
+            continue
+        cfg, state, desc = workload(name, engine=True)
+        cells = cfg["width"] * cfg["height"] * cfg.get("depth", 1)
+        with fl.CudaPropagator(cfg) as p:
+            p.write_state(state)
+            p.profile_run(5, flush_l2=True)
+            prof = p.profile_run(args.other_steps, flush_l2=True, stages=False)
+            t = reduce_max(dist, prof["step_ms"] / 1e3)
+            n_st = min(args.other_steps, 300)
+            st = p.profile_run(n_st, flush_l2=True, stages=True)["stages"]
+            dom = max(st, key=st.get)
+            dom_ms = st[dom] / n_st
+            b = stage_bytes(cfg, dom)
+            ach = b / (dom_ms * 1e-3) / 1e9 if b else None
+            out[name] = {"workload": desc["workload"], "conv_path": {fl.CONV_DIRECT: "direct",
+                                                                     fl.CONV_FFT: "fft"}[p.conv_mode],
+                         "steps": args.other_steps, "us_per_step": 1e6 * t / args.other_steps,
+                         "value": WORLD * cells * args.other_steps / t, "unit": "cell-steps/s",
+                         "stage_us_per_step": {k: 1e3 * v / n_st for k, v in st.items()},
+                         "roofline": {"kernel": dom, "achieved": ach, "unit": "GB/s",
+                                      "frac": ach / peak if ach else None, "algorithmic_bytes_per_launch": b},
+                         "l2": "flushed before every timed step"}
+    return out
+
+
 def measure_sweep(args, dist):
     """Parameter sweep: `--sweep-worlds` worlds of 256x256, 2 channels, 4
     kernels with one set of kernel shapes and per-world weights, mu, sigma,
@@ -662,6 +699,7 @@ def main():
     embedded = measure_embedded(args, dist) if args.embedded_size > 0 else None
     recording = measure_recording(args, dist, cfg, state, p.conv_mode) if args.record_steps > 0 else None
     sweep = measure_sweep(args, dist) if args.sweep_worlds > 0 else None
+    others = measure_other_configs(args, dist, args.workload) if args.other_steps > 0 else None
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.skip_cpu:
@@ -702,6 +740,7 @@ def main():
         "embedded": embedded,
         "recording": recording,
         "sweep": sweep,
+        "other_configs": others,
     }
     print(json.dumps(line), flush=True)
 
