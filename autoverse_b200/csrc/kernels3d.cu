@@ -330,10 +330,20 @@ __device__ float gather3d_generic(const float* __restrict__ DX, const float* __r
 // of once per (source, destination) pair.
 constexpr int G3_NZ = 8;
 
+// With PAIRS a thread takes its column's output planes two at a time (Z and
+// Z+1): a source's mass and its x and y overlaps serve both destinations and
+// the first product ow * oh of its volume is shared, so a pair of terms takes
+// five shared-memory loads instead of eight.  The ring then holds 2RN+3
+// planes.  Pairs whose z windows wrap the torus take the planes one by one.
+#ifndef FLP_GATHER3D_PAIRS
+#define FLP_GATHER3D_PAIRS 1
+#endif
+constexpr bool G3_PAIRS = FLP_GATHER3D_PAIRS != 0;
+
 template <int RN>
 struct March3 {
     static constexpr int SW = G3_W + 2 * RN + 1, SH = G3_H + 2 * RN + 1, NS = SW * SH;
-    static constexpr int NW = 2 * RN + 2, SD = 2 * RN + 2;
+    static constexpr int NW = 2 * RN + 2, SD = 2 * RN + 2 + (G3_PAIRS ? 1 : 0);
     static constexpr int PLANE = (3 * NW + 1) * NS;  // floats per ring slot
     static constexpr size_t bytes = sizeof(float) * size_t(SD) * PLANE;
 };
@@ -370,8 +380,9 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
             }
         }
     };
+    auto slot = [&](int gz) { return sm + ((gz - (z0 - RN)) % SD) * M::PLANE; };
     auto store = [&](int gz, const float (&r)[4][NSP]) {
-        float* P = sm + ((gz - (z0 - RN)) % SD) * M::PLANE;
+        float* P = slot(gz);
         float* OW = P;
         float* OH = P + NW * NS;
         float* OD = P + 2 * NW * NS;
@@ -397,53 +408,127 @@ __device__ void gather3d_march(float* sm, const float* __restrict__ DX, const fl
             }
         }
     };
-    float raw[4][NSP];
-    for (int gz = z0 - RN; gz <= z0 + RN; ++gz) {
-        fetch(gz, raw);
-        store(gz, raw);
-    }
-    fetch(z0 + RN + 1, raw);
+    auto term = [&](float m, float vol) -> float {
+        if (POW2) return __fmul_rn(m, vol);
+        return (m != 0.f && vol > 0.f) ? __fmul_rn(m, __fdiv_rn(vol, fp.total_area)) : 0.f;
+    };
     const int lx = tid & (G3_W - 1), ly = tid / G3_W;
     const int X = x0 + lx, Y = y0 + ly;
+    const bool inside = X < W && Y < H;
     // The wrapped-ascending x order (rot_window) is the natural order
     // kx = -RN..RN+1 rotated left by rx, so the terms are computed at fixed
     // shared-memory offsets and rotated in registers before they are added.
     const int rx = window_rotation(X, RN, W);
-    for (int zz = 0; zz < nz; ++zz) {
-        const int Z = z0 + zz;
-        store(Z + RN + 1, raw);
-        __syncthreads();
-        if (zz + 1 < nz) fetch(Z + RN + 2, raw);
-        if (X < W && Y < H) {
-            float acc = 0.f;
-            for (int jz = 0; jz < NW; ++jz) {
-                const int kz = rot_window(jz, Z, RN, D);
-                const float* P = sm + ((Z + kz - (z0 - RN)) % SD) * M::PLANE;
-                const float* OW = P;
-                const float* OHk = P + NW * NS;
-                const float* ODk = P + 2 * NW * NS + (kz + RN) * NS;
-                const float* Mm = P + 3 * NW * NS;
+    // One output plane Z, its source planes in wrapped-ascending z order.
+    auto single = [&](int Z) {
+        float acc = 0.f;
+        for (int jz = 0; jz < NW; ++jz) {
+            const int kz = rot_window(jz, Z, RN, D);
+            const float* P = slot(Z + kz);
+            const float* OW = P;
+            const float* OHk = P + NW * NS;
+            const float* ODk = P + 2 * NW * NS + (kz + RN) * NS;
+            const float* Mm = P + 3 * NW * NS;
 #pragma unroll
-                for (int jy = 0; jy < NW; ++jy) {
-                    const int ky = rot_window(jy, Y, RN, H);
-                    const int base = (ly + ky + RN) * SW + lx;  // source of kx = -RN
-                    const float* OHr = OHk + (ky + RN) * NS + base;
-                    float t[NW];
+            for (int jy = 0; jy < NW; ++jy) {
+                const int ky = rot_window(jy, Y, RN, H);
+                const int base = (ly + ky + RN) * SW + lx;  // source of kx = -RN
+                const float* OHr = OHk + (ky + RN) * NS + base;
+                float t[NW];
 #pragma unroll
-                    for (int i = 0; i < NW; ++i) {
-                        const float m = Mm[base + i];
-                        const float vol = __fmul_rn(__fmul_rn(OW[i * NS + base + i], OHr[i]), ODk[base + i]);
-                        if (POW2) t[i] = __fmul_rn(m, vol);
-                        else t[i] = (m != 0.f && vol > 0.f) ? __fmul_rn(m, __fdiv_rn(vol, fp.total_area)) : 0.f;
-                    }
-                    rotate_left<NW>(t, rx);
+                for (int i = 0; i < NW; ++i)
+                    t[i] = term(Mm[base + i], __fmul_rn(__fmul_rn(OW[i * NS + base + i], OHr[i]), ODk[base + i]));
+                rotate_left<NW>(t, rx);
 #pragma unroll
-                    for (int i = 0; i < NW; ++i) acc = __fadd_rn(acc, t[i]);
+                for (int i = 0; i < NW; ++i) acc = __fadd_rn(acc, t[i]);
+            }
+        }
+        out[(size_t(Z) * H + Y) * W + X] = acc;
+    };
+    // Output planes Z and Z+1 whose z windows do not wrap: source planes
+    // Z-RN .. Z+RN+2 in ascending order, the first for Z only, the last for
+    // Z+1 only; each destination adds its terms in the same order as single().
+    auto pair = [&](int Z) {
+        float acc0 = 0.f, acc1 = 0.f;
+#pragma unroll
+        for (int r = 0; r <= NW; ++r) {
+            const float* P = slot(Z - RN + r);
+            const float* OW = P;
+            const float* OHk = P + NW * NS;
+            const float* OD0 = P + 2 * NW * NS + r * NS;        // kz = r - RN for plane Z
+            const float* OD1 = P + 2 * NW * NS + (r - 1) * NS;  // kz = r - RN - 1 for plane Z+1
+            const float* Mm = P + 3 * NW * NS;
+#pragma unroll
+            for (int jy = 0; jy < NW; ++jy) {
+                const int ky = rot_window(jy, Y, RN, H);
+                const int base = (ly + ky + RN) * SW + lx;
+                const float* OHr = OHk + (ky + RN) * NS + base;
+                float t0[NW], t1[NW];
+#pragma unroll
+                for (int i = 0; i < NW; ++i) {
+                    const float m = Mm[base + i];
+                    const float wh = __fmul_rn(OW[i * NS + base + i], OHr[i]);
+                    if (r < NW) t0[i] = term(m, __fmul_rn(wh, OD0[base + i]));
+                    if (r > 0) t1[i] = term(m, __fmul_rn(wh, OD1[base + i]));
+                }
+                if (r < NW) {
+                    rotate_left<NW>(t0, rx);
+#pragma unroll
+                    for (int i = 0; i < NW; ++i) acc0 = __fadd_rn(acc0, t0[i]);
+                }
+                if (r > 0) {
+                    rotate_left<NW>(t1, rx);
+#pragma unroll
+                    for (int i = 0; i < NW; ++i) acc1 = __fadd_rn(acc1, t1[i]);
                 }
             }
-            out[(size_t(Z) * H + Y) * W + X] = acc;
         }
-        __syncthreads();
+        out[(size_t(Z) * H + Y) * W + X] = acc0;
+        out[(size_t(Z + 1) * H + Y) * W + X] = acc1;
+    };
+    if constexpr (!G3_PAIRS) {
+        float raw[4][NSP];
+        for (int gz = z0 - RN; gz <= z0 + RN; ++gz) {
+            fetch(gz, raw);
+            store(gz, raw);
+        }
+        fetch(z0 + RN + 1, raw);
+        for (int zz = 0; zz < nz; ++zz) {
+            const int Z = z0 + zz;
+            store(Z + RN + 1, raw);
+            __syncthreads();
+            if (zz + 1 < nz) fetch(Z + RN + 2, raw);
+            if (inside) single(Z);
+            __syncthreads();
+        }
+    } else {
+        float ra[4][NSP], rb[4][NSP];
+        for (int gz = z0 - RN; gz <= z0 + RN; ++gz) {
+            fetch(gz, ra);
+            store(gz, ra);
+        }
+        fetch(z0 + RN + 1, ra);
+        if (nz > 1) fetch(z0 + RN + 2, rb);
+        for (int zz = 0; zz < nz; zz += 2) {
+            const int Z = z0 + zz;
+            const bool two = zz + 1 < nz;
+            store(Z + RN + 1, ra);
+            if (two) store(Z + RN + 2, rb);
+            __syncthreads();
+            if (zz + 2 < nz) fetch(Z + RN + 3, ra);
+            if (zz + 3 < nz) fetch(Z + RN + 4, rb);
+            if (inside) {
+                if (!two) {
+                    single(Z);
+                } else if (Z - RN >= 0 && Z + RN + 2 < D) {
+                    pair(Z);
+                } else {
+                    single(Z);
+                    single(Z + 1);
+                }
+            }
+            __syncthreads();
+        }
     }
 }
 
