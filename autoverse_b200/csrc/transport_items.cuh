@@ -534,6 +534,62 @@ __device__ __forceinline__ void gather_add_terms(bool add, float (&acc)[GBY][4],
         }
 }
 
+// The 4 x GBY destinations of a thread whose whole source window lies inside
+// the torus (no row or column wraps), in a warp whose lanes all do: source
+// rows in natural order, one column pass each.  Out of line, so that the
+// common case gets its own register allocation and none of the edge paths'
+// code.  Taken by the one-row tiles (single world: gather 18.7 -> 18.5 us,
+// step 50.8 -> 49.3 us at 512x512); with two rows per thread the call's stack
+// frame cost more than it saved (4096-world batch gather 3.40 -> 3.66 ms).
+#ifndef FLP_GATHER_INNER_STRIP
+#define FLP_GATHER_INNER_STRIP 1
+#endif
+template <int RN, bool POW2, int GBY, bool WIDE>
+__device__ __noinline__ void gather_strip_inner(const float* sxmin, const float* sxmax, const float* symin,
+                                                const float* symax, const float* smass, float* __restrict__ out,
+                                                int W, int H, float total_area, int x0, int y0, int sw, int tx,
+                                                int ty) {
+    const int Y0 = y0 + GBY * ty, X0 = x0 + 4 * tx;
+    float acc[GBY][4];
+#pragma unroll
+    for (int d = 0; d < GBY; ++d)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[d][i] = 0.f;
+    const int gx_base = x0 - TP + 4 * tx;
+    float fxs[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) fxs[i] = float(X0 + i);
+    constexpr int NSY = GBY + 2 * RN + 1;
+    auto row = [&](auto dm, int r) {
+        constexpr int DM = decltype(dm)::value;
+        float fy[GBY + 1];
+#pragma unroll
+        for (int d = 0; d <= GBY; ++d) fy[d] = float(Y0 + d);
+        const int off = (GBY * ty + r) * sw + 4 * tx;
+        gather_row<WIDE, RN, POW2, false, DM, GBY>(sxmin + off, sxmax + off, symin + off, symax + off, smass + off,
+                                                   fy, fxs, X0, gx_base, W, 1, total_area, acc);
+    };
+    if constexpr (GBY == 1) {
+#pragma unroll 1
+        for (int r = 0; r < NSY; ++r) row(std::integral_constant<int, 1>(), r);
+    } else {
+        row(std::integral_constant<int, 1>(), 0);
+#pragma unroll 1
+        for (int r = 1; r < NSY - 1; ++r) row(std::integral_constant<int, 3>(), r);
+        row(std::integral_constant<int, 2>(), NSY - 1);
+    }
+#pragma unroll
+    for (int d = 0; d < GBY; ++d) {
+        float* o = out + size_t(Y0 + d) * W;
+        if ((W & 3) == 0) {
+            *reinterpret_cast<float4*>(o + X0) = make_float4(acc[d][0], acc[d][1], acc[d][2], acc[d][3]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[X0 + i] = acc[d][i];
+        }
+    }
+}
+
 // Whether one-row tiles (GBY = 1) also take the x-edge path of gather_strip.
 #ifndef FLP_GATHER_EDGE_ONE_ROW
 #define FLP_GATHER_EDGE_ONE_ROW 0
@@ -775,7 +831,16 @@ __device__ __noinline__ void gather_body(float* sm, const float* __restrict__ DX
     }
     __syncthreads();
     if (y0 + GBY * ty < H && x0 + 4 * tx < W)
-        gather_strip<RN, POW2, GBY, WIDE>(sxmin, sxmax, symin, symax, smass, out, W, H, fp, x0, y0, sw, tx, ty);
+    {
+        const int Y0 = y0 + GBY * ty, X0 = x0 + 4 * tx;
+        // a lane whose window wraps neither a row nor a column of the torus
+        const bool inner = Y0 - RN >= 0 && Y0 + GBY + RN < H && X0 - RN >= 0 && X0 + 4 + RN < W;
+        if (FLP_GATHER_INNER_STRIP && GBY == 1 && __all_sync(__activemask(), inner))
+            gather_strip_inner<RN, POW2, GBY, WIDE>(sxmin, sxmax, symin, symax, smass, out, W, H, fp.total_area, x0,
+                                                    y0, sw, tx, ty);
+        else
+            gather_strip<RN, POW2, GBY, WIDE>(sxmin, sxmax, symin, symax, smass, out, W, H, fp, x0, y0, sw, tx, ty);
+    }
     __syncthreads();
 }
 
