@@ -307,7 +307,8 @@ def measure_batched(args, dist):
            "value": sum(c["width"] * c["height"] for c, _ in everything) * args.batch_steps / t, "unit": "cell-steps/s",
            "ms_per_step": 1e3 * t / args.batch_steps,
            "stage_ms_per_step": stage_ms, "roofline": roof,
-           "gpu_launches_per_step": 1 + 3 * 7 + 2, "l2": "working set above L2 (pooled state and spectra)"}
+           # queue reset, three FFT stages x 7 size classes, the flow's 2 channel-count classes, the gather
+           "gpu_launches_per_step": 1 + 3 * 7 + 2 + 1, "l2": "working set above L2 (pooled state and spectra)"}
     b.close()
     if RANK == 0 and not args.skip_cpu:
         out["cpu_baseline"] = cpu_worlds_run(worlds, args.cpu_seconds)
