@@ -131,3 +131,21 @@ def test_batch_layout_match_rules():
     ks = swapped[two]["kernels"]
     ks[0], ks[1] = ks[1], ks[0]
     assert not b.layout_matches(swapped)
+
+
+def test_twin64_rejects_before_device_work():
+    """flp_twin64_step checks its arguments and the config on the host before
+    it touches the device: a null buffer, an invalid config and a 3D world
+    (the twin covers 2D steps) are refused with their codes."""
+    lib = nat.lib()
+    cfg = wl.config(16, 16, 1, [wl.kernel()])
+    a = np.zeros(16 * 16, np.float64)
+    out = np.zeros_like(a)
+    rc = lib.flp_twin64_step(json.dumps(cfg).encode(), None, None, out.ctypes.data)
+    assert rc == -2
+    bad = dict(cfg, dt=0.0)
+    rc = lib.flp_twin64_step(json.dumps(bad).encode(), a.ctypes.data, None, out.ctypes.data)
+    assert rc == -1 and b"Time step" in lib.flp_last_error()
+    cube = dict(cfg, depth=32, width=32, height=32)
+    rc = lib.flp_twin64_step(json.dumps(cube).encode(), a.ctypes.data, None, out.ctypes.data)
+    assert rc == -7 and b"2D" in lib.flp_last_error()
