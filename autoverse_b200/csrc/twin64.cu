@@ -179,11 +179,14 @@ extern "C" int flp_twin64_step(const char* config_json, const double* state, dou
         }
         // Window: every source that can reach a destination, plus one cell; a
         // wider window adds only sources without overlap, which are skipped.
+        // Capped like the engine's window (a non-finite displacement reaches
+        // every cell); windows wider than the grid take the general path's
+        // frame-by-frame visit.
         double dmax = 0.0;
         std::memcpy(&dmax, &bits, sizeof(dmax));
         const double reach = std::ceil(dmax + double(fp.s)) + 1.0;
-        const int lim = (std::min(W, H) - 1) / 2;
-        const int R = reach < double(lim) ? std::max(1, int(reach)) : lim;
+        const int cap = 2 * std::max(W, H) + 2;
+        const int R = reach < double(cap) ? std::max(1, int(reach)) : cap;
         if (fp.area_pow2)
             twin_gather_2d<true><<<dim3((W + 127) / 128, H, C), 128>>>(dDX.p, dDY.p, dA.p, dOut.p, W, H, R, fp);
         else
